@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark: compartment-steps/s of the batched neuron simulation on B200.
+
+Workload (``ttpc_like``): a seeded ~1500-compartment thick-tufted pyramidal
+morphology with the 13-mechanism TTPC channel set, 4096 parameter sets x 3
+stimulus protocols = 12288 instances, dt = 0.025 ms (the 2000 ms protocol is
+80000 steps).  One bench "step" is one pass of the hot path over the whole
+batch for ``--chunk`` timesteps (default 800 = 20 ms of simulated time),
+continuing from the resident state of the previous step.
+
+Timing: W untimed warm-up steps, then exactly K steps between barriers and
+device syncs, timed with CUDA events on the launching stream; max over
+ranks.  The simulation state (>400 MB) is larger than L2, so every step
+streams it from HBM.  ``--gpus N`` runs one process per GPU (torchrun), each
+rank its own 12288-instance batch (weak scaling, no data-path collective).
+
+``--impl reference`` times the reference's CPU path for the same
+configuration.  The reference has no usable CPU implementation of this path
+(its serial path is compiled out and calls an undefined function), so the
+CPU restatement in oracle/ (FP64, OpenMP over all host threads) stands in.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "compartment-steps/s (TTPC-like x4096)"
+UNIT = "compartment-steps/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+TRAFFIC_FILE = ROOT / "profiles" / "ttpc_like_sim_advance.md"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ngpu", choices=["ngpu", "reference"])
+    ap.add_argument("--chunk", type=int, default=800, help="timesteps per bench step")
+    ap.add_argument("--n-sets", type=int, default=4096)
+    ap.add_argument("--e2e-steps", type=int, default=2000, help="timesteps of the end-to-end run")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-sets", type=int, default=16)
+    ap.add_argument("--cpu-sample-steps", type=int, default=400)
+    return ap.parse_args()
+
+
+def workload(n_sets: int):
+    from neurogpu_b200 import configs
+    return configs.ttpc_like(n_sets=n_sets)
+
+
+def hbm_peak():
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_comp_step():
+    """DRAM bytes per compartment-step of the advance kernel from the
+    committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum)."""
+    try:
+        m = re.search(r"traffic_bytes_per_compartment_step:\s*([0-9.eE+-]+)", TRAFFIC_FILE.read_text())
+        return float(m.group(1)) if m else None
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(w, n_sets: int, n_steps: int) -> dict:
+    """Oracle (FP64 C restatement, OpenMP over instances) on a bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py
+    sub = w.subset(n_sets=n_sets, nt=n_steps)
+    threads = os.cpu_count() or 1
+    oracle_py.run_workload(sub.subset(n_sets=1, n_stim=1, nt=10), n_threads=threads)  # warm
+    t = time.perf_counter()
+    oracle_py.run_workload(sub, n_threads=threads)
+    el = time.perf_counter() - t
+    cs = sub.compartment_steps()
+    return {"value": cs / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sub.n_sets} sets x {sub.n_stim} stimuli x {n_steps} steps of the same "
+                      f"{w.cell.n_nodes}-compartment model ({cs:.3e} compartment-steps, {el:.1f} s, FP64)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(args.n_sets)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py
+    # bounded sample per step: a few instances x a short window, all host threads
+    n_sets = max(1, threads // w.n_stim)
+    sub = w.subset(n_sets=n_sets, nt=args.cpu_sample_steps)
+    for _ in range(args.warmup):
+        oracle_py.run_workload(sub.subset(nt=20), n_threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        oracle_py.run_workload(sub, n_threads=threads)
+        times.append(time.perf_counter() - t)
+    el = float(np.mean(times))
+    v = sub.compartment_steps() / el
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": "ttpc_like", "n_nodes": w.cell.n_nodes, "n_sets": args.n_sets,
+                   "n_stim": w.n_stim, "dt_ms": w.dt},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sub.n_sets} sets x {sub.n_stim} stimuli x {sub.nt} steps per step"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    from neurogpu_b200 import _ffi
+    from neurogpu_b200.sim import Model, Simulator, run
+    rank, world, local = dist_setup(args.gpus)
+    w = workload(args.n_sets)
+    n_inst = w.n_sets * w.n_stim
+    total_steps = (args.warmup + args.steps) * args.chunk
+    if total_steps > w.nt:
+        raise SystemExit(f"warmup+steps x chunk = {total_steps} exceeds the protocol ({w.nt} steps)")
+    model = Model(w.cell)
+    sim = Simulator(model, w.n_sets, w.n_stim, "fp32")
+    sim.set_params(w.params)
+    sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+    sim.set_recording(w.rec_nodes, 1)
+    stream = torch.cuda.current_stream()
+    sim.init(w.v_init, stream)
+    t = 0
+    for _ in range(args.warmup):
+        sim.advance(t, args.chunk, stream)
+        t += args.chunk
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    torch.cuda.synchronize()
+    barrier(world)
+    _ffi.lib().ngpu_launch_count(1)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launch_ms = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.advance(t, args.chunk, stream)
+        b.record(stream)
+        launch_ms.append((a, b))
+        t += args.chunk
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(_ffi.lib().ngpu_launch_count(0))
+    barrier(world)
+    clk = clocks.stop() if clocks else None
+    el_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    per_launch_ms = float(np.mean([a.elapsed_time(b) for a, b in launch_ms]))
+    n_bad = sim.n_bad()
+    comp_steps_rank = w.cell.n_nodes * args.chunk * n_inst * args.steps
+    value = comp_steps_rank * world / (el_ms / 1e3)
+
+    # roofline of the advance kernel: algorithmic bytes per launch / launch time
+    bytes_per_step = w.cell.algorithmic_bytes_per_step() * n_inst  # one timestep, all instances
+    alg_bytes_launch = bytes_per_step * args.chunk
+    achieved_gbs = alg_bytes_launch / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    tpcs = traffic_per_comp_step()
+    traffic = None if tpcs is None else tpcs * w.cell.n_nodes * n_inst * args.chunk
+
+    # end to end through the public host-buffer entry point (ngpu_run)
+    e2e = None
+    if not args.no_e2e:
+        we = w.subset(nt=args.e2e_steps)
+        run(model, we.params, we.amps, we.dts, we.stim_node, we.stim_area, we.rec_nodes, we.v_init)
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        out = run(model, we.params, we.amps, we.dts, we.stim_node, we.stim_area, we.rec_nodes, we.v_init)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+        h2d = we.params.nbytes + we.amps.nbytes + we.dts.nbytes + we.rec_nodes.nbytes
+        e2e = {"value": we.compartment_steps() * world / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(out.nbytes),
+               "timesteps": args.e2e_steps, "seconds": e2e_s}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, args.cpu_sample_sets // 1, args.cpu_sample_steps)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "ttpc_like", "n_nodes": w.cell.n_nodes, "n_sets": w.n_sets,
+                       "n_stim": w.n_stim, "instances_per_gpu": n_inst, "dt_ms": w.dt,
+                       "timesteps_per_step": args.chunk, "l2": "state larger than L2 (no flush)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": achieved_gbs / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_compartment_step":
+                             w.cell.algorithmic_bytes_per_step() / w.cell.n_nodes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "non_finite_instances": n_bad,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    model.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,121 @@
+/*
+ * libngpu -- C ABI of the B200 NeuroGPU simulation core.
+ *
+ * Plain pointers and sizes only.  Every call returns 0 on success or a
+ * negative NGPU_E* code; ngpu_last_error() gives a thread-local message.
+ * Nothing here exits, aborts or traps.  Host pointers are caller-owned;
+ * device buffers are owned by the model / sim handles.
+ *
+ * Reference interfaces replaced (paths in the reference project; U/ =
+ * GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/):
+ *   - the files-and-process boundary: Python writes Data/AllParams.csv
+ *     (NeuroGPU_Base/scripts/template/extractModel_mappings.py:326-330) and
+ *     spawns ../bin/neuroGPU <stim> (Figures/Figure4_DEAP/
+ *     neurogpu_multistim_evaluator_par.py:175); U/kernel.cu:8-33 main;
+ *   - topology upload U/CudaStuff.cu:372-437 (initFrameWork, topology into
+ *     __constant__), read from BasicConstSegP.csv by U/MainC.cu:335-551;
+ *   - launch and copies U/CudaStuff.cu:443-516 (callKernel) and
+ *     U/CudaStuff.cu:518-587 (stEfork2Main: timing, VHotP<dev>.dat output).
+ */
+#ifndef NGPU_H
+#define NGPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NGPU_ABI_VERSION 1
+
+enum {
+    NGPU_OK = 0,
+    NGPU_E_INVALID = -1,   /* bad argument / malformed model */
+    NGPU_E_CUDA = -2,      /* a CUDA runtime call failed */
+    NGPU_E_NOMEM = -3,     /* host or device allocation failed */
+    NGPU_E_STATE = -4,     /* call out of order (e.g. advance before init) */
+    NGPU_E_NUMERIC = -5    /* non-finite voltage detected in a run */
+};
+
+/* Mechanism sets compiled into the library (the reference generates one
+ * channel library per model: U/AllModels.cu for the TTPC cell,
+ * Figures/FigureS4_mainen/CParsed/AllModels.cu for the Mainen cell). */
+enum { NGPU_MECHSET_TTPC = 0, NGPU_MECHSET_MAINEN = 1 };
+enum { NGPU_FP32 = 0, NGPU_FP64 = 1 };
+
+typedef struct ngpu_model ngpu_model;
+typedef struct ngpu_sim ngpu_sim;
+
+const char *ngpu_last_error(void);
+int ngpu_abi_version(void);
+/* Mechanism set description: number of mechanisms / parameters. */
+int ngpu_mechset_info(int32_t mechset, int32_t *n_mech, int32_t *n_params);
+
+/*
+ * Morphology + channel placement, shared by every instance.
+ * Replaces ReadParallelNeuronData + initFrameWork (U/MainC.cu:335-551,
+ * U/CudaStuff.cu:372-437).
+ *   parent[n]   parent node, -1 for the root; parent[i] < i (Hines order).
+ *               The reference's parent of node i is N - Ks[N-i] (U/CudaStuff.cu:195).
+ *   a[n], b[n]  axial coupling: row i holds a[i] in column parent(i); row
+ *               parent(i) holds b[i] in column i (the reference's f and e,
+ *               read reversed from BasicConstSegP.csv lines 3-4).
+ *   cm[n]       uF/cm2;  section[n]: node -> parameter section (SegToComp)
+ *   mech_mask   [n_mech][n] 0/1, the reference's boolModel (line 9)
+ */
+int ngpu_model_create(int32_t n_nodes, const int32_t *parent, const double *a, const double *b,
+                      const double *cm, const int32_t *section, int32_t n_sections,
+                      int32_t mechset, const uint8_t *mech_mask, ngpu_model **out);
+int ngpu_model_destroy(ngpu_model *m);
+/* Derived layout numbers (for tests and the bench's byte accounting). */
+int ngpu_model_layout(const ngpu_model *m, int32_t *state_rows, int32_t *param_rows,
+                      int32_t *n_jslots, int64_t *state_vars, int64_t *param_reads);
+
+/*
+ * One complete run from host buffers (the drop-in for one neuroGPU process).
+ * Replaces callKernel + stEfork2Main (U/CudaStuff.cu:443-587).
+ *   params [n_sets][n_params][n_sections] float (AllParams.csv rows, U/Util.cu:210-234)
+ *   amps   [n_stim][nt] nA (Stim_raw.csv); dts [nt] ms (times.csv)
+ *   stim_node, stim_area_um2: Stim_meta.csv loc (0-based) and area
+ *   rec_nodes[n_rec]: recorded nodes (Sim.csv RecSites)
+ *   out    [n_sets][n_stim][n_rec][nt] float: V before step t's update
+ *          (U/CudaStuff.cu:234-248, VHotP layout U/CudaStuff.cu:237)
+ *   precision: NGPU_FP32 (production) or NGPU_FP64 (GPU oracle run)
+ */
+int ngpu_run(ngpu_model *m, int32_t n_sets, const float *params, int32_t n_stim, int32_t nt,
+             const float *amps, const float *dts, int32_t stim_node, float stim_area_um2,
+             int32_t n_rec, const int32_t *rec_nodes, float v_init, int32_t precision,
+             float *out);
+
+/* ---- resident simulation: state stays in HBM across calls ---- */
+/* n_sets x n_stim instances; instance k*n_stim + s runs set k on stimulus s. */
+int ngpu_sim_create(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision,
+                    ngpu_sim **out);
+int ngpu_sim_destroy(ngpu_sim *s);
+/* params as in ngpu_run; on_device != 0: a device pointer. */
+int ngpu_sim_set_params(ngpu_sim *s, const float *params, int32_t on_device);
+int ngpu_sim_set_stimulus(ngpu_sim *s, int32_t nt, const float *amps, const float *dts,
+                          int32_t stim_node, float stim_area_um2, int32_t on_device);
+/* rec_every: record every k-th step (1 = every step, as the reference). */
+int ngpu_sim_set_recording(ngpu_sim *s, int32_t n_rec, const int32_t *rec_nodes,
+                           int32_t rec_every);
+/* V := v_init, channel states := steady state (U/CudaStuff.cu:186-221). */
+int ngpu_sim_init(ngpu_sim *s, float v_init, void *cuda_stream);
+/* Steps [t0, t0 + n_steps) of the stimulus, enqueued on cuda_stream. */
+int ngpu_sim_advance(ngpu_sim *s, int32_t t0, int32_t n_steps, void *cuda_stream);
+/* Number of recorded samples per (instance, site): ceil(nt / rec_every). */
+int ngpu_sim_n_samples(const ngpu_sim *s);
+/* out [n_sets][n_stim][n_rec][n_samples]; on_device != 0: device pointer. */
+int ngpu_sim_get_trace(ngpu_sim *s, float *out, int32_t on_device, void *cuda_stream);
+/* Count of instances whose voltage became non-finite (read after sync). */
+int ngpu_sim_check(ngpu_sim *s, int32_t *n_bad, void *cuda_stream);
+/* Device pointer of the trace buffer, layout [n_samples][n_rec][n_inst_padded]. */
+int ngpu_sim_trace_device(ngpu_sim *s, const float **trace, int32_t *n_inst_padded);
+
+/* Kernel launches issued by this thread since the last call (for accounting). */
+int64_t ngpu_launch_count(int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

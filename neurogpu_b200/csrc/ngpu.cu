@@ -1,0 +1,615 @@
+// libngpu: host runtime and C ABI (include/ngpu.h) of the B200 simulation core.
+//
+// Builds the per-node layout (state rows, parameter rows, junction slots)
+// from the morphology and channel placement once per model, owns the device
+// buffers of each resident simulation, and launches the kernels of
+// sim_kernels.cuh.  No call exits, aborts or traps; every error is a negative
+// return code plus a thread-local message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ngpu.h"
+#include "sim_kernels.cuh"
+
+using namespace ngpu;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<int64_t> g_launches{0};
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define NGPU_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(NGPU_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Mechanism-set tables: per mechanism, the reference parameter indices it
+// reads (in the order the channel code consumes them) and its state rows.
+struct MechDesc {
+    std::vector<int> params;
+    int state_rows;
+};
+struct SetDesc {
+    int n_params;
+    std::vector<MechDesc> mechs;
+    // bits that require a calcium-dynamics mechanism on the same node
+    uint32_t needs_ca_dyn;
+    uint32_t ca_dyn_bit;
+};
+
+const SetDesc& set_desc(int ms) {
+    // TTPC: GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/CudaStuff.cu:220 call list.
+    static const SetDesc ttpc = {
+        19,
+        {{{0}, 2}, {{1}, 2}, {{2, 3, 4, 5}, 2}, {{6, 7}, 1}, {{8}, 1}, {{9}, 2}, {{10}, 2},
+         {{11}, 2}, {{12}, 2}, {{13}, 2}, {{14, 15}, 0}, {{16, 17}, 1}, {{18}, 1}},
+        TTPC::kCaHVA | TTPC::kCaLVA, TTPC::kCaDyn};
+    // Mainen: Figures/FigureS4_mainen/CParsed/AllModels.cuh:63 call list
+    // (ca's cao argument is never read by the channel code).
+    static const SetDesc mainen = {
+        34,
+        {{{0}, 2}, {{}, 2}, {{2, 3, 4, 5}, 1}, {{6, 7, 8, 9, 10}, 1}, {{11, 12, 13, 14, 15}, 1},
+         {{16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27}, 2}, {{28, 29}, 0}, {{30, 31}, 0},
+         {{32, 33}, 0}},
+        Mainen::kCa, Mainen::kCad};
+    return ms == NGPU_MECHSET_TTPC ? ttpc : mainen;
+}
+
+void* dmalloc(size_t bytes, int* rc) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        *rc = fail(NGPU_E_NOMEM, std::string("cudaMalloc(") + std::to_string(bytes) +
+                                     "): " + cudaGetErrorString(e));
+        return nullptr;
+    }
+    return p;
+}
+
+}  // namespace
+
+struct ngpu_model {
+    int n = 0, n_sections = 0, mechset = 0, n_mech = 0, n_params = 0;
+    std::vector<int> parent, section;
+    std::vector<double> a, b, cm;
+    std::vector<uint32_t> mask;
+    std::vector<NodeInfo> info;  // rec filled per simulation
+    std::vector<int> row_param, row_sec;
+    int slab_rows = 0, ptab_rows = 0, n_jslots = 0;
+    int64_t state_vars = 0, param_reads = 0;
+    std::vector<double> dconst;
+};
+
+struct ngpu_sim {
+    ngpu_model* m = nullptr;
+    int n_sets = 0, n_stim = 0, n_inst = 0, n_groups = 0, n_pad = 0, precision = 0;
+    // device buffers
+    NodeInfo* d_info = nullptr;
+    void* d_coef = nullptr;
+    void* d_slab = nullptr;
+    float* d_ptab = nullptr;
+    void* d_scr = nullptr;
+    double* d_jacc = nullptr;
+    void* d_jx = nullptr;
+    int* d_inst_stim = nullptr;
+    int* d_bad = nullptr;
+    int* d_row_param = nullptr;
+    int* d_row_sec = nullptr;
+    float* d_amps = nullptr;
+    float* d_dts = nullptr;
+    float* d_trace = nullptr;
+    float* d_tmp_out = nullptr;
+    size_t tmp_out_bytes = 0;
+    // stimulus / recording
+    int nt = 0, stim_node = 0;
+    float stim_scale = 0.f;
+    std::vector<int> rec_nodes;       // as given
+    std::vector<int> rec_cols;        // column of each given site
+    int n_rec_unique = 0, rec_every = 1, n_samples = 0;
+    float v_init = -65.f;
+    bool has_params = false, has_stim = false, initialized = false;
+};
+
+template <typename R>
+static SimArgs<R> make_args(ngpu_sim* s) {
+    SimArgs<R> A;
+    const ngpu_model* m = s->m;
+    A.info = s->d_info;
+    A.coef = (const NodeCoef<R>*)s->d_coef;
+    A.n_nodes = m->n;
+    A.slab = (R*)s->d_slab;
+    A.slab_rows = m->slab_rows;
+    A.ptab = s->d_ptab;
+    A.ptab_rows = m->ptab_rows;
+    A.scr = (R*)s->d_scr;
+    A.jacc = s->d_jacc;
+    A.jx = (R*)s->d_jx;
+    A.n_jslots = m->n_jslots;
+    A.amps = s->d_amps;
+    A.dts = s->d_dts;
+    A.nt = s->nt;
+    A.stim_node = s->stim_node;
+    A.stim_scale = s->stim_scale;
+    A.inst_stim = s->d_inst_stim;
+    A.trace = s->d_trace;
+    A.n_rec = s->n_rec_unique;
+    A.rec_every = s->rec_every;
+    A.n_inst_pad = s->n_pad;
+    A.v_init = s->v_init;
+    A.bad = s->d_bad;
+    return A;
+}
+
+template <typename R>
+static cudaError_t launch_init(ngpu_sim* s, cudaStream_t st) {
+    SimArgs<R> A = make_args<R>(s);
+    if (s->m->mechset == NGPU_MECHSET_TTPC) k_sim_init<R, 0><<<s->n_groups, kLanes, 0, st>>>(A);
+    else k_sim_init<R, 1><<<s->n_groups, kLanes, 0, st>>>(A);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_advance(ngpu_sim* s, int t0, int n, cudaStream_t st) {
+    SimArgs<R> A = make_args<R>(s);
+    if (s->m->mechset == NGPU_MECHSET_TTPC) k_sim_advance<R, 0><<<s->n_groups, kLanes, 0, st>>>(A, t0, n);
+    else k_sim_advance<R, 1><<<s->n_groups, kLanes, 0, st>>>(A, t0, n);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+extern "C" {
+
+const char* ngpu_last_error(void) { return g_err.c_str(); }
+int ngpu_abi_version(void) { return NGPU_ABI_VERSION; }
+int64_t ngpu_launch_count(int32_t reset) {
+    return reset ? g_launches.exchange(0) : g_launches.load();
+}
+
+int ngpu_mechset_info(int32_t mechset, int32_t* n_mech, int32_t* n_params) {
+    if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN)
+        return fail(NGPU_E_INVALID, "unknown mechanism set");
+    const SetDesc& sd = set_desc(mechset);
+    if (n_mech) *n_mech = (int32_t)sd.mechs.size();
+    if (n_params) *n_params = sd.n_params;
+    return NGPU_OK;
+}
+
+int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, const double* b,
+                      const double* cm, const int32_t* section, int32_t n_sections,
+                      int32_t mechset, const uint8_t* mech_mask, ngpu_model** out) {
+    if (!out) return fail(NGPU_E_INVALID, "out is null");
+    *out = nullptr;
+    if (n_nodes < 1 || !parent || !a || !b || !cm || !section || !mech_mask || n_sections < 1)
+        return fail(NGPU_E_INVALID, "model arrays missing or empty");
+    if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN)
+        return fail(NGPU_E_INVALID, "unknown mechanism set");
+    const SetDesc& sd = set_desc(mechset);
+    const int NM = (int)sd.mechs.size();
+    if (parent[0] != -1) return fail(NGPU_E_INVALID, "parent[0] must be -1 (node 0 is the root)");
+    for (int i = 1; i < n_nodes; ++i)
+        if (parent[i] < 0 || parent[i] >= i)
+            return fail(NGPU_E_INVALID, "parent[" + std::to_string(i) + "] = " +
+                                            std::to_string(parent[i]) +
+                                            " is not an earlier node (Hines order required)");
+    for (int i = 0; i < n_nodes; ++i) {
+        if (section[i] < 0 || section[i] >= n_sections)
+            return fail(NGPU_E_INVALID, "section index out of range at node " + std::to_string(i));
+        if (!std::isfinite(a[i]) || !std::isfinite(b[i]) || !std::isfinite(cm[i]) || cm[i] < 0)
+            return fail(NGPU_E_INVALID, "non-finite coefficient at node " + std::to_string(i));
+    }
+    ngpu_model* m = new (std::nothrow) ngpu_model();
+    if (!m) return fail(NGPU_E_NOMEM, "host allocation failed");
+    m->n = n_nodes;
+    m->n_sections = n_sections;
+    m->mechset = mechset;
+    m->n_mech = NM;
+    m->n_params = sd.n_params;
+    m->parent.assign(parent, parent + n_nodes);
+    m->section.assign(section, section + n_nodes);
+    m->a.assign(a, a + n_nodes);
+    m->b.assign(b, b + n_nodes);
+    m->cm.assign(cm, cm + n_nodes);
+    m->mask.assign(n_nodes, 0u);
+    for (int k = 0; k < NM; ++k)
+        for (int i = 0; i < n_nodes; ++i)
+            if (mech_mask[(size_t)k * n_nodes + i]) m->mask[i] |= (1u << k);
+    for (int i = 0; i < n_nodes; ++i) {
+        if ((m->mask[i] & sd.needs_ca_dyn) && !(m->mask[i] & sd.ca_dyn_bit)) {
+            delete m;
+            return fail(NGPU_E_INVALID, "node " + std::to_string(i) +
+                                            " has a calcium current without calcium dynamics "
+                                            "(its reversal potential would be infinite)");
+        }
+    }
+    // children bookkeeping: dconst and junction slots
+    m->dconst.assign(n_nodes, 0.0);
+    std::vector<int> has_far(n_nodes, 0);
+    for (int i = 0; i < n_nodes; ++i) m->dconst[i] = -m->a[i];
+    m->dconst[0] = 0.0;  // the root has no parent coupling
+    for (int i = 1; i < n_nodes; ++i) {
+        m->dconst[parent[i]] -= m->b[i];
+        if (parent[i] != i - 1) has_far[parent[i]] = 1;
+    }
+    std::vector<int> jslot(n_nodes, -1);
+    int nj = 0;
+    for (int i = 0; i < n_nodes; ++i)
+        if (has_far[i]) jslot[i] = nj++;
+    m->n_jslots = nj;
+    // state and parameter rows
+    std::map<std::pair<int, uint32_t>, int> prow_of;
+    m->info.resize(n_nodes);
+    int srow = 0;
+    for (int i = 0; i < n_nodes; ++i) {
+        NodeInfo& ni = m->info[i];
+        ni.parent = parent[i];
+        ni.mask = m->mask[i];
+        ni.srow = srow;
+        int srows = 0;
+        std::vector<int> plist;
+        for (int k = 0; k < NM; ++k)
+            if (ni.mask & (1u << k)) {
+                srows += sd.mechs[k].state_rows;
+                plist.insert(plist.end(), sd.mechs[k].params.begin(), sd.mechs[k].params.end());
+            }
+        srow += 2 + srows;
+        m->state_vars += srows;
+        m->param_reads += (int64_t)plist.size();
+        auto key = std::make_pair(section[i], ni.mask);
+        auto it = prow_of.find(key);
+        if (it == prow_of.end()) {
+            int first = (int)m->row_param.size();
+            for (int p : plist) {
+                m->row_param.push_back(p);
+                m->row_sec.push_back(section[i]);
+            }
+            it = prow_of.emplace(key, first).first;
+        }
+        ni.prow = it->second;
+        ni.jslot = jslot[i];
+        ni.pslot = (i > 0 && parent[i] != i - 1) ? jslot[parent[i]] : -1;
+        ni.rec = -1;
+        ni.pad = 0;
+    }
+    m->slab_rows = srow;
+    m->ptab_rows = std::max(1, (int)m->row_param.size());
+    if (m->row_param.empty()) {
+        m->row_param.push_back(0);
+        m->row_sec.push_back(0);
+    }
+    *out = m;
+    return NGPU_OK;
+}
+
+int ngpu_model_destroy(ngpu_model* m) {
+    delete m;
+    return NGPU_OK;
+}
+
+int ngpu_model_layout(const ngpu_model* m, int32_t* state_rows, int32_t* param_rows,
+                      int32_t* n_jslots, int64_t* state_vars, int64_t* param_reads) {
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    if (state_rows) *state_rows = m->slab_rows;
+    if (param_rows) *param_rows = m->ptab_rows;
+    if (n_jslots) *n_jslots = m->n_jslots;
+    if (state_vars) *state_vars = m->state_vars;
+    if (param_reads) *param_reads = m->param_reads;
+    return NGPU_OK;
+}
+
+static void sim_free(ngpu_sim* s) {
+    if (!s) return;
+    void* ptrs[] = {s->d_info, s->d_coef, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc,
+                    s->d_jx, s->d_inst_stim, s->d_bad, s->d_row_param, s->d_row_sec,
+                    s->d_amps, s->d_dts, s->d_trace, s->d_tmp_out};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete s;
+}
+
+int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision,
+                    ngpu_sim** out) {
+    if (!out) return fail(NGPU_E_INVALID, "out is null");
+    *out = nullptr;
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    if (n_sets < 1 || n_stim < 1) return fail(NGPU_E_INVALID, "need n_sets >= 1 and n_stim >= 1");
+    if (precision != NGPU_FP32 && precision != NGPU_FP64)
+        return fail(NGPU_E_INVALID, "precision must be NGPU_FP32 or NGPU_FP64");
+    if ((int64_t)n_sets * n_stim > (int64_t)1 << 30) return fail(NGPU_E_INVALID, "too many instances");
+    ngpu_sim* s = new (std::nothrow) ngpu_sim();
+    if (!s) return fail(NGPU_E_NOMEM, "host allocation failed");
+    s->m = m;
+    s->n_sets = n_sets;
+    s->n_stim = n_stim;
+    s->n_inst = n_sets * n_stim;
+    s->n_groups = (s->n_inst + kLanes - 1) / kLanes;
+    s->n_pad = s->n_groups * kLanes;
+    s->precision = precision;
+    const size_t esz = precision == NGPU_FP64 ? 8 : 4;
+    const size_t G = (size_t)s->n_groups, L = kLanes;
+    int rc = NGPU_OK;
+#define ALLOC(field, type, bytes)                              \
+    s->field = (type)dmalloc((bytes), &rc);                    \
+    if (!s->field) {                                           \
+        sim_free(s);                                           \
+        return rc;                                             \
+    }
+    ALLOC(d_info, NodeInfo*, sizeof(NodeInfo) * m->n);
+    ALLOC(d_coef, void*, 4 * esz * m->n);
+    ALLOC(d_slab, void*, G * m->slab_rows * L * esz);
+    ALLOC(d_ptab, float*, G * m->ptab_rows * L * sizeof(float));
+    ALLOC(d_scr, void*, G * 2 * m->n * L * esz);
+    ALLOC(d_jacc, double*, G * 2 * std::max(1, m->n_jslots) * L * sizeof(double));
+    ALLOC(d_jx, void*, G * 2 * std::max(1, m->n_jslots) * L * esz);
+    ALLOC(d_inst_stim, int*, sizeof(int) * s->n_pad);
+    ALLOC(d_bad, int*, sizeof(int) * s->n_pad);
+    ALLOC(d_row_param, int*, sizeof(int) * m->row_param.size());
+    ALLOC(d_row_sec, int*, sizeof(int) * m->row_sec.size());
+#undef ALLOC
+    // coefficients in the run's precision
+    if (precision == NGPU_FP64) {
+        std::vector<NodeCoef<double>> c(m->n);
+        for (int i = 0; i < m->n; ++i) c[i] = {m->a[i], m->b[i], m->dconst[i], m->cm[i] / 1000.0};
+        cudaMemcpy(s->d_coef, c.data(), sizeof(NodeCoef<double>) * m->n, cudaMemcpyHostToDevice);
+    } else {
+        std::vector<NodeCoef<float>> c(m->n);
+        for (int i = 0; i < m->n; ++i)
+            c[i] = {(float)m->a[i], (float)m->b[i], (float)m->dconst[i], (float)(m->cm[i] / 1000.0)};
+        cudaMemcpy(s->d_coef, c.data(), sizeof(NodeCoef<float>) * m->n, cudaMemcpyHostToDevice);
+    }
+    std::vector<int> inst_stim(s->n_pad);
+    for (int k = 0; k < s->n_pad; ++k) inst_stim[k] = std::min(k, s->n_inst - 1) % n_stim;
+    cudaMemcpy(s->d_inst_stim, inst_stim.data(), sizeof(int) * s->n_pad, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->d_row_param, m->row_param.data(), sizeof(int) * m->row_param.size(),
+               cudaMemcpyHostToDevice);
+    cudaMemcpy(s->d_row_sec, m->row_sec.data(), sizeof(int) * m->row_sec.size(),
+               cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemset(s->d_bad, 0, sizeof(int) * s->n_pad);
+    if (e != cudaSuccess) {
+        sim_free(s);
+        return fail(NGPU_E_CUDA, std::string("sim create: ") + cudaGetErrorString(e));
+    }
+    // default recording: the root, every step
+    s->rec_nodes = {0};
+    s->rec_cols = {0};
+    s->n_rec_unique = 1;
+    *out = s;
+    return NGPU_OK;
+}
+
+int ngpu_sim_destroy(ngpu_sim* s) {
+    sim_free(s);
+    return NGPU_OK;
+}
+
+int ngpu_sim_set_params(ngpu_sim* s, const float* params, int32_t on_device) {
+    if (!s || !params) return fail(NGPU_E_INVALID, "null sim or params");
+    const ngpu_model* m = s->m;
+    const size_t n = (size_t)s->n_sets * m->n_params * m->n_sections;
+    const float* src = params;
+    float* tmp = nullptr;
+    if (!on_device) {
+        int rc = NGPU_OK;
+        tmp = (float*)dmalloc(n * sizeof(float), &rc);
+        if (!tmp) return rc;
+        cudaError_t e = cudaMemcpy(tmp, params, n * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(tmp);
+            return fail(NGPU_E_CUDA, std::string("params upload: ") + cudaGetErrorString(e));
+        }
+        src = tmp;
+    }
+    const size_t total = (size_t)s->n_groups * m->ptab_rows * kLanes;
+    int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    k_gather_params<<<blocks, 256>>>(src, s->d_row_param, s->d_row_sec, m->ptab_rows, m->n_params,
+                                     m->n_sections, s->n_stim, s->n_inst, s->n_groups, s->d_ptab);
+    g_launches++;
+    cudaError_t e = cudaGetLastError();
+    if (tmp) {
+        cudaError_t e2 = cudaDeviceSynchronize();
+        cudaFree(tmp);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("param gather: ") + cudaGetErrorString(e));
+    s->has_params = true;
+    return NGPU_OK;
+}
+
+int ngpu_sim_set_stimulus(ngpu_sim* s, int32_t nt, const float* amps, const float* dts,
+                          int32_t stim_node, float stim_area_um2, int32_t on_device) {
+    if (!s || !amps || !dts) return fail(NGPU_E_INVALID, "null sim or stimulus arrays");
+    if (nt < 1) return fail(NGPU_E_INVALID, "nt must be >= 1");
+    if (stim_node < 0 || stim_node >= s->m->n) return fail(NGPU_E_INVALID, "stim_node out of range");
+    if (!(stim_area_um2 > 0.f) || !std::isfinite(stim_area_um2))
+        return fail(NGPU_E_INVALID, "stimulus area must be positive");
+    if (!on_device) {
+        for (int t = 0; t < nt; ++t)
+            if (!(dts[t] > 0.f) || !std::isfinite(dts[t]))
+                return fail(NGPU_E_INVALID, "dt must be positive and finite at step " + std::to_string(t));
+    }
+    if (s->d_amps) cudaFree(s->d_amps);
+    if (s->d_dts) cudaFree(s->d_dts);
+    s->d_amps = nullptr;
+    s->d_dts = nullptr;
+    int rc = NGPU_OK;
+    s->d_amps = (float*)dmalloc(sizeof(float) * (size_t)nt * s->n_stim, &rc);
+    if (!s->d_amps) return rc;
+    s->d_dts = (float*)dmalloc(sizeof(float) * (size_t)nt, &rc);
+    if (!s->d_dts) return rc;
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    NGPU_CUDA(cudaMemcpy(s->d_amps, amps, sizeof(float) * (size_t)nt * s->n_stim, kind));
+    NGPU_CUDA(cudaMemcpy(s->d_dts, dts, sizeof(float) * (size_t)nt, kind));
+    s->nt = nt;
+    s->stim_node = stim_node;
+    s->stim_scale = 100.0f / stim_area_um2;
+    s->has_stim = true;
+    s->initialized = false;
+    return NGPU_OK;
+}
+
+int ngpu_sim_set_recording(ngpu_sim* s, int32_t n_rec, const int32_t* rec_nodes, int32_t rec_every) {
+    if (!s) return fail(NGPU_E_INVALID, "null sim");
+    if (n_rec < 1 || !rec_nodes) return fail(NGPU_E_INVALID, "need at least one recording site");
+    if (rec_every < 1) return fail(NGPU_E_INVALID, "rec_every must be >= 1");
+    std::vector<int> uniq;
+    std::vector<int> cols(n_rec);
+    for (int r = 0; r < n_rec; ++r) {
+        if (rec_nodes[r] < 0 || rec_nodes[r] >= s->m->n)
+            return fail(NGPU_E_INVALID, "recording node out of range");
+        auto it = std::find(uniq.begin(), uniq.end(), rec_nodes[r]);
+        if (it == uniq.end()) {
+            cols[r] = (int)uniq.size();
+            uniq.push_back(rec_nodes[r]);
+        } else {
+            cols[r] = (int)(it - uniq.begin());
+        }
+    }
+    s->rec_nodes.assign(rec_nodes, rec_nodes + n_rec);
+    s->rec_cols = cols;
+    s->n_rec_unique = (int)uniq.size();
+    s->rec_every = rec_every;
+    s->initialized = false;
+    return NGPU_OK;
+}
+
+int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
+    if (!s) return fail(NGPU_E_INVALID, "null sim");
+    if (!s->has_params) return fail(NGPU_E_STATE, "set_params must precede init");
+    if (!s->has_stim) return fail(NGPU_E_STATE, "set_stimulus must precede init");
+    if (!std::isfinite(v_init)) return fail(NGPU_E_INVALID, "v_init must be finite");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const ngpu_model* m = s->m;
+    // node table with this run's recording columns
+    std::vector<NodeInfo> info = m->info;
+    std::vector<int> uniq(s->n_rec_unique, -1);
+    for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
+    for (int c = 0; c < s->n_rec_unique; ++c) info[uniq[c]].rec = c;
+    NGPU_CUDA(cudaMemcpyAsync(s->d_info, info.data(), sizeof(NodeInfo) * m->n, cudaMemcpyHostToDevice, st));
+    s->n_samples = (s->nt + s->rec_every - 1) / s->rec_every;
+    if (s->d_trace) cudaFree(s->d_trace);
+    s->d_trace = nullptr;
+    int rc = NGPU_OK;
+    s->d_trace = (float*)dmalloc(sizeof(float) * (size_t)s->n_samples * s->n_rec_unique * s->n_pad, &rc);
+    if (!s->d_trace) return rc;
+    NGPU_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(int) * s->n_pad, st));
+    s->v_init = v_init;
+    cudaError_t e = s->precision == NGPU_FP64 ? launch_init<double>(s, st) : launch_init<float>(s, st);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("init launch: ") + cudaGetErrorString(e));
+    s->initialized = true;
+    return NGPU_OK;
+}
+
+int ngpu_sim_advance(ngpu_sim* s, int32_t t0, int32_t n_steps, void* cuda_stream) {
+    if (!s) return fail(NGPU_E_INVALID, "null sim");
+    if (!s->initialized) return fail(NGPU_E_STATE, "init must precede advance");
+    if (t0 < 0 || n_steps < 0 || (int64_t)t0 + n_steps > s->nt)
+        return fail(NGPU_E_INVALID, "step range outside the stimulus");
+    if (n_steps == 0) return NGPU_OK;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    cudaError_t e = s->precision == NGPU_FP64 ? launch_advance<double>(s, t0, n_steps, st)
+                                              : launch_advance<float>(s, t0, n_steps, st);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("advance launch: ") + cudaGetErrorString(e));
+    return NGPU_OK;
+}
+
+int ngpu_sim_n_samples(const ngpu_sim* s) { return s ? s->n_samples : 0; }
+
+int ngpu_sim_trace_device(ngpu_sim* s, const float** trace, int32_t* n_inst_padded) {
+    if (!s || !trace) return fail(NGPU_E_INVALID, "null argument");
+    *trace = s->d_trace;
+    if (n_inst_padded) *n_inst_padded = s->n_pad;
+    return NGPU_OK;
+}
+
+int ngpu_sim_get_trace(ngpu_sim* s, float* out, int32_t on_device, void* cuda_stream) {
+    if (!s || !out) return fail(NGPU_E_INVALID, "null sim or out");
+    if (!s->initialized) return fail(NGPU_E_STATE, "no run to read");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const int nr = s->n_rec_unique, ns = s->n_samples;
+    const size_t per_inst_u = (size_t)nr * ns;
+    const size_t bytes_u = sizeof(float) * per_inst_u * s->n_inst;
+    if (s->tmp_out_bytes < bytes_u) {
+        if (s->d_tmp_out) cudaFree(s->d_tmp_out);
+        s->d_tmp_out = nullptr;
+        s->tmp_out_bytes = 0;
+        int rc = NGPU_OK;
+        s->d_tmp_out = (float*)dmalloc(bytes_u, &rc);
+        if (!s->d_tmp_out) return rc;
+        s->tmp_out_bytes = bytes_u;
+    }
+    dim3 grid((s->n_pad + 31) / 32, (ns + 31) / 32, nr), block(32, 8);
+    k_trace_transpose<<<grid, block, 0, st>>>(s->d_trace, ns, nr, s->n_pad, s->n_inst, s->d_tmp_out);
+    g_launches++;
+    NGPU_CUDA(cudaGetLastError());
+    const int n_rec = (int)s->rec_nodes.size();
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    bool identity = (n_rec == nr);
+    for (int r = 0; r < n_rec && identity; ++r) identity = s->rec_cols[r] == r;
+    if (identity) {
+        NGPU_CUDA(cudaMemcpyAsync(out, s->d_tmp_out, bytes_u, kind, st));
+    } else {
+        // duplicated sites: strided copies of each requested column
+        for (int r = 0; r < n_rec; ++r) {
+            NGPU_CUDA(cudaMemcpy2DAsync(out + (size_t)r * ns, sizeof(float) * n_rec * ns,
+                                        s->d_tmp_out + (size_t)s->rec_cols[r] * ns, sizeof(float) * per_inst_u,
+                                        sizeof(float) * ns, s->n_inst, kind, st));
+        }
+    }
+    NGPU_CUDA(cudaStreamSynchronize(st));
+    return NGPU_OK;
+}
+
+int ngpu_sim_check(ngpu_sim* s, int32_t* n_bad, void* cuda_stream) {
+    if (!s || !n_bad) return fail(NGPU_E_INVALID, "null argument");
+    std::vector<int> bad(s->n_pad);
+    NGPU_CUDA(cudaMemcpyAsync(bad.data(), s->d_bad, sizeof(int) * s->n_pad, cudaMemcpyDeviceToHost,
+                              (cudaStream_t)cuda_stream));
+    NGPU_CUDA(cudaStreamSynchronize((cudaStream_t)cuda_stream));
+    int c = 0;
+    for (int i = 0; i < s->n_inst; ++i) c += bad[i] != 0;
+    *n_bad = c;
+    return NGPU_OK;
+}
+
+int ngpu_run(ngpu_model* m, int32_t n_sets, const float* params, int32_t n_stim, int32_t nt,
+             const float* amps, const float* dts, int32_t stim_node, float stim_area_um2,
+             int32_t n_rec, const int32_t* rec_nodes, float v_init, int32_t precision, float* out) {
+    if (!out) return fail(NGPU_E_INVALID, "out is null");
+    ngpu_sim* s = nullptr;
+    int rc = ngpu_sim_create(m, n_sets, n_stim, precision, &s);
+    if (rc) return rc;
+    if ((rc = ngpu_sim_set_params(s, params, 0)) ||
+        (rc = ngpu_sim_set_stimulus(s, nt, amps, dts, stim_node, stim_area_um2, 0)) ||
+        (rc = ngpu_sim_set_recording(s, n_rec, rec_nodes, 1)) || (rc = ngpu_sim_init(s, v_init, nullptr)) ||
+        (rc = ngpu_sim_advance(s, 0, nt, nullptr)) || (rc = ngpu_sim_get_trace(s, out, 0, nullptr))) {
+        std::string msg = g_err;
+        sim_free(s);
+        g_err = msg;
+        return rc;
+    }
+    int32_t nbad = 0;
+    rc = ngpu_sim_check(s, &nbad, nullptr);
+    sim_free(s);
+    if (rc) return rc;
+    if (nbad) return fail(NGPU_E_NUMERIC, std::to_string(nbad) + " instance(s) produced non-finite voltage");
+    return NGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// Precision policy for the simulation kernels.
+//
+// The production build computes gates, currents and the Hines solve in FP32
+// (the GPU's fast SFU paths: ex2 / lg2 / rcp), keeps membrane voltage as a
+// Kahan-compensated FP32 pair, and accumulates junction sums in FP64.  The
+// FP64 build of the same kernel template is the GPU-side oracle run and uses
+// the correctly rounded double-precision library functions throughout.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ngpu {
+
+template <typename R> struct Math;
+
+template <> struct Math<float> {
+    static __device__ __forceinline__ float ex(float x) { return __expf(x); }
+    static __device__ __forceinline__ float lg(float x) { return __logf(x); }
+    static __device__ __forceinline__ float dv(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float rc(float a) { return __fdividef(1.0f, a); }
+    static __device__ __forceinline__ float pw(float a, float b) { return __powf(a, b); }
+    // 1 - exp(-z) for z >= 0 without the cancellation 1 - exp(-z) suffers in
+    // FP32 when z = dt/tau is small (slow gates, Ca decay): below z = 1/32 the
+    // alternating Taylor series z - z^2/2 + z^3/6 - z^4/24 has truncation
+    // error < z^5/120 < 3e-10 relative.
+    static __device__ __forceinline__ float one_minus_exp_neg(float z) {
+        if (z < 0.03125f) {
+            return z * (1.0f - z * (0.5f - z * (0.16666667f - z * 0.041666668f)));
+        }
+        return 1.0f - __expf(-z);
+    }
+};
+
+template <> struct Math<double> {
+    static __device__ __forceinline__ double ex(double x) { return exp(x); }
+    static __device__ __forceinline__ double lg(double x) { return log(x); }
+    static __device__ __forceinline__ double dv(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double rc(double a) { return 1.0 / a; }
+    static __device__ __forceinline__ double pw(double a, double b) { return pow(a, b); }
+    static __device__ __forceinline__ double one_minus_exp_neg(double z) { return -expm1(-z); }
+};
+
+// cnexp update of a first-order gate: x += (1 - exp(-dt/tau)) (xinf - x).
+template <typename R>
+__device__ __forceinline__ R cnexp(R x, R xinf, R tau, R dt) {
+    return x + Math<R>::one_minus_exp_neg(Math<R>::dv(dt, tau)) * (xinf - x);
+}
+
+// Physical constants shared by the generated channel libraries.
+constexpr double kFaraday = 96485.309;
+constexpr double kDefCai = 5.e-5;
+constexpr double kDefCao = 2.;
+__host__ __device__ constexpr double ktf_of(double celsius) {
+    return 1000. * 8.3134 * (celsius + 273.15) / kFaraday;
+}
+
+}  // namespace ngpu

@@ -1,0 +1,165 @@
+"""Python front end of the simulation core (a thin layer over include/ngpu.h).
+
+``run`` is the drop-in for one reference ``neuroGPU`` process
+(GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/kernel.cu:8-33 -> RunByModelP ->
+stEfork2Main, src/CudaStuff.cu:518-587): parameters, stimuli and recording
+sites in, voltage traces out, with the reference's array layouts.
+``Simulator`` keeps the simulation resident on the GPU between calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _ffi
+from .model import CellModel, to_ffi_model
+
+_PREC = {"fp32": _ffi.NGPU_FP32, "fp64": _ffi.NGPU_FP64}
+
+
+def _stream_ptr(stream) -> C.c_void_p | None:
+    if stream is None:
+        return None
+    h = getattr(stream, "cuda_stream", stream)
+    return C.c_void_p(int(h))
+
+
+def _as_f32(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+
+
+class Model:
+    """libngpu model handle for a :class:`CellModel`."""
+
+    def __init__(self, cell: CellModel):
+        self.cell = cell
+        self._h = to_ffi_model(cell)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def layout(self) -> dict:
+        L = _ffi.lib()
+        sr, pr, nj = C.c_int32(), C.c_int32(), C.c_int32()
+        sv, prd = C.c_int64(), C.c_int64()
+        _ffi.check("ngpu_model_layout", L.ngpu_model_layout(self._h, C.byref(sr), C.byref(pr),
+                                                            C.byref(nj), C.byref(sv), C.byref(prd)))
+        return {"state_rows": sr.value, "param_rows": pr.value, "n_jslots": nj.value,
+                "state_vars": sv.value, "param_reads": prd.value}
+
+    def close(self) -> None:
+        if self._h:
+            _ffi.lib().ngpu_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Simulator:
+    """Resident simulation of n_sets x n_stim instances of one model."""
+
+    def __init__(self, model: Model | CellModel, n_sets: int, n_stim: int, precision: str = "fp32"):
+        self.model = model if isinstance(model, Model) else Model(model)
+        self.n_sets, self.n_stim = int(n_sets), int(n_stim)
+        self.precision = precision
+        h = C.c_void_p()
+        _ffi.check("ngpu_sim_create", _ffi.lib().ngpu_sim_create(
+            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], C.byref(h)))
+        self._h = h
+        self.nt = 0
+        self.n_rec = 1
+
+    def set_params(self, params) -> None:
+        """params [n_sets, n_params, n_sections]: numpy (host) or a CUDA tensor."""
+        L = _ffi.lib()
+        if hasattr(params, "is_cuda") and params.is_cuda:
+            t = params.contiguous().float()
+            _ffi.check("ngpu_sim_set_params", L.ngpu_sim_set_params(self._h, C.c_void_p(t.data_ptr()), 1))
+            self._keep = t
+        else:
+            p = _as_f32(params)
+            cell = self.model.cell
+            exp = (self.n_sets, cell.n_params(), cell.n_sections)
+            if p.shape != exp:
+                raise ValueError(f"params shape {p.shape} != {exp}")
+            _ffi.check("ngpu_sim_set_params", L.ngpu_sim_set_params(self._h, _ffi.ptr(p), 0))
+
+    def set_stimulus(self, amps, dts, stim_node: int, stim_area_um2: float) -> None:
+        a = _as_f32(amps)
+        if a.ndim != 2 or a.shape[0] != self.n_stim:
+            raise ValueError("amps must be [n_stim, nt]")
+        nt = a.shape[1]
+        d = _as_f32(np.broadcast_to(np.asarray(dts, dtype=np.float32), (nt,)))
+        _ffi.check("ngpu_sim_set_stimulus", _ffi.lib().ngpu_sim_set_stimulus(
+            self._h, nt, _ffi.ptr(a), _ffi.ptr(d), int(stim_node), float(stim_area_um2), 0))
+        self.nt = nt
+
+    def set_recording(self, rec_nodes, rec_every: int = 1) -> None:
+        r = np.ascontiguousarray(np.asarray(rec_nodes, dtype=np.int32).reshape(-1))
+        _ffi.check("ngpu_sim_set_recording", _ffi.lib().ngpu_sim_set_recording(
+            self._h, r.size, _ffi.ptr(r), int(rec_every)))
+        self.n_rec = int(r.size)
+
+    def init(self, v_init: float, stream=None) -> None:
+        _ffi.check("ngpu_sim_init", _ffi.lib().ngpu_sim_init(self._h, float(v_init), _stream_ptr(stream)))
+
+    def advance(self, t0: int, n_steps: int, stream=None) -> None:
+        _ffi.check("ngpu_sim_advance", _ffi.lib().ngpu_sim_advance(
+            self._h, int(t0), int(n_steps), _stream_ptr(stream)))
+
+    @property
+    def n_samples(self) -> int:
+        return int(_ffi.lib().ngpu_sim_n_samples(self._h))
+
+    def trace(self, stream=None) -> np.ndarray:
+        out = np.empty((self.n_sets, self.n_stim, self.n_rec, self.n_samples), dtype=np.float32)
+        _ffi.check("ngpu_sim_get_trace", _ffi.lib().ngpu_sim_get_trace(
+            self._h, _ffi.ptr(out), 0, _stream_ptr(stream)))
+        return out
+
+    def trace_into(self, dev_ptr: int, stream=None) -> None:
+        """Write the trace [n_sets, n_stim, n_rec, n_samples] to device memory."""
+        _ffi.check("ngpu_sim_get_trace", _ffi.lib().ngpu_sim_get_trace(
+            self._h, C.c_void_p(dev_ptr), 1, _stream_ptr(stream)))
+
+    def n_bad(self, stream=None) -> int:
+        n = C.c_int32()
+        _ffi.check("ngpu_sim_check", _ffi.lib().ngpu_sim_check(self._h, C.byref(n), _stream_ptr(stream)))
+        return n.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _ffi.lib().ngpu_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run(cell: CellModel | Model, params, amps, dts, stim_node: int, stim_area_um2: float,
+        rec_nodes, v_init: float, precision: str = "fp32") -> np.ndarray:
+    """One complete simulation from host arrays through ``ngpu_run``.
+
+    params [n_sets, n_params, n_sections]; amps [n_stim, nt] nA; dts [nt] ms.
+    Returns V [n_sets, n_stim, n_rec, nt] (V before each step's update)."""
+    model = cell if isinstance(cell, Model) else Model(cell)
+    p = _as_f32(params)
+    a = _as_f32(amps)
+    nt = a.shape[1]
+    d = _as_f32(np.broadcast_to(np.asarray(dts, dtype=np.float32), (nt,)))
+    r = np.ascontiguousarray(np.asarray(rec_nodes, dtype=np.int32).reshape(-1))
+    out = np.empty((p.shape[0], a.shape[0], r.size, nt), dtype=np.float32)
+    _ffi.check("ngpu_run", _ffi.lib().ngpu_run(
+        model.handle, p.shape[0], _ffi.ptr(p), a.shape[0], nt, _ffi.ptr(a), _ffi.ptr(d),
+        int(stim_node), float(stim_area_um2), r.size, _ffi.ptr(r), float(v_init),
+        _PREC[precision], _ffi.ptr(out)))
+    return out

@@ -1,0 +1,136 @@
+"""GPU parity: the CUDA simulation (through the C ABI) against the CPU oracle.
+
+Tolerances (stated by the north-star target):
+  * FP64 kernel vs FP64 oracle: max |dV| <= 1e-5 mV (same algorithm, both
+    double; the kernel uses the analytic conductance where the oracle uses
+    the reference's finite difference, equal to ~1e-10 relative; the bound
+    is the rounding of the float32 trace output, ulp(100 mV)/2 = 3.8e-6);
+  * FP32 kernel vs FP64 oracle: max |dV| <= 0.1 mV and spike-time error
+    <= 0.05 ms.
+"""
+import numpy as np
+import pytest
+
+from helpers import spike_time_error
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64_MV = 1e-5
+TOL_FP32_MV = 0.1
+TOL_SPIKE_MS = 0.05
+
+
+def _gpu_run(w, precision, chunks=None):
+    from neurogpu_b200.sim import Simulator
+    sim = Simulator(w.cell, w.n_sets, w.n_stim, precision)
+    sim.set_params(w.params)
+    sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+    sim.set_recording(w.rec_nodes)
+    sim.init(w.v_init)
+    if chunks is None:
+        sim.advance(0, w.nt)
+    else:
+        t = 0
+        for c in chunks:
+            sim.advance(t, c)
+            t += c
+        assert t == w.nt
+    out = sim.trace()
+    assert sim.n_bad() == 0
+    sim.close()
+    return out
+
+
+@pytest.fixture(scope="module")
+def cfg():
+    from neurogpu_b200 import configs
+    return {
+        "passive": configs.passive_cable(),
+        "hh": configs.hh_active(n_sets=24, t_stop=150.0),
+        "ttpc": configs.ttpc_like(n_sets=12, t_stop=200.0),
+    }
+
+
+@pytest.fixture(scope="module")
+def refs(oracle, cfg):
+    return {k: oracle.run_workload(w) for k, w in cfg.items()}
+
+
+@pytest.mark.parametrize("name", ["passive", "hh", "ttpc"])
+def test_fp64_matches_oracle(ngpu_built, refs, cfg, name):
+    w = cfg[name]
+    ref = refs[name]
+    got = _gpu_run(w, "fp64")
+    assert got.shape == ref.shape
+    err = np.max(np.abs(got.astype(np.float64) - ref))
+    assert err <= TOL_FP64_MV, f"{name}: FP64 max|dV| = {err:.3e} mV"
+
+
+@pytest.mark.parametrize("name", ["passive", "hh", "ttpc"])
+def test_fp32_matches_oracle(ngpu_built, refs, cfg, name):
+    w = cfg[name]
+    ref = refs[name]
+    got = _gpu_run(w, "fp32").astype(np.float64)
+    err = np.max(np.abs(got - ref))
+    st, mism = spike_time_error(got, ref, w.dt)
+    print(f"{name}: FP32 max|dV| = {err:.4e} mV, spike-time err = {st:.4e} ms, count mismatches = {mism}")
+    assert mism == 0
+    assert st <= TOL_SPIKE_MS
+    assert err <= TOL_FP32_MV, f"{name}: FP32 max|dV| = {err:.3e} mV"
+
+
+def test_chunked_advance_is_bitwise_identical(ngpu_built, cfg):
+    w = cfg["hh"]
+    a = _gpu_run(w, "fp32")
+    b = _gpu_run(w, "fp32", chunks=[1, 999, 2000, w.nt - 3000])
+    assert np.array_equal(a, b)
+
+
+def test_run_twice_deterministic(ngpu_built, cfg):
+    w = cfg["ttpc"]
+    assert np.array_equal(_gpu_run(w, "fp32"), _gpu_run(w, "fp32"))
+
+
+def test_host_entry_point_matches_resident_sim(ngpu_built, cfg):
+    from neurogpu_b200.sim import run
+    w = cfg["hh"]
+    out = run(w.cell, w.params, w.amps, w.dts, w.stim_node, w.stim_area, w.rec_nodes, w.v_init)
+    assert np.array_equal(out, _gpu_run(w, "fp32"))
+
+
+def test_ragged_instances_recording_and_cadence(ngpu_built, oracle, cfg):
+    """5 sets x 3 stimuli (15 instances, half a warp), duplicated and
+    multiple recording sites, recording every 7th step."""
+    from neurogpu_b200.sim import Simulator
+    w = cfg["hh"].subset(n_sets=5, nt=1001)
+    rec = np.array([0, 17, w.cell.n_nodes - 1, 17], dtype=np.int32)
+    w.rec_nodes = rec
+    ref = oracle.run_workload(w)
+    sim = Simulator(w.cell, w.n_sets, w.n_stim, "fp64")
+    sim.set_params(w.params)
+    sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+    sim.set_recording(rec, rec_every=7)
+    sim.init(w.v_init)
+    sim.advance(0, w.nt)
+    got = sim.trace()
+    sim.close()
+    assert got.shape == (5, 3, 4, (1001 + 6) // 7)
+    np.testing.assert_allclose(got, ref[..., ::7], atol=TOL_FP64_MV, rtol=0)
+
+
+def test_single_step_and_single_instance(ngpu_built, oracle, cfg):
+    w = cfg["ttpc"].subset(n_sets=1, n_stim=1, nt=1)
+    ref = oracle.run_workload(w)
+    got = _gpu_run(w, "fp64")
+    np.testing.assert_allclose(got, ref, atol=TOL_FP64_MV, rtol=0)
+
+
+def test_nonfinite_parameters_are_reported(ngpu_built, cfg):
+    from neurogpu_b200._ffi import NgpuError
+    from neurogpu_b200.sim import run
+    w = cfg["passive"].subset(n_sets=3, nt=50)
+    p = w.params.copy()
+    p[1, :, :] = np.nan
+    with pytest.raises(NgpuError) as ei:
+        run(w.cell, p, w.amps, w.dts, w.stim_node, w.stim_area, w.rec_nodes, w.v_init)
+    assert ei.value.code == -5  # NGPU_E_NUMERIC
