@@ -71,6 +71,13 @@ int ngpu_model_destroy(ngpu_model *m);
 int ngpu_model_layout(const ngpu_model *m, int32_t *state_rows, int32_t *param_rows,
                       int32_t *n_jslots, int64_t *state_vars, int64_t *param_reads);
 
+/* Introspection of the tree split used by a CTA of n_warps warps: per node,
+ * top_flag (1 = top tree, solved by warp 0), owner (warp of its subtree, -1
+ * for top nodes), junction slot and parent junction slot.  Any pointer may
+ * be NULL. */
+int ngpu_model_partition(const ngpu_model *m, int32_t n_warps, int32_t *top_flag, int32_t *owner,
+                         int32_t *jslot, int32_t *pslot, int32_t *n_jslots);
+
 /*
  * One complete run from host buffers (the drop-in for one neuroGPU process).
  * Replaces callKernel + stEfork2Main (U/CudaStuff.cu:443-587).

@@ -43,6 +43,10 @@ class Workload:
     seed: int = 0
     info: dict = field(default_factory=dict)
 
+    def __post_init__(self):
+        # the C ABI (and the reference's Stim_meta.csv reader) carries the area as float32
+        self.stim_area = float(np.float32(self.stim_area))
+
     @property
     def n_sets(self) -> int:
         return int(self.params.shape[0])

@@ -32,7 +32,7 @@ struct Mainen {
 };
 
 template <typename R, bool INIT>
-__device__ __forceinline__ void mainen_node(uint32_t mk, R v, R dt, R* __restrict__ st,
+NGPU_HD void mainen_node(uint32_t mk, R v, R dt, R* __restrict__ st,
                                             const float* __restrict__ pr, R& I, R& G) {
     using M = Math<R>;
     constexpr int S = 32;

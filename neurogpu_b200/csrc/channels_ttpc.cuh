@@ -7,7 +7,8 @@
 // per-mechanism state lists of its CALL_TO_* expansion (CudaStuff.cu:220,
 // 264, 325).  Rewritten for the GPU:
 //   * alpha/beta rates use efun(z) = z/(e^z - 1) with a series near z = 0
-//     in place of the reference's exact-equality singularity nudges;
+//     (the reference's exact-equality nudges v += 1e-4 at the singular
+//     voltages are kept, so results agree at those points too);
 //   * dt/tau is formed as dt*(alpha+beta)*qt, so one reciprocal per gate;
 //   * the membrane conductance is the analytic dI/dv = sum of channel
 //     conductances (every channel here is ohmic), which equals the
@@ -41,25 +42,25 @@ struct TTPC {
 
 // z/(e^z - 1), with the series 1 - z/2 + z^2/12 near 0.
 template <typename R>
-__device__ __forceinline__ R efun(R z) {
+NGPU_HD R efun(R z) {
     if (fabs(z) < (R)1e-2) return (R)1 - z * ((R)0.5 - z * (R)(1.0 / 12.0));
     return Math<R>::dv(z, Math<R>::ex(z) - (R)1);
 }
 // 1/(1 + e^z)
 template <typename R>
-__device__ __forceinline__ R sigm(R z) {
+NGPU_HD R sigm(R z) {
     return Math<R>::rc((R)1 + Math<R>::ex(z));
 }
 // Gate with alpha/beta rates: returns xinf, sets *rate = qt*(alpha+beta) = 1/tau.
 template <typename R>
-__device__ __forceinline__ R ab_gate(R a, R b, R qt, R* rate) {
+NGPU_HD R ab_gate(R a, R b, R qt, R* rate) {
     R s = a + b;
     *rate = qt * s;
     return Math<R>::dv(a, s);
 }
 // cnexp given 1/tau.
 template <typename R>
-__device__ __forceinline__ R cnexp_rate(R x, R xinf, R rate, R dt) {
+NGPU_HD R cnexp_rate(R x, R xinf, R rate, R dt) {
     return x + Math<R>::one_minus_exp_neg(dt * rate) * (xinf - x);
 }
 
@@ -68,7 +69,8 @@ struct TTPCRates {
     using M = Math<R>;
     static constexpr R qt = (R)TTPC::kQt;
     // AllModels.cu:66-78
-    static __device__ __forceinline__ void ca_hva(R v, R& mi, R& mr, R& hi, R& hr) {
+    static NGPU_HD void ca_hva(R v, R& mi, R& mr, R& hi, R& hr) {
+        if (v == (R)-27.0) v = v + (R)0.0001;
         R ma = (R)(0.055 * 3.8) * efun((-(R)27 - v) * (R)(1.0 / 3.8));
         R mb = (R)0.94 * M::ex((-(R)75 - v) * (R)(1.0 / 17.0));
         mi = ab_gate(ma, mb, (R)1, &mr);
@@ -77,7 +79,7 @@ struct TTPCRates {
         hi = ab_gate(ha, hb, (R)1, &hr);
     }
     // AllModels.cu:79-88
-    static __device__ __forceinline__ void ca_lva(R v, R& mi, R& mr, R& hi, R& hr) {
+    static NGPU_HD void ca_lva(R v, R& mi, R& mr, R& hi, R& hr) {
         v = v + (R)10;
         mi = sigm((v + (R)30) * (R)(-1.0 / 6.0));
         mr = qt * M::rc((R)5 + (R)20 * sigm((v + (R)25) * (R)(1.0 / 5.0)));
@@ -85,19 +87,20 @@ struct TTPCRates {
         hr = qt * M::rc((R)20 + (R)50 * sigm((v + (R)40) * (R)(1.0 / 7.0)));
     }
     // AllModels.cu:89-97
-    static __device__ __forceinline__ void ih(R v, R& mi, R& mr) {
+    static NGPU_HD void ih(R v, R& mi, R& mr) {
+        if (v == (R)-154.9) v = v + (R)0.0001;
         R ma = (R)(0.001 * 6.43 * 11.9) * efun((v + (R)154.9) * (R)(1.0 / 11.9));
         R mb = (R)(0.001 * 193.0) * M::ex(v * (R)(1.0 / 33.1));
         mi = ab_gate(ma, mb, (R)1, &mr);
     }
     // AllModels.cu:98-105
-    static __device__ __forceinline__ void im(R v, R& mi, R& mr) {
+    static NGPU_HD void im(R v, R& mi, R& mr) {
         R ma = (R)3.3e-3 * M::ex((R)(2.5 * 0.04) * (v + (R)35));
         R mb = (R)3.3e-3 * M::ex((R)(-2.5 * 0.04) * (v + (R)35));
         mi = ab_gate(ma, mb, qt, &mr);
     }
     // AllModels.cu:106-120
-    static __device__ __forceinline__ void k_pst(R v, R& mi, R& mr, R& hi, R& hr) {
+    static NGPU_HD void k_pst(R v, R& mi, R& mr, R& hi, R& hr) {
         v = v + (R)10;
         mi = sigm(-(v + (R)1) * (R)(1.0 / 12.0));
         R mt = (v < (R)-50) ? (R)1.25 + (R)175.03 * M::ex(v * (R)0.026)
@@ -108,7 +111,7 @@ struct TTPCRates {
         hr = qt * M::rc((R)360 + ((R)1010 + (R)24 * (v + (R)55)) * M::ex(-(z * z)));
     }
     // AllModels.cu:121-130
-    static __device__ __forceinline__ void k_tst(R v, R& mi, R& mr, R& hi, R& hr) {
+    static NGPU_HD void k_tst(R v, R& mi, R& mr, R& hi, R& hr) {
         v = v + (R)10;
         mi = sigm(-v * (R)(1.0 / 19.0));
         R zm = (v + (R)71) * (R)(1.0 / 59.0);
@@ -118,32 +121,37 @@ struct TTPCRates {
         hr = qt * M::rc((R)8 + (R)49 * M::ex(-(zh * zh)));
     }
     // AllModels.cu:131-151
-    static __device__ __forceinline__ void nap(R v, R& mi, R& mr, R& hi, R& hr) {
+    static NGPU_HD void nap(R v, R& mi, R& mr, R& hi, R& hr) {
         mi = sigm((v + (R)52.6) * (R)(-1.0 / 4.6));
+        if (v == (R)-38.0) v = v + (R)0.0001;
         R ma = (R)(0.182 * 6.0) * efun(-(v + (R)38) * (R)(1.0 / 6.0));
         R mb = (R)(0.124 * 6.0) * efun((v + (R)38) * (R)(1.0 / 6.0));
         mr = qt * (R)(1.0 / 6.0) * (ma + mb);
+        if (v == (R)-17.0) v = v + (R)0.0001;
+        if (v == (R)-64.4) v = v + (R)0.0001;
         hi = sigm((v + (R)48.8) * (R)(1.0 / 10.0));
         R ha = (R)(2.88e-6 * 4.63) * efun((v + (R)17) * (R)(1.0 / 4.63));
         R hb = (R)(6.94e-6 * 2.63) * efun(-(v + (R)64.4) * (R)(1.0 / 2.63));
         hr = qt * (ha + hb);
     }
     // AllModels.cu:152-169 (NaTa_t: th_m=-38, th_h=-66), :170-187 (NaTs2_t: -32, -60)
-    static __device__ __forceinline__ void nat(R v, R thm, R thh, R& mi, R& mr, R& hi, R& hr) {
+    static NGPU_HD void nat(R v, R thm, R thh, R& mi, R& mr, R& hi, R& hr) {
+        if (v == thm) v = v + (R)0.0001;
         R ma = (R)(0.182 * 6.0) * efun(-(v - thm) * (R)(1.0 / 6.0));
         R mb = (R)(0.124 * 6.0) * efun((v - thm) * (R)(1.0 / 6.0));
         mi = ab_gate(ma, mb, qt, &mr);
+        if (v == thh) v = v + (R)0.0001;
         R ha = (R)(0.015 * 6.0) * efun((v - thh) * (R)(1.0 / 6.0));
         R hb = (R)(0.015 * 6.0) * efun(-(v - thh) * (R)(1.0 / 6.0));
         hi = ab_gate(ha, hb, qt, &hr);
     }
     // AllModels.cu:188-193
-    static __device__ __forceinline__ R sk_zinf(R ca) {
+    static NGPU_HD R sk_zinf(R ca) {
         if (ca < (R)1e-7) ca = ca + (R)1e-7;
         return M::rc((R)1 + M::pw((R)0.00043 * M::rc(ca), (R)4.8));
     }
     // AllModels.cu:194-197
-    static __device__ __forceinline__ void skv3(R v, R& mi, R& mr) {
+    static NGPU_HD void skv3(R v, R& mi, R& mr) {
         mi = sigm((v - (R)18.7) * (R)(-1.0 / 9.7));
         mr = ((R)1 + M::ex((v + (R)46.56) * (R)(-1.0 / 44.14))) * (R)(1.0 / 4.0);
     }
@@ -157,7 +165,7 @@ struct TTPCRates {
 // st: the node's first state row (row stride 32 elements); pr: its first
 // parameter row.  Returns I (mA/cm2) and G = dI/dv; writes the states back.
 template <typename R, bool INIT>
-__device__ __forceinline__ void ttpc_node(uint32_t mk, R v, R dt, R* __restrict__ st,
+NGPU_HD void ttpc_node(uint32_t mk, R v, R dt, R* __restrict__ st,
                                           const float* __restrict__ pr, R& I, R& G) {
     using Q = TTPCRates<R>;
     using M = Math<R>;

@@ -11,6 +11,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -44,6 +45,7 @@ int fail(int code, const std::string& msg) {
 struct MechDesc {
     std::vector<int> params;
     int state_rows;
+    int cost;  // rough instruction weight, for balancing node ranges over warps
 };
 struct SetDesc {
     int n_params;
@@ -57,16 +59,17 @@ const SetDesc& set_desc(int ms) {
     // TTPC: GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/CudaStuff.cu:220 call list.
     static const SetDesc ttpc = {
         19,
-        {{{0}, 2}, {{1}, 2}, {{2, 3, 4, 5}, 2}, {{6, 7}, 1}, {{8}, 1}, {{9}, 2}, {{10}, 2},
-         {{11}, 2}, {{12}, 2}, {{13}, 2}, {{14, 15}, 0}, {{16, 17}, 1}, {{18}, 1}},
+        {{{0}, 2, 40}, {{1}, 2, 40}, {{2, 3, 4, 5}, 2, 15}, {{6, 7}, 1, 20}, {{8}, 1, 20},
+         {{9}, 2, 40}, {{10}, 2, 40}, {{11}, 2, 50}, {{12}, 2, 50}, {{13}, 2, 50}, {{14, 15}, 0, 4},
+         {{16, 17}, 1, 20}, {{18}, 1, 20}},
         TTPC::kCaHVA | TTPC::kCaLVA, TTPC::kCaDyn};
     // Mainen: Figures/FigureS4_mainen/CParsed/AllModels.cuh:63 call list
     // (ca's cao argument is never read by the channel code).
     static const SetDesc mainen = {
         34,
-        {{{0}, 2}, {{}, 2}, {{2, 3, 4, 5}, 1}, {{6, 7, 8, 9, 10}, 1}, {{11, 12, 13, 14, 15}, 1},
-         {{16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27}, 2}, {{28, 29}, 0}, {{30, 31}, 0},
-         {{32, 33}, 0}},
+        {{{0}, 2, 40}, {{}, 2, 15}, {{2, 3, 4, 5}, 1, 25}, {{6, 7, 8, 9, 10}, 1, 25},
+         {{11, 12, 13, 14, 15}, 1, 25}, {{16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27}, 2, 55},
+         {{28, 29}, 0, 4}, {{30, 31}, 0, 4}, {{32, 33}, 0, 4}},
         Mainen::kCa, Mainen::kCad};
     return ms == NGPU_MECHSET_TTPC ? ttpc : mainen;
 }
@@ -92,10 +95,93 @@ struct ngpu_model {
     std::vector<uint32_t> mask;
     std::vector<NodeInfo> info;  // rec filled per simulation
     std::vector<int> row_param, row_sec;
-    int slab_rows = 0, ptab_rows = 0, n_jslots = 0;
+    int slab_rows = 0, ptab_rows = 0;
     int64_t state_vars = 0, param_reads = 0;
     std::vector<double> dconst;
+    std::vector<int> weight;        // per-node channel cost
+    std::vector<int2> rows;         // (state rows, parameter rows) per node
 };
+
+// Split of the tree for one CTA of W warps (see sim_kernels.cuh).
+struct Partition {
+    std::vector<int2> seg;          // subtree ranges, grouped by warp
+    std::vector<int> seg_off;       // [W+1]
+    std::vector<int> top;           // top-tree nodes ascending
+    std::vector<int> tch, tch_off;  // top nodes whose channels each warp updates
+    std::vector<int> jslot, pslot;
+    int n_jslots = 0;
+};
+
+static Partition make_partition(const ngpu_model* m, int W) {
+    const int N = m->n;
+    Partition P;
+    std::vector<std::vector<int>> kids(N);
+    for (int i = 1; i < N; ++i) kids[m->parent[i]].push_back(i);
+    std::vector<int64_t> subw(N, 0);
+    std::vector<int> subn(N, 1);
+    for (int i = N - 1; i >= 0; --i) {
+        subw[i] += m->weight[i];
+        if (i > 0) {
+            subw[m->parent[i]] += subw[i];
+            subn[m->parent[i]] += subn[i];
+        }
+    }
+    const int64_t total = subw[0];
+    const int64_t target = std::max<int64_t>(1, total / W);
+    std::vector<char> in_top(N, 0);
+    in_top[0] = 1;
+    std::vector<int> cand(kids[0].begin(), kids[0].end());
+    while (!cand.empty()) {
+        size_t best = 0;
+        for (size_t k = 1; k < cand.size(); ++k)
+            if (subw[cand[k]] > subw[cand[best]]) best = k;
+        if (W == 1 || subw[cand[best]] <= target) break;
+        const int c = cand[best];
+        cand.erase(cand.begin() + best);
+        in_top[c] = 1;
+        cand.insert(cand.end(), kids[c].begin(), kids[c].end());
+    }
+    // bin-pack the subtrees (largest first) onto the least-loaded warp
+    std::sort(cand.begin(), cand.end(), [&](int x, int y) { return subw[x] > subw[y]; });
+    std::vector<int64_t> load(W, 0);
+    std::vector<std::vector<int2>> per(W);
+    for (int c : cand) {
+        int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[w] += subw[c];
+        per[w].push_back(make_int2(c, c + subn[c]));
+    }
+    // the top nodes' channel work goes to the least-loaded warps as well
+    for (int i = 0; i < N; ++i)
+        if (in_top[i]) P.top.push_back(i);
+    std::vector<std::vector<int>> tper(W);
+    for (int i : P.top) {
+        int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[w] += m->weight[i];
+        tper[w].push_back(i);
+    }
+    P.seg_off.assign(1, 0);
+    P.tch_off.assign(1, 0);
+    for (int w = 0; w < W; ++w) {
+        std::sort(per[w].begin(), per[w].end(), [](int2 x, int2 y) { return x.x < y.x; });
+        P.seg.insert(P.seg.end(), per[w].begin(), per[w].end());
+        P.seg_off.push_back((int)P.seg.size());
+        P.tch.insert(P.tch.end(), tper[w].begin(), tper[w].end());
+        P.tch_off.push_back((int)P.tch.size());
+    }
+    // junction slots: parents of a child other than node+1, and top parents of subtree roots
+    std::vector<char> sub_root(N, 0);
+    for (int c : cand) sub_root[c] = 1;
+    std::vector<char> need(N, 0);
+    for (int i = 1; i < N; ++i)
+        if (m->parent[i] != i - 1 || sub_root[i]) need[m->parent[i]] = 1;
+    P.jslot.assign(N, -1);
+    P.pslot.assign(N, -1);
+    for (int i = 0; i < N; ++i)
+        if (need[i]) P.jslot[i] = P.n_jslots++;
+    for (int i = 1; i < N; ++i)
+        if (m->parent[i] != i - 1 || sub_root[i]) P.pslot[i] = P.jslot[m->parent[i]];
+    return P;
+}
 
 struct ngpu_sim {
     ngpu_model* m = nullptr;
@@ -103,9 +189,18 @@ struct ngpu_sim {
     // device buffers
     NodeInfo* d_info = nullptr;
     void* d_coef = nullptr;
+    void* d_solve = nullptr;
+    void* d_vbuf = nullptr;
     void* d_slab = nullptr;
     float* d_ptab = nullptr;
     void* d_scr = nullptr;
+    int* d_err = nullptr;
+    int2* d_rows = nullptr;
+    int2* d_seg = nullptr;
+    int* d_top = nullptr;
+    int* d_tch = nullptr;
+    int n_warps = 1;
+    Partition part;
     double* d_jacc = nullptr;
     void* d_jx = nullptr;
     int* d_inst_stim = nullptr;
@@ -119,7 +214,7 @@ struct ngpu_sim {
     size_t tmp_out_bytes = 0;
     // stimulus / recording
     int nt = 0, stim_node = 0;
-    float stim_scale = 0.f;
+    double stim_scale = 0.0;
     std::vector<int> rec_nodes;       // as given
     std::vector<int> rec_cols;        // column of each given site
     int n_rec_unique = 0, rec_every = 1, n_samples = 0;
@@ -134,6 +229,8 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.info = s->d_info;
     A.coef = (const NodeCoef<R>*)s->d_coef;
     A.n_nodes = m->n;
+    A.solve = (const SolveNode<R>*)s->d_solve;
+    A.vbuf = (R*)s->d_vbuf;
     A.slab = (R*)s->d_slab;
     A.slab_rows = m->slab_rows;
     A.ptab = s->d_ptab;
@@ -141,7 +238,7 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.scr = (R*)s->d_scr;
     A.jacc = s->d_jacc;
     A.jx = (R*)s->d_jx;
-    A.n_jslots = m->n_jslots;
+    A.n_jslots = s->part.n_jslots;
     A.amps = s->d_amps;
     A.dts = s->d_dts;
     A.nt = s->nt;
@@ -154,14 +251,27 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.n_inst_pad = s->n_pad;
     A.v_init = s->v_init;
     A.bad = s->d_bad;
+    A.err = s->d_err;
+    A.n_warps = s->n_warps;
+    A.rows = s->d_rows;
+    A.seg = s->d_seg;
+    A.top = s->d_top;
+    A.n_top = (int)s->part.top.size();
+    A.tch = s->d_tch;
+    for (int w = 0; w <= kMaxWarps; ++w) {
+        const int ww = std::min(w, s->n_warps);
+        A.seg_off[w] = s->part.seg_off[ww];
+        A.tch_off[w] = s->part.tch_off[ww];
+    }
     return A;
 }
 
 template <typename R>
 static cudaError_t launch_init(ngpu_sim* s, cudaStream_t st) {
     SimArgs<R> A = make_args<R>(s);
-    if (s->m->mechset == NGPU_MECHSET_TTPC) k_sim_init<R, 0><<<s->n_groups, kLanes, 0, st>>>(A);
-    else k_sim_init<R, 1><<<s->n_groups, kLanes, 0, st>>>(A);
+    const int threads = kLanes * s->n_warps;
+    if (s->m->mechset == NGPU_MECHSET_TTPC) k_sim_init<R, 0><<<s->n_groups, threads, 0, st>>>(A);
+    else k_sim_init<R, 1><<<s->n_groups, threads, 0, st>>>(A);
     g_launches++;
     return cudaGetLastError();
 }
@@ -169,8 +279,18 @@ static cudaError_t launch_init(ngpu_sim* s, cudaStream_t st) {
 template <typename R>
 static cudaError_t launch_advance(ngpu_sim* s, int t0, int n, cudaStream_t st) {
     SimArgs<R> A = make_args<R>(s);
-    if (s->m->mechset == NGPU_MECHSET_TTPC) k_sim_advance<R, 0><<<s->n_groups, kLanes, 0, st>>>(A, t0, n);
-    else k_sim_advance<R, 1><<<s->n_groups, kLanes, 0, st>>>(A, t0, n);
+    const int threads = kLanes * s->n_warps;
+    const size_t smem = SmemPlan<R>::bytes(s->m->n);
+    cudaError_t e;
+    if (s->m->mechset == NGPU_MECHSET_TTPC) {
+        e = cudaFuncSetAttribute(k_sim_advance<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_sim_advance<R, 0><<<s->n_groups, threads, smem, st>>>(A, t0, n);
+    } else {
+        e = cudaFuncSetAttribute(k_sim_advance<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_sim_advance<R, 1><<<s->n_groups, threads, smem, st>>>(A, t0, n);
+    }
     g_launches++;
     return cudaGetLastError();
 }
@@ -239,20 +359,11 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
                                             "(its reversal potential would be infinite)");
         }
     }
-    // children bookkeeping: dconst and junction slots
+    // constant part of the diagonal
     m->dconst.assign(n_nodes, 0.0);
-    std::vector<int> has_far(n_nodes, 0);
     for (int i = 0; i < n_nodes; ++i) m->dconst[i] = -m->a[i];
     m->dconst[0] = 0.0;  // the root has no parent coupling
-    for (int i = 1; i < n_nodes; ++i) {
-        m->dconst[parent[i]] -= m->b[i];
-        if (parent[i] != i - 1) has_far[parent[i]] = 1;
-    }
-    std::vector<int> jslot(n_nodes, -1);
-    int nj = 0;
-    for (int i = 0; i < n_nodes; ++i)
-        if (has_far[i]) jslot[i] = nj++;
-    m->n_jslots = nj;
+    for (int i = 1; i < n_nodes; ++i) m->dconst[parent[i]] -= m->b[i];
     // state and parameter rows
     std::map<std::pair<int, uint32_t>, int> prow_of;
     m->info.resize(n_nodes);
@@ -262,14 +373,16 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
         ni.parent = parent[i];
         ni.mask = m->mask[i];
         ni.srow = srow;
-        int srows = 0;
+        int srows = 0, wt = 12;
         std::vector<int> plist;
         for (int k = 0; k < NM; ++k)
             if (ni.mask & (1u << k)) {
                 srows += sd.mechs[k].state_rows;
+                wt += sd.mechs[k].cost;
                 plist.insert(plist.end(), sd.mechs[k].params.begin(), sd.mechs[k].params.end());
             }
-        srow += 2 + srows;
+        srow += srows;
+        m->weight.push_back(wt);
         m->state_vars += srows;
         m->param_reads += (int64_t)plist.size();
         auto key = std::make_pair(section[i], ni.mask);
@@ -283,12 +396,13 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
             it = prow_of.emplace(key, first).first;
         }
         ni.prow = it->second;
-        ni.jslot = jslot[i];
-        ni.pslot = (i > 0 && parent[i] != i - 1) ? jslot[parent[i]] : -1;
+        ni.jslot = -1;
+        ni.pslot = -1;
         ni.rec = -1;
         ni.pad = 0;
+        m->rows.push_back(make_int2(srows, (int)plist.size()));
     }
-    m->slab_rows = srow;
+    m->slab_rows = std::max(1, srow);
     m->ptab_rows = std::max(1, (int)m->row_param.size());
     if (m->row_param.empty()) {
         m->row_param.push_back(0);
@@ -308,17 +422,39 @@ int ngpu_model_layout(const ngpu_model* m, int32_t* state_rows, int32_t* param_r
     if (!m) return fail(NGPU_E_INVALID, "null model");
     if (state_rows) *state_rows = m->slab_rows;
     if (param_rows) *param_rows = m->ptab_rows;
-    if (n_jslots) *n_jslots = m->n_jslots;
+    if (n_jslots) *n_jslots = make_partition(m, 1).n_jslots;
     if (state_vars) *state_vars = m->state_vars;
     if (param_reads) *param_reads = m->param_reads;
     return NGPU_OK;
 }
 
+int ngpu_model_partition(const ngpu_model* m, int32_t n_warps, int32_t* top_flag, int32_t* owner,
+                         int32_t* jslot, int32_t* pslot, int32_t* n_jslots) {
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    if (n_warps < 1 || n_warps > kMaxWarps) return fail(NGPU_E_INVALID, "n_warps out of range");
+    Partition P = make_partition(m, n_warps);
+    for (int i = 0; i < m->n; ++i) {
+        if (top_flag) top_flag[i] = 0;
+        if (owner) owner[i] = -1;
+        if (jslot) jslot[i] = P.jslot[i];
+        if (pslot) pslot[i] = P.pslot[i];
+    }
+    for (int i : P.top)
+        if (top_flag) top_flag[i] = 1;
+    for (int w = 0; w < n_warps; ++w)
+        for (int k = P.seg_off[w]; k < P.seg_off[w + 1]; ++k)
+            for (int i = P.seg[k].x; i < P.seg[k].y; ++i)
+                if (owner) owner[i] = w;
+    if (n_jslots) *n_jslots = P.n_jslots;
+    return NGPU_OK;
+}
+
 static void sim_free(ngpu_sim* s) {
     if (!s) return;
-    void* ptrs[] = {s->d_info, s->d_coef, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc,
-                    s->d_jx, s->d_inst_stim, s->d_bad, s->d_row_param, s->d_row_sec,
-                    s->d_amps, s->d_dts, s->d_trace, s->d_tmp_out};
+    void* ptrs[] = {s->d_info, s->d_coef, s->d_solve, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr,
+                    s->d_jacc, s->d_jx, s->d_inst_stim, s->d_bad, s->d_err, s->d_row_param,
+                    s->d_row_sec, s->d_amps, s->d_dts, s->d_trace, s->d_tmp_out, s->d_rows,
+                    s->d_seg, s->d_top, s->d_tch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete s;
@@ -333,6 +469,12 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
     if (precision != NGPU_FP32 && precision != NGPU_FP64)
         return fail(NGPU_E_INVALID, "precision must be NGPU_FP32 or NGPU_FP64");
     if ((int64_t)n_sets * n_stim > (int64_t)1 << 30) return fail(NGPU_E_INVALID, "too many instances");
+    {
+        const size_t need = precision == NGPU_FP64 ? SmemPlan<double>::bytes(m->n) : SmemPlan<float>::bytes(m->n);
+        if (need > 227 * 1024)
+            return fail(NGPU_E_INVALID, "morphology too large for the shared-memory solve plan (" +
+                                            std::to_string(m->n) + " nodes)");
+    }
     ngpu_sim* s = new (std::nothrow) ngpu_sim();
     if (!s) return fail(NGPU_E_NOMEM, "host allocation failed");
     s->m = m;
@@ -345,6 +487,13 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
     const size_t esz = precision == NGPU_FP64 ? 8 : 4;
     const size_t G = (size_t)s->n_groups, L = kLanes;
     int rc = NGPU_OK;
+    // warps per CTA and the tree split over them
+    int W = std::min(8, std::max(1, m->n / 48));
+    if (const char* ev = getenv("NGPU_WARPS")) W = std::max(1, std::min(kMaxWarps, atoi(ev)));
+    W = std::min(W, m->n);
+    s->n_warps = W;
+    s->part = make_partition(m, W);
+    const int nj = s->part.n_jslots;
 #define ALLOC(field, type, bytes)                              \
     s->field = (type)dmalloc((bytes), &rc);                    \
     if (!s->field) {                                           \
@@ -353,27 +502,50 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
     }
     ALLOC(d_info, NodeInfo*, sizeof(NodeInfo) * m->n);
     ALLOC(d_coef, void*, 4 * esz * m->n);
+    ALLOC(d_solve, void*, (precision == NGPU_FP64 ? sizeof(SolveNode<double>) : sizeof(SolveNode<float>)) * m->n);
+    ALLOC(d_vbuf, void*, G * 2 * m->n * L * esz);
     ALLOC(d_slab, void*, G * m->slab_rows * L * esz);
     ALLOC(d_ptab, float*, G * m->ptab_rows * L * sizeof(float));
-    ALLOC(d_scr, void*, G * 2 * m->n * L * esz);
-    ALLOC(d_jacc, double*, G * 2 * std::max(1, m->n_jslots) * L * sizeof(double));
-    ALLOC(d_jx, void*, G * 2 * std::max(1, m->n_jslots) * L * esz);
+    ALLOC(d_scr, void*, G * 3 * m->n * L * esz);
+    ALLOC(d_jacc, double*, G * 2 * std::max(1, nj) * L * sizeof(double));
+    ALLOC(d_jx, void*, G * std::max(1, nj) * L * esz);
+    ALLOC(d_err, int*, sizeof(int));
+    ALLOC(d_rows, int2*, sizeof(int2) * m->n);
+    ALLOC(d_seg, int2*, sizeof(int2) * std::max<size_t>(1, s->part.seg.size()));
+    ALLOC(d_top, int*, sizeof(int) * std::max<size_t>(1, s->part.top.size()));
+    ALLOC(d_tch, int*, sizeof(int) * std::max<size_t>(1, s->part.tch.size()));
     ALLOC(d_inst_stim, int*, sizeof(int) * s->n_pad);
     ALLOC(d_bad, int*, sizeof(int) * s->n_pad);
     ALLOC(d_row_param, int*, sizeof(int) * m->row_param.size());
     ALLOC(d_row_sec, int*, sizeof(int) * m->row_sec.size());
 #undef ALLOC
-    // coefficients in the run's precision
+    // coefficients and the phase-S topology in the run's precision
     if (precision == NGPU_FP64) {
         std::vector<NodeCoef<double>> c(m->n);
-        for (int i = 0; i < m->n; ++i) c[i] = {m->a[i], m->b[i], m->dconst[i], m->cm[i] / 1000.0};
-        cudaMemcpy(s->d_coef, c.data(), sizeof(NodeCoef<double>) * m->n, cudaMemcpyHostToDevice);
+        std::vector<SolveNode<double>> sv(m->n);
+        for (int i = 0; i < m->n; ++i) {
+            c[i] = {m->a[i], m->b[i], m->dconst[i], m->cm[i] / 1000.0};
+            sv[i] = {m->a[i], m->b[i], s->part.jslot[i], s->part.pslot[i]};
+        }
+        cudaMemcpy(s->d_coef, c.data(), sizeof(c[0]) * m->n, cudaMemcpyHostToDevice);
+        cudaMemcpy(s->d_solve, sv.data(), sizeof(sv[0]) * m->n, cudaMemcpyHostToDevice);
     } else {
         std::vector<NodeCoef<float>> c(m->n);
-        for (int i = 0; i < m->n; ++i)
+        std::vector<SolveNode<float>> sv(m->n);
+        for (int i = 0; i < m->n; ++i) {
             c[i] = {(float)m->a[i], (float)m->b[i], (float)m->dconst[i], (float)(m->cm[i] / 1000.0)};
-        cudaMemcpy(s->d_coef, c.data(), sizeof(NodeCoef<float>) * m->n, cudaMemcpyHostToDevice);
+            sv[i] = {(float)m->a[i], (float)m->b[i], s->part.jslot[i], s->part.pslot[i]};
+        }
+        cudaMemcpy(s->d_coef, c.data(), sizeof(c[0]) * m->n, cudaMemcpyHostToDevice);
+        cudaMemcpy(s->d_solve, sv.data(), sizeof(sv[0]) * m->n, cudaMemcpyHostToDevice);
     }
+    cudaMemcpy(s->d_rows, m->rows.data(), sizeof(int2) * m->n, cudaMemcpyHostToDevice);
+    if (!s->part.seg.empty())
+        cudaMemcpy(s->d_seg, s->part.seg.data(), sizeof(int2) * s->part.seg.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(s->d_top, s->part.top.data(), sizeof(int) * s->part.top.size(), cudaMemcpyHostToDevice);
+    if (!s->part.tch.empty())
+        cudaMemcpy(s->d_tch, s->part.tch.data(), sizeof(int) * s->part.tch.size(), cudaMemcpyHostToDevice);
+    cudaMemset(s->d_err, 0, sizeof(int));
     std::vector<int> inst_stim(s->n_pad);
     for (int k = 0; k < s->n_pad; ++k) inst_stim[k] = std::min(k, s->n_inst - 1) % n_stim;
     cudaMemcpy(s->d_inst_stim, inst_stim.data(), sizeof(int) * s->n_pad, cudaMemcpyHostToDevice);
@@ -458,7 +630,7 @@ int ngpu_sim_set_stimulus(ngpu_sim* s, int32_t nt, const float* amps, const floa
     NGPU_CUDA(cudaMemcpy(s->d_dts, dts, sizeof(float) * (size_t)nt, kind));
     s->nt = nt;
     s->stim_node = stim_node;
-    s->stim_scale = 100.0f / stim_area_um2;
+    s->stim_scale = 100.0 / (double)stim_area_um2;
     s->has_stim = true;
     s->initialized = false;
     return NGPU_OK;
@@ -498,6 +670,10 @@ int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
     const ngpu_model* m = s->m;
     // node table with this run's recording columns
     std::vector<NodeInfo> info = m->info;
+    for (int i = 0; i < m->n; ++i) {
+        info[i].jslot = s->part.jslot[i];
+        info[i].pslot = s->part.pslot[i];
+    }
     std::vector<int> uniq(s->n_rec_unique, -1);
     for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
     for (int c = 0; c < s->n_rec_unique; ++c) info[uniq[c]].rec = c;
@@ -585,6 +761,9 @@ int ngpu_sim_check(ngpu_sim* s, int32_t* n_bad, void* cuda_stream) {
     int c = 0;
     for (int i = 0; i < s->n_inst; ++i) c += bad[i] != 0;
     *n_bad = c;
+    int err = 0;
+    NGPU_CUDA(cudaMemcpy(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(NGPU_E_CUDA, "a shared-memory pipeline wait timed out in the solve phase");
     return NGPU_OK;
 }
 

@@ -9,40 +9,52 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#define NGPU_HD __host__ __device__ __forceinline__
+
 namespace ngpu {
 
 template <typename R> struct Math;
 
+// FP32 uses the SFU approximations on the device; a host build (tests only)
+// falls back to the C library.
 template <> struct Math<float> {
-    static __device__ __forceinline__ float ex(float x) { return __expf(x); }
-    static __device__ __forceinline__ float lg(float x) { return __logf(x); }
-    static __device__ __forceinline__ float dv(float a, float b) { return __fdividef(a, b); }
-    static __device__ __forceinline__ float rc(float a) { return __fdividef(1.0f, a); }
-    static __device__ __forceinline__ float pw(float a, float b) { return __powf(a, b); }
+#ifdef __CUDA_ARCH__
+    static NGPU_HD float ex(float x) { return __expf(x); }
+    static NGPU_HD float lg(float x) { return __logf(x); }
+    static NGPU_HD float dv(float a, float b) { return __fdividef(a, b); }
+    static NGPU_HD float rc(float a) { return __fdividef(1.0f, a); }
+    static NGPU_HD float pw(float a, float b) { return __powf(a, b); }
+#else
+    static NGPU_HD float ex(float x) { return expf(x); }
+    static NGPU_HD float lg(float x) { return logf(x); }
+    static NGPU_HD float dv(float a, float b) { return a / b; }
+    static NGPU_HD float rc(float a) { return 1.0f / a; }
+    static NGPU_HD float pw(float a, float b) { return powf(a, b); }
+#endif
     // 1 - exp(-z) for z >= 0 without the cancellation 1 - exp(-z) suffers in
     // FP32 when z = dt/tau is small (slow gates, Ca decay): below z = 1/32 the
     // alternating Taylor series z - z^2/2 + z^3/6 - z^4/24 has truncation
     // error < z^5/120 < 3e-10 relative.
-    static __device__ __forceinline__ float one_minus_exp_neg(float z) {
+    static NGPU_HD float one_minus_exp_neg(float z) {
         if (z < 0.03125f) {
             return z * (1.0f - z * (0.5f - z * (0.16666667f - z * 0.041666668f)));
         }
-        return 1.0f - __expf(-z);
+        return 1.0f - ex(-z);
     }
 };
 
 template <> struct Math<double> {
-    static __device__ __forceinline__ double ex(double x) { return exp(x); }
-    static __device__ __forceinline__ double lg(double x) { return log(x); }
-    static __device__ __forceinline__ double dv(double a, double b) { return a / b; }
-    static __device__ __forceinline__ double rc(double a) { return 1.0 / a; }
-    static __device__ __forceinline__ double pw(double a, double b) { return pow(a, b); }
-    static __device__ __forceinline__ double one_minus_exp_neg(double z) { return -expm1(-z); }
+    static NGPU_HD double ex(double x) { return exp(x); }
+    static NGPU_HD double lg(double x) { return log(x); }
+    static NGPU_HD double dv(double a, double b) { return a / b; }
+    static NGPU_HD double rc(double a) { return 1.0 / a; }
+    static NGPU_HD double pw(double a, double b) { return pow(a, b); }
+    static NGPU_HD double one_minus_exp_neg(double z) { return -expm1(-z); }
 };
 
 // cnexp update of a first-order gate: x += (1 - exp(-dt/tau)) (xinf - x).
 template <typename R>
-__device__ __forceinline__ R cnexp(R x, R xinf, R tau, R dt) {
+NGPU_HD R cnexp(R x, R xinf, R tau, R dt) {
     return x + Math<R>::one_minus_exp_neg(Math<R>::dv(dt, tau)) * (xinf - x);
 }
 

@@ -49,6 +49,15 @@ class Model:
         return {"state_rows": sr.value, "param_rows": pr.value, "n_jslots": nj.value,
                 "state_vars": sv.value, "param_reads": prd.value}
 
+    def partition(self, n_warps: int) -> dict:
+        """The tree split a CTA of n_warps warps uses (see ngpu_model_partition)."""
+        n = self.cell.n_nodes
+        top, own, js, ps = (np.zeros(n, dtype=np.int32) for _ in range(4))
+        nj = C.c_int32()
+        _ffi.check("ngpu_model_partition", _ffi.lib().ngpu_model_partition(
+            self._h, int(n_warps), _ffi.ptr(top), _ffi.ptr(own), _ffi.ptr(js), _ffi.ptr(ps), C.byref(nj)))
+        return {"top": top.astype(bool), "owner": own, "jslot": js, "pslot": ps, "n_jslots": nj.value}
+
     def close(self) -> None:
         if self._h:
             _ffi.lib().ngpu_model_destroy(self._h)
