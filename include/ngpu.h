@@ -71,12 +71,20 @@ int ngpu_model_destroy(ngpu_model *m);
 int ngpu_model_layout(const ngpu_model *m, int32_t *state_rows, int32_t *param_rows,
                       int32_t *n_jslots, int64_t *state_vars, int64_t *param_reads);
 
-/* Introspection of the tree split used by a CTA of n_warps warps: per node,
- * top_flag (1 = top tree, solved by warp 0), owner (warp of its subtree, -1
- * for top nodes), junction slot and parent junction slot.  Any pointer may
- * be NULL. */
-int ngpu_model_partition(const ngpu_model *m, int32_t n_warps, int32_t *top_flag, int32_t *owner,
+/* Introspection of the tree split used by a CTA of n_warps warps, per node in
+ * the caller's numbering: sep_flag (1 = separator, solved by warp 0 in the
+ * skeleton), item (work item holding the node, -1 for separators), junction
+ * slot and parent junction slot.  Any pointer may be NULL. */
+int ngpu_model_partition(const ngpu_model *m, int32_t n_warps, int32_t *sep_flag, int32_t *item,
                          int32_t *jslot, int32_t *pslot, int32_t *n_jslots);
+/* The same split in the library's internal node order (heavy-first depth
+ * first): perm[n] maps internal -> caller's node; comps[6*k] = (root, upper
+ * separator, lower separator or -1, its separator index, light range lo, hi);
+ * seps[3*k] = (node, skeleton parent index, linking item or -1); jslot/pslot
+ * per internal node.  For tests and tools. */
+int ngpu_model_split_info(const ngpu_model *m, int32_t n_warps, int32_t *perm, int32_t *n_comps,
+                          int32_t *comps, int32_t max_comps, int32_t *n_seps, int32_t *seps,
+                          int32_t max_seps, int32_t *jslot, int32_t *pslot);
 
 /*
  * One complete run from host buffers (the drop-in for one neuroGPU process).

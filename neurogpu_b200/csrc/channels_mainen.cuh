@@ -31,108 +31,128 @@ struct Mainen {
     static constexpr double kVshiftNa = -5.0;
 };
 
+// One node, three phases (load every row / compute / store), as ttpc_node.
 template <typename R, bool INIT>
-NGPU_HD void mainen_node(uint32_t mk, R v, R dt, R* __restrict__ st,
-                                            const float* __restrict__ pr, R& I, R& G) {
+NGPU_HD void mainen_node(uint32_t mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,
+                         R& G) {
     using M = Math<R>;
     constexpr int S = 32;
     const R tadj = (R)Mainen::kTadj;
-    int s = 0, q = 0;
+    // ---------------------------------------------------------------- load
+    R ca_m = 0, ca_h = 0, cai = 0, ica = 0, kca_n = 0, km_n = 0, kv_n = 0, na_m = 0, na_h = 0;
+    R g_ca = 0, g_kca = 0, caix = 1, ra_kca = 0, rb_kca = 0;
+    R km[5] = {0, 0, 1, 0, 0}, kv[5] = {0, 0, 1, 0, 0};  // gbar, tha, qa, Ra, Rb
+    R na[12] = {0, 0, 1, 0, 0, 0, 0, 1, 0, 1, 0, 0};    // gbar tha qa Ra Rb thi1 thi2 qi thinf qinf Rg Rd
+    R pas[6] = {0, 0, 0, 0, 0, 0};
+    {
+        int s = 0, q = 0;
+        if (mk & Mainen::kCa) { if (!INIT) { ca_m = st[s * S]; ca_h = st[(s + 1) * S]; } s += 2; g_ca = (R)pr[q * S]; q += 1; }
+        if (mk & Mainen::kCad) { if (!INIT) { cai = st[s * S]; ica = st[(s + 1) * S]; } s += 2; }
+        if (mk & Mainen::kKca) {
+            if (!INIT) kca_n = st[s * S];
+            s += 1;
+            g_kca = (R)pr[q * S]; caix = (R)pr[(q + 1) * S]; ra_kca = (R)pr[(q + 2) * S]; rb_kca = (R)pr[(q + 3) * S];
+            q += 4;
+        }
+        if (mk & Mainen::kKm) {
+            if (!INIT) km_n = st[s * S];
+            s += 1;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) km[k] = (R)pr[(q + k) * S];
+            q += 5;
+        }
+        if (mk & Mainen::kKv) {
+            if (!INIT) kv_n = st[s * S];
+            s += 1;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) kv[k] = (R)pr[(q + k) * S];
+            q += 5;
+        }
+        if (mk & Mainen::kNa) {
+            if (!INIT) { na_m = st[s * S]; na_h = st[(s + 1) * S]; }
+            s += 2;
+#pragma unroll
+            for (int k = 0; k < 12; ++k) na[k] = (R)pr[(q + k) * S];
+            q += 12;
+        }
+        if (mk & Mainen::kPas) { pas[0] = (R)pr[q * S]; pas[1] = (R)pr[(q + 1) * S]; q += 2; }
+        if (mk & Mainen::kPas2) { pas[2] = (R)pr[q * S]; pas[3] = (R)pr[(q + 1) * S]; q += 2; }
+        if (mk & Mainen::kPasx) { pas[4] = (R)pr[q * S]; pas[5] = (R)pr[(q + 1) * S]; q += 2; }
+    }
+    // ------------------------------------------------------------- compute
     R Itot = 0, Gtot = 0;
     R mi, mr, hi, hr;
-    R ca_m = 0, ca_h = 0, ca_g = 0;
     if (mk & Mainen::kCa) {  // AllModels.cu:117-129, 228-233
-        ca_g = (R)pr[q * S]; q += 1;
         R a = (R)0.209 * efun(-((R)27 + v) * (R)(1.0 / 3.8));
         R b = (R)0.94 * M::ex((-(R)75 - v) * (R)(1.0 / 17.0));
         mi = ab_gate(a, b, tadj, &mr);
         a = (R)0.000457 * M::ex((-(R)13 - v) * (R)(1.0 / 50.0));
         b = (R)0.0065 * sigm((-v - (R)15) * (R)(1.0 / 28.0));
         hi = ab_gate(a, b, tadj, &hr);
-        ca_m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        ca_h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = ca_m; st[(s + 1) * S] = ca_h; s += 2;
+        ca_m = INIT ? mi : cnexp_rate(ca_m, mi, mr, dt);
+        ca_h = INIT ? hi : cnexp_rate(ca_h, hi, hr, dt);
     }
-    R cai = 0;
-    int ica_row = -1;
     if (mk & Mainen::kCad) {  // AllModels.cu:198-203, 234-242
         if (INIT) cai = (R)Mainen::kCainfCad;
         else {
-            R ica = st[(s + 1) * S];
             R drive = (R)(-10000.0 / (2.0 * kFaraday * Mainen::kDepthCad)) * ica;
             if (drive <= (R)0) drive = (R)0;
             R cinf = (drive + (R)(Mainen::kCainfCad / Mainen::kTaurCad)) * (R)Mainen::kTaurCad;
-            cai = cnexp_rate(st[s * S], cinf, (R)(1.0 / Mainen::kTaurCad), dt);
+            cai = cnexp_rate(cai, cinf, (R)(1.0 / Mainen::kTaurCad), dt);
         }
-        st[s * S] = cai;
-        ica_row = s + 1;
-        s += 2;
     }
     if (mk & Mainen::kKca) {  // AllModels.cu:130-136, 243-249
-        R g = (R)pr[q * S], caix = (R)pr[(q + 1) * S];
-        R Ra = (R)pr[(q + 2) * S], Rb = (R)pr[(q + 3) * S];
-        q += 4;
-        R a = Ra * M::pw(cai, caix);
-        mi = ab_gate(a, Rb, tadj, &mr);
-        R n = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        st[s * S] = n; s += 1;
-        R gx = (R)1e-4 * tadj * g * n; Itot += gx * (v - (R)Mainen::kEk); Gtot += gx;
+        R a = ra_kca * M::pw(cai, caix);
+        mi = ab_gate(a, rb_kca, tadj, &mr);
+        kca_n = INIT ? mi : cnexp_rate(kca_n, mi, mr, dt);
+        R gx = (R)1e-4 * tadj * g_kca * kca_n; Itot += gx * (v - (R)Mainen::kEk); Gtot += gx;
     }
-#define NGPU_MAINEN_K(BIT)                                                                \
-    if (mk & (BIT)) { /* km AllModels.cu:140-146, kv :150-156 */                          \
-        R g = (R)pr[q * S], tha = (R)pr[(q + 1) * S], qa = (R)pr[(q + 2) * S];            \
-        R Ra = (R)pr[(q + 3) * S], Rb = (R)pr[(q + 4) * S];                               \
-        q += 5;                                                                           \
-        R z = M::dv(v - tha, qa);                                                         \
-        R a = Ra * qa * efun(-z);                                                         \
-        R b = Rb * qa * efun(z);                                                          \
-        mi = ab_gate(a, b, tadj, &mr);                                                    \
-        R n = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);                              \
-        st[s * S] = n; s += 1;                                                            \
-        R gx = (R)1e-4 * tadj * g * n; Itot += gx * (v - (R)Mainen::kEk); Gtot += gx;    \
-    }
-    NGPU_MAINEN_K(Mainen::kKm)
-    NGPU_MAINEN_K(Mainen::kKv)
-#undef NGPU_MAINEN_K
-    if (mk & Mainen::kNa) {  // AllModels.cu:160-172, 266-273 (rates at v + vshift)
-        R g = (R)pr[q * S], tha = (R)pr[(q + 1) * S], qa = (R)pr[(q + 2) * S];
-        R Ra = (R)pr[(q + 3) * S], Rb = (R)pr[(q + 4) * S], thi1 = (R)pr[(q + 5) * S];
-        R thi2 = (R)pr[(q + 6) * S], qi = (R)pr[(q + 7) * S], thinf = (R)pr[(q + 8) * S];
-        R qinf = (R)pr[(q + 9) * S], Rg = (R)pr[(q + 10) * S], Rd = (R)pr[(q + 11) * S];
-        q += 12;
-        R vm = v + (R)Mainen::kVshiftNa;
-        R a = Ra * qa * efun(-M::dv(vm - tha, qa));
-        R b = Rb * qa * efun(M::dv(vm - tha, qa));
+    // km AllModels.cu:140-146, kv :150-156 (same rate form)
+    auto kgate = [&](const R* p, R& n) {
+        R z = M::dv(v - p[1], p[2]);
+        R a = p[3] * p[2] * efun(-z);
+        R b = p[4] * p[2] * efun(z);
         mi = ab_gate(a, b, tadj, &mr);
-        a = Rd * qi * efun(-M::dv(vm - thi1, qi));
-        b = Rg * qi * efun(M::dv(vm - thi2, qi));
+        n = INIT ? mi : cnexp_rate(n, mi, mr, dt);
+        R gx = (R)1e-4 * tadj * p[0] * n; Itot += gx * (v - (R)Mainen::kEk); Gtot += gx;
+    };
+    if (mk & Mainen::kKm) kgate(km, km_n);
+    if (mk & Mainen::kKv) kgate(kv, kv_n);
+    if (mk & Mainen::kNa) {  // AllModels.cu:160-172, 266-273 (rates at v + vshift)
+        R vm = v + (R)Mainen::kVshiftNa;
+        R a = na[3] * na[2] * efun(-M::dv(vm - na[1], na[2]));
+        R b = na[4] * na[2] * efun(M::dv(vm - na[1], na[2]));
+        mi = ab_gate(a, b, tadj, &mr);
+        a = na[11] * na[7] * efun(-M::dv(vm - na[5], na[7]));
+        b = na[10] * na[7] * efun(M::dv(vm - na[6], na[7]));
         hr = tadj * (a + b);
-        hi = sigm(M::dv(vm - thinf, qinf));
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        R h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = m; st[(s + 1) * S] = h; s += 2;
-        R gx = (R)1e-4 * tadj * g * m * m * m * h; Itot += gx * (v - (R)Mainen::kEna); Gtot += gx;
+        hi = sigm(M::dv(vm - na[8], na[9]));
+        na_m = INIT ? mi : cnexp_rate(na_m, mi, mr, dt);
+        na_h = INIT ? hi : cnexp_rate(na_h, hi, hr, dt);
+        R gx = (R)1e-4 * tadj * na[0] * na_m * na_m * na_m * na_h; Itot += gx * (v - (R)Mainen::kEna); Gtot += gx;
     }
-#define NGPU_MAINEN_PAS(BIT)                                                              \
-    if (mk & (BIT)) {                                                                     \
-        R g = (R)pr[q * S], e = (R)pr[(q + 1) * S]; q += 2;                               \
-        Itot += g * (v - e); Gtot += g;                                                   \
-    }
-    NGPU_MAINEN_PAS(Mainen::kPas)
-    NGPU_MAINEN_PAS(Mainen::kPas2)
-    NGPU_MAINEN_PAS(Mainen::kPasx)
-#undef NGPU_MAINEN_PAS
+    if (mk & Mainen::kPas) { Itot += pas[0] * (v - pas[1]); Gtot += pas[0]; }
+    if (mk & Mainen::kPas2) { Itot += pas[2] * (v - pas[3]); Gtot += pas[2]; }
+    if (mk & Mainen::kPasx) { Itot += pas[4] * (v - pas[5]); Gtot += pas[4]; }
+    ica = 0;
     if (mk & Mainen::kCa) {  // AllModels.cu:276-285, eca from the updated cai
         R eca = (R)(ktf_of(Mainen::kCelsius) / 2) * M::lg(M::dv((R)kDefCao, cai));
-        R gx = (R)1e-4 * tadj * ca_g * ca_m * ca_m * ca_h;
-        R ica = gx * (v - eca);
+        R gx = (R)1e-4 * tadj * g_ca * ca_m * ca_m * ca_h;
+        ica = gx * (v - eca);
         Itot += ica; Gtot += gx;
-        if (ica_row >= 0) st[ica_row * S] = ica;
-    } else if (ica_row >= 0) {
-        st[ica_row * S] = (R)0;
     }
     I = Itot;
     G = Gtot;
+    // --------------------------------------------------------------- store
+    {
+        int s = 0;
+        if (mk & Mainen::kCa) { st[s * S] = ca_m; st[(s + 1) * S] = ca_h; s += 2; }
+        if (mk & Mainen::kCad) { st[s * S] = cai; st[(s + 1) * S] = ica; s += 2; }
+        if (mk & Mainen::kKca) { st[s * S] = kca_n; s += 1; }
+        if (mk & Mainen::kKm) { st[s * S] = km_n; s += 1; }
+        if (mk & Mainen::kKv) { st[s * S] = kv_n; s += 1; }
+        if (mk & Mainen::kNa) { st[s * S] = na_m; st[(s + 1) * S] = na_h; s += 2; }
+    }
 }
 
 }  // namespace ngpu

@@ -157,148 +157,148 @@ struct TTPCRates {
     }
 };
 
-// Channel update of one node for one lane.
-//   INIT:  states := steady state at v (AllModels.cu:202-296; cai := 5e-5),
-//          then currents at v.
-//   !INIT: cnexp state update over dt at the new v (nrn_state), then
-//          currents at v with the new states (nrn_current of the next step).
+// Channel update of one node for one lane, in three phases so that all of
+// the node's state and parameter rows are requested from memory at once
+// (one round trip instead of one per mechanism):
+//   load     every state / parameter row of the mechanisms present
+//   compute  INIT:  states := steady state at v (AllModels.cu:202-296;
+//                   cai := 5e-5), then currents at v;
+//            !INIT: cnexp state update over dt at the new v (nrn_state), then
+//                   currents at v with the new states (nrn_current of the next
+//                   step)
+//   store    the updated states (and the Ca current for the next step's
+//            CaDynamics update)
 // st: the node's first state row (row stride 32 elements); pr: its first
-// parameter row.  Returns I (mA/cm2) and G = dI/dv; writes the states back.
+// parameter row.  Returns I (mA/cm2) and G = dI/dv.
 template <typename R, bool INIT>
-NGPU_HD void ttpc_node(uint32_t mk, R v, R dt, R* __restrict__ st,
-                                          const float* __restrict__ pr, R& I, R& G) {
+NGPU_HD void ttpc_node(uint32_t mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,
+                       R& G) {
     using Q = TTPCRates<R>;
     using M = Math<R>;
     constexpr int S = 32;
-    int s = 0, q = 0;
+    // ---------------------------------------------------------------- load
+    R hva_m = 0, hva_h = 0, lva_m = 0, lva_h = 0, cai = 0, ica = 0, ih_m = 0, im_m = 0;
+    R kp_m = 0, kp_h = 0, kt_m = 0, kt_h = 0, nap_m = 0, nap_h = 0, nta_m = 0, nta_h = 0;
+    R nts_m = 0, nts_h = 0, sk_z = 0, skv_m = 0;
+    R g_hva = 0, g_lva = 0, gamma = 0, decay = 1, depth = 1, mincai = 0, g_ih = 0, e_ih = 0;
+    R g_im = 0, g_kp = 0, g_kt = 0, g_nap = 0, g_nta = 0, g_nts = 0, g_pas = 0, e_pas = 0;
+    R g_sk = 0, ztau = 1, g_skv = 0;
+    {
+        int s = 0, q = 0;
+#define LD2(A, B) { if (!INIT) { A = st[s * S]; B = st[(s + 1) * S]; } s += 2; }
+#define LD1(A) { if (!INIT) A = st[s * S]; s += 1; }
+#define P1(A) { A = (R)pr[q * S]; q += 1; }
+        if (mk & TTPC::kCaHVA) { LD2(hva_m, hva_h) P1(g_hva) }
+        if (mk & TTPC::kCaLVA) { LD2(lva_m, lva_h) P1(g_lva) }
+        if (mk & TTPC::kCaDyn) { LD2(cai, ica) P1(gamma) P1(decay) P1(depth) P1(mincai) }
+        if (mk & TTPC::kIh) { LD1(ih_m) P1(g_ih) P1(e_ih) }
+        if (mk & TTPC::kIm) { LD1(im_m) P1(g_im) }
+        if (mk & TTPC::kKP) { LD2(kp_m, kp_h) P1(g_kp) }
+        if (mk & TTPC::kKT) { LD2(kt_m, kt_h) P1(g_kt) }
+        if (mk & TTPC::kNap) { LD2(nap_m, nap_h) P1(g_nap) }
+        if (mk & TTPC::kNaTa) { LD2(nta_m, nta_h) P1(g_nta) }
+        if (mk & TTPC::kNaTs2) { LD2(nts_m, nts_h) P1(g_nts) }
+        if (mk & TTPC::kPas) { P1(g_pas) P1(e_pas) }
+        if (mk & TTPC::kSK) { LD1(sk_z) P1(g_sk) P1(ztau) }
+        if (mk & TTPC::kSKv3) { LD1(skv_m) P1(g_skv) }
+#undef LD2
+#undef LD1
+#undef P1
+    }
+    // ------------------------------------------------------------- compute
     R Itot = 0, Gtot = 0;
     R mi, mr, hi, hr;
-    // ---- Ca gates (their currents need cai, which CaDynamics updates first) ----
-    R hva_m = 0, hva_h = 0, hva_g = 0;
-    if (mk & TTPC::kCaHVA) {
-        hva_g = (R)pr[q * S]; q += 1;
-        Q::ca_hva(v, mi, mr, hi, hr);
-        if (INIT) { hva_m = mi; hva_h = hi; }
-        else {
-            hva_m = cnexp_rate(st[s * S], mi, mr, dt);
-            hva_h = cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        }
-        st[s * S] = hva_m; st[(s + 1) * S] = hva_h; s += 2;
+#define GATE2(M_, H_, CALL)                                                               \
+    {                                                                                     \
+        CALL;                                                                             \
+        if (INIT) { M_ = mi; H_ = hi; }                                                   \
+        else { M_ = cnexp_rate(M_, mi, mr, dt); H_ = cnexp_rate(H_, hi, hr, dt); }        \
     }
-    R lva_m = 0, lva_h = 0, lva_g = 0;
-    if (mk & TTPC::kCaLVA) {
-        lva_g = (R)pr[q * S]; q += 1;
-        Q::ca_lva(v, mi, mr, hi, hr);
-        if (INIT) { lva_m = mi; lva_h = hi; }
-        else {
-            lva_m = cnexp_rate(st[s * S], mi, mr, dt);
-            lva_h = cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        }
-        st[s * S] = lva_m; st[(s + 1) * S] = lva_h; s += 2;
+#define GATE1(M_, CALL)                                                                   \
+    {                                                                                     \
+        CALL;                                                                             \
+        M_ = INIT ? mi : cnexp_rate(M_, mi, mr, dt);                                      \
     }
-    R cai = 0;
-    int ica_row = -1;
-    if (mk & TTPC::kCaDyn) {
-        // AllModels.cu:222-225 (init), :313-317 (cnexp with the previous step's ica)
-        R gamma = (R)pr[q * S], decay = (R)pr[(q + 1) * S];
-        R depth = (R)pr[(q + 2) * S], mincai = (R)pr[(q + 3) * S];
-        q += 4;
+    if (mk & TTPC::kCaHVA) GATE2(hva_m, hva_h, Q::ca_hva(v, mi, mr, hi, hr))
+    if (mk & TTPC::kCaLVA) GATE2(lva_m, lva_h, Q::ca_lva(v, mi, mr, hi, hr))
+    if (mk & TTPC::kCaDyn) {  // AllModels.cu:222-225 (init), :313-317 (cnexp, previous step's ica)
         if (INIT) cai = (R)kDefCai;
         else {
-            R ica = st[(s + 1) * S];
-            R cinf = ((R)(-10000.0 / (2.0 * kFaraday)) * M::dv(ica * gamma, depth) +
-                      M::dv(mincai, decay)) * decay;
-            cai = cnexp_rate(st[s * S], cinf, M::rc(decay), dt);
+            R cinf = ((R)(-10000.0 / (2.0 * kFaraday)) * M::dv(ica * gamma, depth) + M::dv(mincai, decay)) * decay;
+            cai = cnexp_rate(cai, cinf, M::rc(decay), dt);
         }
-        st[s * S] = cai;
-        ica_row = s + 1;
-        s += 2;
     }
     if (mk & TTPC::kIh) {
-        R g = (R)pr[q * S], e = (R)pr[(q + 1) * S]; q += 2;
-        Q::ih(v, mi, mr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        st[s * S] = m; s += 1;
-        R gx = g * m; Itot += gx * (v - e); Gtot += gx;
+        GATE1(ih_m, Q::ih(v, mi, mr))
+        R gx = g_ih * ih_m; Itot += gx * (v - e_ih); Gtot += gx;
     }
     if (mk & TTPC::kIm) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::im(v, mi, mr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        st[s * S] = m; s += 1;
-        R gx = g * m; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
+        GATE1(im_m, Q::im(v, mi, mr))
+        R gx = g_im * im_m; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
     }
     if (mk & TTPC::kKP) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::k_pst(v, mi, mr, hi, hr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        R h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = m; st[(s + 1) * S] = h; s += 2;
-        R gx = g * m * m * h; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
+        GATE2(kp_m, kp_h, Q::k_pst(v, mi, mr, hi, hr))
+        R gx = g_kp * kp_m * kp_m * kp_h; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
     }
     if (mk & TTPC::kKT) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::k_tst(v, mi, mr, hi, hr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        R h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = m; st[(s + 1) * S] = h; s += 2;
-        R m2 = m * m;
-        R gx = g * m2 * m2 * h; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
+        GATE2(kt_m, kt_h, Q::k_tst(v, mi, mr, hi, hr))
+        R m2 = kt_m * kt_m;
+        R gx = g_kt * m2 * m2 * kt_h; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
     }
     if (mk & TTPC::kNap) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::nap(v, mi, mr, hi, hr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        R h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = m; st[(s + 1) * S] = h; s += 2;
-        R gx = g * m * m * m * h; Itot += gx * (v - (R)TTPC::kEna); Gtot += gx;
+        GATE2(nap_m, nap_h, Q::nap(v, mi, mr, hi, hr))
+        R gx = g_nap * nap_m * nap_m * nap_m * nap_h; Itot += gx * (v - (R)TTPC::kEna); Gtot += gx;
     }
     if (mk & TTPC::kNaTa) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::nat(v, (R)-38, (R)-66, mi, mr, hi, hr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        R h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = m; st[(s + 1) * S] = h; s += 2;
-        R gx = g * m * m * m * h; Itot += gx * (v - (R)TTPC::kEna); Gtot += gx;
+        GATE2(nta_m, nta_h, Q::nat(v, (R)-38, (R)-66, mi, mr, hi, hr))
+        R gx = g_nta * nta_m * nta_m * nta_m * nta_h; Itot += gx * (v - (R)TTPC::kEna); Gtot += gx;
     }
     if (mk & TTPC::kNaTs2) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::nat(v, (R)-32, (R)-60, mi, mr, hi, hr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        R h = INIT ? hi : cnexp_rate(st[(s + 1) * S], hi, hr, dt);
-        st[s * S] = m; st[(s + 1) * S] = h; s += 2;
-        R gx = g * m * m * m * h; Itot += gx * (v - (R)TTPC::kEna); Gtot += gx;
+        GATE2(nts_m, nts_h, Q::nat(v, (R)-32, (R)-60, mi, mr, hi, hr))
+        R gx = g_nts * nts_m * nts_m * nts_m * nts_h; Itot += gx * (v - (R)TTPC::kEna); Gtot += gx;
     }
-    if (mk & TTPC::kPas) {
-        R g = (R)pr[q * S], e = (R)pr[(q + 1) * S]; q += 2;
-        Itot += g * (v - e); Gtot += g;
-    }
+    if (mk & TTPC::kPas) { Itot += g_pas * (v - e_pas); Gtot += g_pas; }
     if (mk & TTPC::kSK) {
-        R g = (R)pr[q * S], ztau = (R)pr[(q + 1) * S]; q += 2;
         R zi = Q::sk_zinf(cai);
-        R z = INIT ? zi : cnexp(st[s * S], zi, ztau, dt);
-        st[s * S] = z; s += 1;
-        R gx = g * z; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
+        sk_z = INIT ? zi : cnexp(sk_z, zi, ztau, dt);
+        R gx = g_sk * sk_z; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
     }
     if (mk & TTPC::kSKv3) {
-        R g = (R)pr[q * S]; q += 1;
-        Q::skv3(v, mi, mr);
-        R m = INIT ? mi : cnexp_rate(st[s * S], mi, mr, dt);
-        st[s * S] = m; s += 1;
-        R gx = g * m; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
+        GATE1(skv_m, Q::skv3(v, mi, mr))
+        R gx = g_skv * skv_m; Itot += gx * (v - (R)TTPC::kEk); Gtot += gx;
     }
-    // ---- Ca currents with eca from the updated cai (AllModels.cu:382-407) ----
+#undef GATE2
+#undef GATE1
+    // Ca currents with eca from the updated cai (AllModels.cu:382-407)
+    ica = 0;
     if (mk & (TTPC::kCaHVA | TTPC::kCaLVA)) {
         R eca = (R)(ktf_of(TTPC::kCelsius) / 2) * M::lg(M::dv((R)kDefCao, cai));
-        R gca = hva_g * hva_m * hva_m * hva_h + lva_g * lva_m * lva_m * lva_h;
-        R ica = gca * (v - eca);
+        R gca = g_hva * hva_m * hva_m * hva_h + g_lva * lva_m * lva_m * lva_h;
+        ica = gca * (v - eca);
         Itot += ica; Gtot += gca;
-        if (ica_row >= 0) st[ica_row * S] = ica;
-    } else if (ica_row >= 0) {
-        st[ica_row * S] = (R)0;
     }
     I = Itot;
     G = Gtot;
+    // --------------------------------------------------------------- store
+    {
+        int s = 0;
+#define ST2(A, B) { st[s * S] = A; st[(s + 1) * S] = B; s += 2; }
+#define ST1(A) { st[s * S] = A; s += 1; }
+        if (mk & TTPC::kCaHVA) ST2(hva_m, hva_h)
+        if (mk & TTPC::kCaLVA) ST2(lva_m, lva_h)
+        if (mk & TTPC::kCaDyn) ST2(cai, ica)
+        if (mk & TTPC::kIh) ST1(ih_m)
+        if (mk & TTPC::kIm) ST1(im_m)
+        if (mk & TTPC::kKP) ST2(kp_m, kp_h)
+        if (mk & TTPC::kKT) ST2(kt_m, kt_h)
+        if (mk & TTPC::kNap) ST2(nap_m, nap_h)
+        if (mk & TTPC::kNaTa) ST2(nta_m, nta_h)
+        if (mk & TTPC::kNaTs2) ST2(nts_m, nts_h)
+        if (mk & TTPC::kSK) ST1(sk_z)
+        if (mk & TTPC::kSKv3) ST1(skv_m)
+#undef ST2
+#undef ST1
+    }
 }
 
 }  // namespace ngpu

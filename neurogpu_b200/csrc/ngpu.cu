@@ -16,6 +16,7 @@
 #include <map>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/ngpu.h"
@@ -86,6 +87,14 @@ void* dmalloc(size_t bytes, int* rc) {
     return p;
 }
 
+// Host-side per-node layout of a model.
+struct HostNode {
+    int32_t parent;
+    uint32_t mask;
+    int32_t srow;  // first channel-state row
+    int32_t prow;  // first parameter row
+};
+
 }  // namespace
 
 struct ngpu_model {
@@ -93,93 +102,145 @@ struct ngpu_model {
     std::vector<int> parent, section;
     std::vector<double> a, b, cm;
     std::vector<uint32_t> mask;
-    std::vector<NodeInfo> info;  // rec filled per simulation
+    std::vector<HostNode> info;
     std::vector<int> row_param, row_sec;
     int slab_rows = 0, ptab_rows = 0;
     int64_t state_vars = 0, param_reads = 0;
     std::vector<double> dconst;
     std::vector<int> weight;        // per-node channel cost
     std::vector<int2> rows;         // (state rows, parameter rows) per node
+    std::vector<int> perm, inv;     // internal node -> caller's node, and back
 };
 
-// Split of the tree for one CTA of W warps (see sim_kernels.cuh).
+// Split of the tree for one CTA of W warps (see sim_kernels.cuh).  Nodes are
+// already in heavy-first depth-first order (model creation reorders them), so
+// every heavy path is a run of consecutive nodes.  Separator nodes cut the
+// tree into work items ("components") of at most ~1/W of the channel cost:
+//   plain component    a whole subtree [r, r + size(r)) hanging off separator u
+//   segment component  a heavy-path piece r..l-1 (the spine) ending just above
+//                      a lower separator l, plus the light subtrees of the
+//                      spine nodes, which occupy [l + size(l), r + size(r))
+// The separators form a small tree (the skeleton) that warp 0 solves.
+struct Comp {
+    int r, u, l;          // root, upper separator, lower separator (-1: plain)
+    int lk;               // index of l in the separator list (-1: plain)
+    int light_lo, light_hi;
+    int64_t weight;
+};
+
 struct Partition {
-    std::vector<int2> seg;          // subtree ranges, grouped by warp
-    std::vector<int> seg_off;       // [W+1]
-    std::vector<int> top;           // top-tree nodes ascending
-    std::vector<int> tch, tch_off;  // top nodes whose channels each warp updates
+    std::vector<Comp> comps;        // by decreasing weight (the dynamic schedule order)
+    std::vector<int> seps;          // separator nodes, ascending
+    std::vector<int> sep_par;       // skeleton parent (index into seps), -1 for the root
+    std::vector<int> sep_comp;      // segment component whose lower separator this is, or -1
     std::vector<int> jslot, pslot;
     int n_jslots = 0;
 };
 
 static Partition make_partition(const ngpu_model* m, int W) {
     const int N = m->n;
+    const std::vector<int>& par = m->parent;
     Partition P;
     std::vector<std::vector<int>> kids(N);
-    for (int i = 1; i < N; ++i) kids[m->parent[i]].push_back(i);
+    for (int i = 1; i < N; ++i) kids[par[i]].push_back(i);
     std::vector<int64_t> subw(N, 0);
     std::vector<int> subn(N, 1);
     for (int i = N - 1; i >= 0; --i) {
         subw[i] += m->weight[i];
         if (i > 0) {
-            subw[m->parent[i]] += subw[i];
-            subn[m->parent[i]] += subn[i];
+            subw[par[i]] += subw[i];
+            subn[par[i]] += subn[i];
         }
     }
-    const int64_t total = subw[0];
-    const int64_t target = std::max<int64_t>(1, total / W);
-    std::vector<char> in_top(N, 0);
-    in_top[0] = 1;
-    std::vector<int> cand(kids[0].begin(), kids[0].end());
-    while (!cand.empty()) {
-        size_t best = 0;
-        for (size_t k = 1; k < cand.size(); ++k)
-            if (subw[cand[k]] > subw[cand[best]]) best = k;
-        if (W == 1 || subw[cand[best]] <= target) break;
-        const int c = cand[best];
-        cand.erase(cand.begin() + best);
-        in_top[c] = 1;
-        cand.insert(cand.end(), kids[c].begin(), kids[c].end());
+    auto heavy = [&](int i) { return (i + 1 < N && par[i + 1] == i) ? i + 1 : -1; };
+    const int64_t target = std::max<int64_t>(1, (subw[0] + W - 1) / W);
+    std::vector<char> is_sep(N, 0);
+    is_sep[0] = 1;
+    struct Raw { int r, l; };
+    std::vector<Raw> raw;
+    auto cweight = [&](const Raw& c) { return subw[c.r] - (c.l >= 0 ? subw[c.l] : 0); };
+    for (int c : kids[0]) raw.push_back({c, -1});
+    for (;;) {
+        int best = -1;
+        for (size_t k = 0; k < raw.size(); ++k)
+            if (W > 1 && cweight(raw[k]) > target && (best < 0 || cweight(raw[k]) > cweight(raw[best])))
+                best = (int)k;
+        if (best < 0) break;
+        Raw C = raw[best];
+        raw.erase(raw.begin() + best);
+        // walk the spine from r; cut at the first node whose own cost (itself
+        // plus its light subtrees) would take the part above over the target
+        int64_t acc = 0;
+        int s = C.r;
+        for (int i = C.r;; i = heavy(i)) {
+            int64_t own = m->weight[i];
+            for (int c : kids[i])
+                if (c != heavy(i)) own += subw[c];
+            const int h = heavy(i);
+            if (acc + own > target || h < 0 || h == C.l) { s = i; break; }
+            acc += own;
+        }
+        is_sep[s] = 1;
+        if (s > C.r) raw.push_back({C.r, s});
+        const int h = heavy(s);
+        if (h >= 0 && h != C.l) raw.push_back({h, C.l});
+        for (int c : kids[s])
+            if (c != h) raw.push_back({c, -1});
     }
-    // bin-pack the subtrees (largest first) onto the least-loaded warp
-    std::sort(cand.begin(), cand.end(), [&](int x, int y) { return subw[x] > subw[y]; });
-    std::vector<int64_t> load(W, 0);
-    std::vector<std::vector<int2>> per(W);
-    for (int c : cand) {
-        int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        load[w] += subw[c];
-        per[w].push_back(make_int2(c, c + subn[c]));
-    }
-    // the top nodes' channel work goes to the least-loaded warps as well
     for (int i = 0; i < N; ++i)
-        if (in_top[i]) P.top.push_back(i);
-    std::vector<std::vector<int>> tper(W);
-    for (int i : P.top) {
-        int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        load[w] += m->weight[i];
-        tper[w].push_back(i);
+        if (is_sep[i]) P.seps.push_back(i);
+    std::vector<int> sep_index(N, -1);
+    for (size_t k = 0; k < P.seps.size(); ++k) sep_index[P.seps[k]] = (int)k;
+    for (const Raw& c : raw) {
+        Comp q;
+        q.r = c.r;
+        q.u = par[c.r];
+        q.l = c.l;
+        q.lk = c.l >= 0 ? sep_index[c.l] : -1;
+        if (c.l >= 0) {
+            q.light_lo = c.l + subn[c.l];
+            q.light_hi = c.r + subn[c.r];
+        } else {
+            q.light_lo = c.r;
+            q.light_hi = c.r + subn[c.r];
+        }
+        q.weight = cweight(c);
+        P.comps.push_back(q);
     }
-    P.seg_off.assign(1, 0);
-    P.tch_off.assign(1, 0);
-    for (int w = 0; w < W; ++w) {
-        std::sort(per[w].begin(), per[w].end(), [](int2 x, int2 y) { return x.x < y.x; });
-        P.seg.insert(P.seg.end(), per[w].begin(), per[w].end());
-        P.seg_off.push_back((int)P.seg.size());
-        P.tch.insert(P.tch.end(), tper[w].begin(), tper[w].end());
-        P.tch_off.push_back((int)P.tch.size());
+    std::sort(P.comps.begin(), P.comps.end(), [](const Comp& x, const Comp& y) {
+        return x.weight != y.weight ? x.weight > y.weight : x.r < y.r;
+    });
+    // skeleton links
+    std::vector<int> seg_of_lower(N, -1);
+    for (size_t k = 0; k < P.comps.size(); ++k)
+        if (P.comps[k].l >= 0) seg_of_lower[P.comps[k].l] = (int)k;
+    P.sep_par.assign(P.seps.size(), -1);
+    P.sep_comp.assign(P.seps.size(), -1);
+    for (size_t k = 1; k < P.seps.size(); ++k) {
+        const int sn = P.seps[k];
+        if (is_sep[par[sn]]) {
+            P.sep_par[k] = sep_index[par[sn]];
+        } else {
+            const int ci = seg_of_lower[sn];
+            P.sep_comp[k] = ci;
+            P.sep_par[k] = sep_index[P.comps[ci].u];
+        }
     }
-    // junction slots: parents of a child other than node+1, and top parents of subtree roots
-    std::vector<char> sub_root(N, 0);
-    for (int c : cand) sub_root[c] = 1;
+    // junction slots: every separator; every parent of a child that is not
+    // node+1 or that roots a component
+    std::vector<char> comp_root(N, 0);
+    for (const Comp& c : P.comps) comp_root[c.r] = 1;
     std::vector<char> need(N, 0);
+    for (int i = 0; i < N; ++i)
+        if (is_sep[i]) need[i] = 1;
     for (int i = 1; i < N; ++i)
-        if (m->parent[i] != i - 1 || sub_root[i]) need[m->parent[i]] = 1;
+        if (!is_sep[i] && (par[i] != i - 1 || comp_root[i])) need[par[i]] = 1;
     P.jslot.assign(N, -1);
     P.pslot.assign(N, -1);
     for (int i = 0; i < N; ++i)
         if (need[i]) P.jslot[i] = P.n_jslots++;
     for (int i = 1; i < N; ++i)
-        if (m->parent[i] != i - 1 || sub_root[i]) P.pslot[i] = P.jslot[m->parent[i]];
+        if (!is_sep[i] && (par[i] != i - 1 || comp_root[i])) P.pslot[i] = P.jslot[par[i]];
     return P;
 }
 
@@ -187,18 +248,15 @@ struct ngpu_sim {
     ngpu_model* m = nullptr;
     int n_sets = 0, n_stim = 0, n_inst = 0, n_groups = 0, n_pad = 0, precision = 0;
     // device buffers
-    NodeInfo* d_info = nullptr;
-    void* d_coef = nullptr;
-    void* d_solve = nullptr;
+    void* d_nodes = nullptr;
     void* d_vbuf = nullptr;
     void* d_slab = nullptr;
     float* d_ptab = nullptr;
     void* d_scr = nullptr;
     int* d_err = nullptr;
-    int2* d_rows = nullptr;
-    int2* d_seg = nullptr;
-    int* d_top = nullptr;
-    int* d_tch = nullptr;
+    DevComp* d_comps = nullptr;
+    DevSep* d_seps = nullptr;
+    void* d_sepv = nullptr;
     int n_warps = 1;
     Partition part;
     double* d_jacc = nullptr;
@@ -212,11 +270,11 @@ struct ngpu_sim {
     float* d_trace = nullptr;
     float* d_tmp_out = nullptr;
     size_t tmp_out_bytes = 0;
-    // stimulus / recording
+    // stimulus / recording (internal node numbering)
     int nt = 0, stim_node = 0;
     double stim_scale = 0.0;
-    std::vector<int> rec_nodes;       // as given
-    std::vector<int> rec_cols;        // column of each given site
+    std::vector<int> rec_nodes;       // per requested site
+    std::vector<int> rec_cols;        // column of each requested site
     int n_rec_unique = 0, rec_every = 1, n_samples = 0;
     float v_init = -65.f;
     bool has_params = false, has_stim = false, initialized = false;
@@ -226,10 +284,8 @@ template <typename R>
 static SimArgs<R> make_args(ngpu_sim* s) {
     SimArgs<R> A;
     const ngpu_model* m = s->m;
-    A.info = s->d_info;
-    A.coef = (const NodeCoef<R>*)s->d_coef;
+    A.nodes = (const NodeRec<R>*)s->d_nodes;
     A.n_nodes = m->n;
-    A.solve = (const SolveNode<R>*)s->d_solve;
     A.vbuf = (R*)s->d_vbuf;
     A.slab = (R*)s->d_slab;
     A.slab_rows = m->slab_rows;
@@ -253,16 +309,11 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.bad = s->d_bad;
     A.err = s->d_err;
     A.n_warps = s->n_warps;
-    A.rows = s->d_rows;
-    A.seg = s->d_seg;
-    A.top = s->d_top;
-    A.n_top = (int)s->part.top.size();
-    A.tch = s->d_tch;
-    for (int w = 0; w <= kMaxWarps; ++w) {
-        const int ww = std::min(w, s->n_warps);
-        A.seg_off[w] = s->part.seg_off[ww];
-        A.tch_off[w] = s->part.tch_off[ww];
-    }
+    A.comps = s->d_comps;
+    A.n_comps = (int)s->part.comps.size();
+    A.seps = s->d_seps;
+    A.n_seps = (int)s->part.seps.size();
+    A.sepv = (R*)s->d_sepv;
     return A;
 }
 
@@ -335,26 +386,69 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
         if (!std::isfinite(a[i]) || !std::isfinite(b[i]) || !std::isfinite(cm[i]) || cm[i] < 0)
             return fail(NGPU_E_INVALID, "non-finite coefficient at node " + std::to_string(i));
     }
+    if (n_nodes > 32767) return fail(NGPU_E_INVALID, "at most 32767 nodes per morphology");
+    if (NM > 16) return fail(NGPU_E_INVALID, "at most 16 mechanisms per set");
+    // Internal node order: heavy-first depth-first (children by decreasing
+    // channel-cost subtree weight), so heavy paths are runs of consecutive
+    // nodes.  Any Hines order the caller gives is accepted; stimulus and
+    // recording nodes are mapped through the permutation.
+    std::vector<uint32_t> mask0(n_nodes, 0u);
+    for (int k = 0; k < NM; ++k)
+        for (int i = 0; i < n_nodes; ++i)
+            if (mech_mask[(size_t)k * n_nodes + i]) mask0[i] |= (1u << k);
+    std::vector<int64_t> subw(n_nodes, 0);
+    for (int i = n_nodes - 1; i >= 0; --i) {
+        int wt = 12;
+        for (int k = 0; k < NM; ++k)
+            if (mask0[i] & (1u << k)) wt += sd.mechs[k].cost;
+        subw[i] += wt;
+        if (i > 0) subw[parent[i]] += subw[i];
+    }
+    std::vector<std::vector<int>> kids(n_nodes);
+    for (int i = 1; i < n_nodes; ++i) kids[parent[i]].push_back(i);
+    std::vector<int> order;
+    order.reserve(n_nodes);
+    {
+        std::vector<int> stack{0};
+        while (!stack.empty()) {
+            const int v = stack.back();
+            stack.pop_back();
+            order.push_back(v);
+            std::vector<int> ks = kids[v];
+            std::stable_sort(ks.begin(), ks.end(), [&](int x, int y) { return subw[x] > subw[y]; });
+            for (auto it = ks.rbegin(); it != ks.rend(); ++it) stack.push_back(*it);
+        }
+    }
     ngpu_model* m = new (std::nothrow) ngpu_model();
     if (!m) return fail(NGPU_E_NOMEM, "host allocation failed");
+    m->perm = order;
+    m->inv.assign(n_nodes, 0);
+    for (int i = 0; i < n_nodes; ++i) m->inv[order[i]] = i;
     m->n = n_nodes;
     m->n_sections = n_sections;
     m->mechset = mechset;
     m->n_mech = NM;
     m->n_params = sd.n_params;
-    m->parent.assign(parent, parent + n_nodes);
-    m->section.assign(section, section + n_nodes);
-    m->a.assign(a, a + n_nodes);
-    m->b.assign(b, b + n_nodes);
-    m->cm.assign(cm, cm + n_nodes);
-    m->mask.assign(n_nodes, 0u);
-    for (int k = 0; k < NM; ++k)
-        for (int i = 0; i < n_nodes; ++i)
-            if (mech_mask[(size_t)k * n_nodes + i]) m->mask[i] |= (1u << k);
+    m->parent.resize(n_nodes);
+    m->section.resize(n_nodes);
+    m->a.resize(n_nodes);
+    m->b.resize(n_nodes);
+    m->cm.resize(n_nodes);
+    m->mask.resize(n_nodes);
+    for (int i = 0; i < n_nodes; ++i) {
+        const int o = order[i];
+        m->parent[i] = i == 0 ? -1 : m->inv[parent[o]];
+        m->section[i] = section[o];
+        m->a[i] = a[o];
+        m->b[i] = b[o];
+        m->cm[i] = cm[o];
+        m->mask[i] = mask0[o];
+    }
     for (int i = 0; i < n_nodes; ++i) {
         if ((m->mask[i] & sd.needs_ca_dyn) && !(m->mask[i] & sd.ca_dyn_bit)) {
+            const int o = order[i];
             delete m;
-            return fail(NGPU_E_INVALID, "node " + std::to_string(i) +
+            return fail(NGPU_E_INVALID, "node " + std::to_string(o) +
                                             " has a calcium current without calcium dynamics "
                                             "(its reversal potential would be infinite)");
         }
@@ -363,14 +457,14 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
     m->dconst.assign(n_nodes, 0.0);
     for (int i = 0; i < n_nodes; ++i) m->dconst[i] = -m->a[i];
     m->dconst[0] = 0.0;  // the root has no parent coupling
-    for (int i = 1; i < n_nodes; ++i) m->dconst[parent[i]] -= m->b[i];
+    for (int i = 1; i < n_nodes; ++i) m->dconst[m->parent[i]] -= m->b[i];
     // state and parameter rows
     std::map<std::pair<int, uint32_t>, int> prow_of;
     m->info.resize(n_nodes);
     int srow = 0;
     for (int i = 0; i < n_nodes; ++i) {
-        NodeInfo& ni = m->info[i];
-        ni.parent = parent[i];
+        HostNode& ni = m->info[i];
+        ni.parent = m->parent[i];
         ni.mask = m->mask[i];
         ni.srow = srow;
         int srows = 0, wt = 12;
@@ -385,24 +479,24 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
         m->weight.push_back(wt);
         m->state_vars += srows;
         m->param_reads += (int64_t)plist.size();
-        auto key = std::make_pair(section[i], ni.mask);
+        auto key = std::make_pair(m->section[i], ni.mask);
         auto it = prow_of.find(key);
         if (it == prow_of.end()) {
             int first = (int)m->row_param.size();
             for (int p : plist) {
                 m->row_param.push_back(p);
-                m->row_sec.push_back(section[i]);
+                m->row_sec.push_back(m->section[i]);
             }
             it = prow_of.emplace(key, first).first;
         }
         ni.prow = it->second;
-        ni.jslot = -1;
-        ni.pslot = -1;
-        ni.rec = -1;
-        ni.pad = 0;
         m->rows.push_back(make_int2(srows, (int)plist.size()));
     }
     m->slab_rows = std::max(1, srow);
+    if (m->row_param.size() > 65535) {
+        delete m;
+        return fail(NGPU_E_INVALID, "too many distinct parameter rows (more than 65535)");
+    }
     m->ptab_rows = std::max(1, (int)m->row_param.size());
     if (m->row_param.empty()) {
         m->row_param.push_back(0);
@@ -428,33 +522,64 @@ int ngpu_model_layout(const ngpu_model* m, int32_t* state_rows, int32_t* param_r
     return NGPU_OK;
 }
 
-int ngpu_model_partition(const ngpu_model* m, int32_t n_warps, int32_t* top_flag, int32_t* owner,
+int ngpu_model_partition(const ngpu_model* m, int32_t n_warps, int32_t* sep_flag, int32_t* item,
                          int32_t* jslot, int32_t* pslot, int32_t* n_jslots) {
     if (!m) return fail(NGPU_E_INVALID, "null model");
     if (n_warps < 1 || n_warps > kMaxWarps) return fail(NGPU_E_INVALID, "n_warps out of range");
     Partition P = make_partition(m, n_warps);
+    std::vector<int> owner(m->n, -1), sep(m->n, 0);
+    for (int i : P.seps) sep[i] = 1;
+    for (size_t k = 0; k < P.comps.size(); ++k) {
+        const Comp& c = P.comps[k];
+        if (c.l >= 0)
+            for (int i = c.r; i < c.l; ++i) owner[i] = (int)k;
+        for (int i = c.light_lo; i < c.light_hi; ++i) owner[i] = (int)k;
+    }
+    for (int j = 0; j < m->n; ++j) {  // j: node in the caller's numbering
+        const int i = m->inv[j];
+        if (sep_flag) sep_flag[j] = sep[i];
+        if (item) item[j] = owner[i];
+        if (jslot) jslot[j] = P.jslot[i];
+        if (pslot) pslot[j] = P.pslot[i];
+    }
+    if (n_jslots) *n_jslots = P.n_jslots;
+    return NGPU_OK;
+}
+
+int ngpu_model_split_info(const ngpu_model* m, int32_t n_warps, int32_t* perm, int32_t* n_comps,
+                          int32_t* comps, int32_t max_comps, int32_t* n_seps, int32_t* seps,
+                          int32_t max_seps, int32_t* jslot, int32_t* pslot) {
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    if (n_warps < 1 || n_warps > kMaxWarps) return fail(NGPU_E_INVALID, "n_warps out of range");
+    Partition P = make_partition(m, n_warps);
+    if (perm)
+        for (int i = 0; i < m->n; ++i) perm[i] = m->perm[i];
+    if (n_comps) *n_comps = (int32_t)P.comps.size();
+    if (n_seps) *n_seps = (int32_t)P.seps.size();
+    if (comps)
+        for (int k = 0; k < (int)P.comps.size() && k < max_comps; ++k) {
+            const Comp& c = P.comps[k];
+            const int32_t v[6] = {c.r, c.u, c.l, c.lk, c.light_lo, c.light_hi};
+            for (int j = 0; j < 6; ++j) comps[6 * k + j] = v[j];
+        }
+    if (seps)
+        for (int k = 0; k < (int)P.seps.size() && k < max_seps; ++k) {
+            seps[3 * k] = P.seps[k];
+            seps[3 * k + 1] = P.sep_par[k];
+            seps[3 * k + 2] = P.sep_comp[k];
+        }
     for (int i = 0; i < m->n; ++i) {
-        if (top_flag) top_flag[i] = 0;
-        if (owner) owner[i] = -1;
         if (jslot) jslot[i] = P.jslot[i];
         if (pslot) pslot[i] = P.pslot[i];
     }
-    for (int i : P.top)
-        if (top_flag) top_flag[i] = 1;
-    for (int w = 0; w < n_warps; ++w)
-        for (int k = P.seg_off[w]; k < P.seg_off[w + 1]; ++k)
-            for (int i = P.seg[k].x; i < P.seg[k].y; ++i)
-                if (owner) owner[i] = w;
-    if (n_jslots) *n_jslots = P.n_jslots;
     return NGPU_OK;
 }
 
 static void sim_free(ngpu_sim* s) {
     if (!s) return;
-    void* ptrs[] = {s->d_info, s->d_coef, s->d_solve, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr,
-                    s->d_jacc, s->d_jx, s->d_inst_stim, s->d_bad, s->d_err, s->d_row_param,
-                    s->d_row_sec, s->d_amps, s->d_dts, s->d_trace, s->d_tmp_out, s->d_rows,
-                    s->d_seg, s->d_top, s->d_tch};
+    void* ptrs[] = {s->d_nodes, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc, s->d_jx,
+                    s->d_inst_stim, s->d_bad, s->d_err, s->d_row_param, s->d_row_sec, s->d_amps,
+                    s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete s;
@@ -500,9 +625,7 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
         sim_free(s);                                           \
         return rc;                                             \
     }
-    ALLOC(d_info, NodeInfo*, sizeof(NodeInfo) * m->n);
-    ALLOC(d_coef, void*, 4 * esz * m->n);
-    ALLOC(d_solve, void*, (precision == NGPU_FP64 ? sizeof(SolveNode<double>) : sizeof(SolveNode<float>)) * m->n);
+    ALLOC(d_nodes, void*, (precision == NGPU_FP64 ? sizeof(NodeRec<double>) : sizeof(NodeRec<float>)) * m->n);
     ALLOC(d_vbuf, void*, G * 2 * m->n * L * esz);
     ALLOC(d_slab, void*, G * m->slab_rows * L * esz);
     ALLOC(d_ptab, float*, G * m->ptab_rows * L * sizeof(float));
@@ -510,41 +633,23 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
     ALLOC(d_jacc, double*, G * 2 * std::max(1, nj) * L * sizeof(double));
     ALLOC(d_jx, void*, G * std::max(1, nj) * L * esz);
     ALLOC(d_err, int*, sizeof(int));
-    ALLOC(d_rows, int2*, sizeof(int2) * m->n);
-    ALLOC(d_seg, int2*, sizeof(int2) * std::max<size_t>(1, s->part.seg.size()));
-    ALLOC(d_top, int*, sizeof(int) * std::max<size_t>(1, s->part.top.size()));
-    ALLOC(d_tch, int*, sizeof(int) * std::max<size_t>(1, s->part.tch.size()));
+    ALLOC(d_comps, DevComp*, sizeof(DevComp) * std::max<size_t>(1, s->part.comps.size()));
+    ALLOC(d_seps, DevSep*, sizeof(DevSep) * std::max<size_t>(1, s->part.seps.size()));
+    ALLOC(d_sepv, void*, G * 4 * std::max<size_t>(1, s->part.seps.size()) * L * esz);
     ALLOC(d_inst_stim, int*, sizeof(int) * s->n_pad);
     ALLOC(d_bad, int*, sizeof(int) * s->n_pad);
     ALLOC(d_row_param, int*, sizeof(int) * m->row_param.size());
     ALLOC(d_row_sec, int*, sizeof(int) * m->row_sec.size());
 #undef ALLOC
-    // coefficients and the phase-S topology in the run's precision
-    if (precision == NGPU_FP64) {
-        std::vector<NodeCoef<double>> c(m->n);
-        std::vector<SolveNode<double>> sv(m->n);
-        for (int i = 0; i < m->n; ++i) {
-            c[i] = {m->a[i], m->b[i], m->dconst[i], m->cm[i] / 1000.0};
-            sv[i] = {m->a[i], m->b[i], s->part.jslot[i], s->part.pslot[i]};
-        }
-        cudaMemcpy(s->d_coef, c.data(), sizeof(c[0]) * m->n, cudaMemcpyHostToDevice);
-        cudaMemcpy(s->d_solve, sv.data(), sizeof(sv[0]) * m->n, cudaMemcpyHostToDevice);
-    } else {
-        std::vector<NodeCoef<float>> c(m->n);
-        std::vector<SolveNode<float>> sv(m->n);
-        for (int i = 0; i < m->n; ++i) {
-            c[i] = {(float)m->a[i], (float)m->b[i], (float)m->dconst[i], (float)(m->cm[i] / 1000.0)};
-            sv[i] = {(float)m->a[i], (float)m->b[i], s->part.jslot[i], s->part.pslot[i]};
-        }
-        cudaMemcpy(s->d_coef, c.data(), sizeof(c[0]) * m->n, cudaMemcpyHostToDevice);
-        cudaMemcpy(s->d_solve, sv.data(), sizeof(sv[0]) * m->n, cudaMemcpyHostToDevice);
+    {
+        std::vector<DevComp> dc;
+        for (const Comp& c : s->part.comps) dc.push_back({c.r, c.u, c.l, c.lk, c.light_lo, c.light_hi});
+        std::vector<DevSep> ds;
+        for (size_t k = 0; k < s->part.seps.size(); ++k)
+            ds.push_back({s->part.seps[k], s->part.sep_par[k], s->part.sep_comp[k], 0});
+        if (!dc.empty()) cudaMemcpy(s->d_comps, dc.data(), sizeof(DevComp) * dc.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(s->d_seps, ds.data(), sizeof(DevSep) * ds.size(), cudaMemcpyHostToDevice);
     }
-    cudaMemcpy(s->d_rows, m->rows.data(), sizeof(int2) * m->n, cudaMemcpyHostToDevice);
-    if (!s->part.seg.empty())
-        cudaMemcpy(s->d_seg, s->part.seg.data(), sizeof(int2) * s->part.seg.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(s->d_top, s->part.top.data(), sizeof(int) * s->part.top.size(), cudaMemcpyHostToDevice);
-    if (!s->part.tch.empty())
-        cudaMemcpy(s->d_tch, s->part.tch.data(), sizeof(int) * s->part.tch.size(), cudaMemcpyHostToDevice);
     cudaMemset(s->d_err, 0, sizeof(int));
     std::vector<int> inst_stim(s->n_pad);
     for (int k = 0; k < s->n_pad; ++k) inst_stim[k] = std::min(k, s->n_inst - 1) % n_stim;
@@ -629,7 +734,7 @@ int ngpu_sim_set_stimulus(ngpu_sim* s, int32_t nt, const float* amps, const floa
     NGPU_CUDA(cudaMemcpy(s->d_amps, amps, sizeof(float) * (size_t)nt * s->n_stim, kind));
     NGPU_CUDA(cudaMemcpy(s->d_dts, dts, sizeof(float) * (size_t)nt, kind));
     s->nt = nt;
-    s->stim_node = stim_node;
+    s->stim_node = s->m->inv[stim_node];
     s->stim_scale = 100.0 / (double)stim_area_um2;
     s->has_stim = true;
     s->initialized = false;
@@ -653,7 +758,8 @@ int ngpu_sim_set_recording(ngpu_sim* s, int32_t n_rec, const int32_t* rec_nodes,
             cols[r] = (int)(it - uniq.begin());
         }
     }
-    s->rec_nodes.assign(rec_nodes, rec_nodes + n_rec);
+    s->rec_nodes.assign(n_rec, 0);
+    for (int r = 0; r < n_rec; ++r) s->rec_nodes[r] = s->m->inv[rec_nodes[r]];
     s->rec_cols = cols;
     s->n_rec_unique = (int)uniq.size();
     s->rec_every = rec_every;
@@ -668,16 +774,39 @@ int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
     if (!std::isfinite(v_init)) return fail(NGPU_E_INVALID, "v_init must be finite");
     cudaStream_t st = (cudaStream_t)cuda_stream;
     const ngpu_model* m = s->m;
-    // node table with this run's recording columns
-    std::vector<NodeInfo> info = m->info;
-    for (int i = 0; i < m->n; ++i) {
-        info[i].jslot = s->part.jslot[i];
-        info[i].pslot = s->part.pslot[i];
-    }
+    // node records with this run's split and recording columns
     std::vector<int> uniq(s->n_rec_unique, -1);
     for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
-    for (int c = 0; c < s->n_rec_unique; ++c) info[uniq[c]].rec = c;
-    NGPU_CUDA(cudaMemcpyAsync(s->d_info, info.data(), sizeof(NodeInfo) * m->n, cudaMemcpyHostToDevice, st));
+    std::vector<int> rec(m->n, -1);
+    for (int c = 0; c < s->n_rec_unique; ++c) rec[uniq[c]] = c;
+    auto fill = [&](auto* recs) {
+        for (int i = 0; i < m->n; ++i) {
+            auto& q = recs[i];
+            using RT = std::remove_reference_t<decltype(q.a)>;
+            q.a = (RT)m->a[i];
+            q.b = (RT)m->b[i];
+            q.dconst = (RT)m->dconst[i];
+            q.cm = (RT)(m->cm[i] / 1000.0);
+            q.srow = m->info[i].srow;
+            q.parent = (int16_t)m->parent[i];
+            q.jslot = (int16_t)s->part.jslot[i];
+            q.pslot = (int16_t)s->part.pslot[i];
+            q.rec = (int16_t)rec[i];
+            q.mask = (uint16_t)m->mask[i];
+            q.prow = (uint16_t)m->info[i].prow;
+            q.srows = (uint16_t)m->rows[i].x;
+            q.prows = (uint16_t)m->rows[i].y;
+        }
+    };
+    if (s->precision == NGPU_FP64) {
+        std::vector<NodeRec<double>> recs(m->n);
+        fill(recs.data());
+        NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<NodeRec<float>> recs(m->n);
+        fill(recs.data());
+        NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
+    }
     s->n_samples = (s->nt + s->rec_every - 1) / s->rec_every;
     if (s->d_trace) cudaFree(s->d_trace);
     s->d_trace = nullptr;

@@ -40,38 +40,46 @@
 namespace ngpu {
 
 constexpr int kLanes = 32;
-constexpr int kMaxWarps = 16;
+constexpr int kMaxWarps = 8;   // 256 threads; with 3 CTAs per SM the 85-register cap keeps a whole batch resident
+#ifndef NGPU_ADV_MIN_BLOCKS
+#define NGPU_ADV_MIN_BLOCKS 3
+#endif
 
-struct NodeInfo {
-    int32_t parent;  // -1 for the root
-    uint32_t mask;   // mechanism bits
+// Per-node record, identical for every instance; staged in shared memory
+// once per launch (36 bytes in FP32).
+template <typename R>
+struct NodeRec {
+    R a;        // row i, column parent(i)
+    R b;        // row parent(i), column i
+    R dconst;   // -a_i - sum over children c of b_c
+    R cm;       // cm_i / 1000  (uF/cm2 -> mA/cm2/mV per 1/ms)
     int32_t srow;    // first channel-state row in slab
-    int32_t prow;    // first parameter row
-    int32_t jslot;   // junction slot if this node has a child other than node+1, else -1
-    int32_t pslot;   // the parent's junction slot if parent != node-1, else -1
-    int32_t rec;     // recording column or -1
-    int32_t pad;
+    int16_t parent;  // -1 for the root
+    int16_t jslot;   // junction slot of this node, or -1
+    int16_t pslot;   // the parent's junction slot if this node is a far child / subtree root
+    int16_t rec;     // recording column or -1
+    uint16_t mask;   // mechanism bits
+    uint16_t prow;   // first parameter row
+    uint16_t srows;  // number of state rows
+    uint16_t prows;  // number of parameter rows
 };
 
-template <typename R>
-struct NodeCoef {
-    R a;       // row i, column parent(i)
-    R b;       // row parent(i), column i
-    R dconst;  // -a_i - sum over children c of b_c
-    R cm;      // cm_i / 1000  (uF/cm2 -> mA/cm2/mV per 1/ms)
+// A work item of the split (see make_partition on the host): a plain
+// subtree [r, r + size) hanging off separator u, or a segment: spine r..l-1
+// just above lower separator l plus the spine's light subtrees [lo, hi).
+struct DevComp {
+    int r, u, l, lk;   // root, upper separator, lower separator (-1 plain), l's skeleton index
+    int lo, hi;        // light node range (plain: the whole subtree)
 };
-
-template <typename R>
-struct SolveNode {  // phase-S topology, staged in shared memory
-    R a, b;
-    int32_t jslot, pslot;
+// A separator: node, skeleton parent (index) and, for a lower separator, the
+// segment item that links it to its skeleton parent (-1: direct tree edge).
+struct DevSep {
+    int node, par, seg, pad;
 };
 
 template <typename R>
 struct SimArgs {
-    const NodeInfo* info;
-    const NodeCoef<R>* coef;
-    const SolveNode<R>* solve;
+    const NodeRec<R>* nodes;  // [N], staged into shared memory by every CTA
     int n_nodes;
     R* vbuf;
     R* slab;
@@ -96,13 +104,11 @@ struct SimArgs {
     int* bad;              // [n_inst_pad] non-finite voltage flags
     int* err;              // device error word
     int n_warps;
-    const int2* rows;      // [N] (state rows, parameter rows) per node, for prefetch
-    const int2* seg;       // subtree node ranges [start, end), grouped by warp
-    int seg_off[kMaxWarps + 1];
-    const int* top;        // top-tree nodes, ascending
-    int n_top;
-    const int* tch;        // top nodes whose channels each warp updates
-    int tch_off[kMaxWarps + 1];
+    const DevComp* comps;  // work items, by decreasing cost
+    int n_comps;
+    const DevSep* seps;    // skeleton, ascending node index
+    int n_seps;
+    R* sepv;               // [n_seps][4] rows per group: A, B, dd, drhs of segment links
 };
 
 template <typename R, int MS, bool INIT>
@@ -129,6 +135,7 @@ struct Group {  // per-CTA pointers (lane offset included)
     R* scr;
     double* jacc;
     R* jx;
+    R* sepv;
     int inst;
 };
 
@@ -143,14 +150,15 @@ __device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A) {
     p.scr = A.scr + (size_t)g * N * 3 * kLanes + lane;
     p.jacc = A.jacc + (size_t)g * 2 * A.n_jslots * kLanes + lane;
     p.jx = A.jx + (size_t)g * A.n_jslots * kLanes + lane;
+    p.sepv = A.sepv + (size_t)g * 4 * A.n_seps * kLanes + lane;
     p.inst = g * kLanes + lane;
     return p;
 }
 
-// Shared memory: the solve topology of every node.
+// Shared memory: the node records.
 template <typename R>
 struct SmemPlan {
-    static size_t bytes(int n_nodes) { return sizeof(SolveNode<R>) * (size_t)n_nodes; }
+    static size_t bytes(int n_nodes) { return sizeof(NodeRec<R>) * (size_t)n_nodes; }
 };
 
 // Bulk prefetch of a run of rows into L2 (one instruction per contiguous block).
@@ -159,22 +167,21 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 }
 
 template <typename R>
-__device__ __forceinline__ void prefetch_node(const SimArgs<R>& A, const Group<R>& G, int i, int lane) {
+__device__ __forceinline__ void prefetch_node(const Group<R>& G, const NodeRec<R>& n, int i) {
+    const int lane = threadIdx.x & 31;
     if (lane == 0) {
-        const NodeInfo ni = A.info[i];
-        const int2 rows = A.rows[i];  // (state rows, parameter rows) of node i
         prefetch_l2(G.scr - lane + (size_t)i * 3 * kLanes, 3 * kLanes * sizeof(R));
         prefetch_l2(G.vbuf - lane + (size_t)i * 2 * kLanes, 2 * kLanes * sizeof(R));
-        if (rows.x) prefetch_l2(G.slab - lane + (size_t)ni.srow * kLanes, rows.x * kLanes * sizeof(R));
-        if (rows.y) prefetch_l2(G.ptab - lane + (size_t)ni.prow * kLanes, rows.y * kLanes * sizeof(float));
+        if (n.srows) prefetch_l2(G.slab - lane + (size_t)n.srow * kLanes, n.srows * kLanes * sizeof(R));
+        if (n.prows) prefetch_l2(G.ptab - lane + (size_t)n.prow * kLanes, n.prows * kLanes * sizeof(float));
     }
 }
 
-// Elimination of node i given its (d, rhs, e) rows; updates the chain carry
-// or the parent's junction accumulator, writes (r, c).
+// Elimination of node i given its (d, rhs, e); updates the chain carry or the
+// parent's FP64 junction accumulator, writes (r, c).
 template <typename R>
-__device__ __forceinline__ void eliminate_node(const Group<R>& G, const SolveNode<R>& s, int i, R d0,
-                                               R r0, R e0, R& carry_d, R& carry_r) {
+__device__ __forceinline__ void eliminate_node(const Group<R>& G, const NodeRec<R>& s, int i, R d0, R r0,
+                                               R e0, R& carry_d, R& carry_r) {
     using M = Math<R>;
     R d, r;
     if (s.jslot >= 0) {
@@ -211,67 +218,79 @@ __device__ __forceinline__ void eliminate_node(const Group<R>& G, const SolveNod
     }
 }
 
-// Leaf -> root elimination over nodes [lo, hi), with the next rows loaded
-// one node ahead.
-template <typename R>
-__device__ __forceinline__ void eliminate_range(const Group<R>& G, const SolveNode<R>* sn, int lo, int hi) {
+// Leaf -> root elimination over the nodes idx(hi-1) .. idx(lo) of a list
+// (a node range or the top-tree list), with rows read two nodes ahead.
+template <typename R, typename Idx>
+__device__ __forceinline__ void eliminate_list(const Group<R>& G, const NodeRec<R>* nr, int lo, int hi, Idx idx) {
     if (hi <= lo) return;
     R carry_d = 0, carry_r = 0;
-    const R* row = G.scr + (size_t)(hi - 1) * 3 * kLanes;
-    R d = row[0], r = row[kLanes], e = row[2 * kLanes];
-    for (int i = hi - 1; i >= lo; --i) {
-        R dn = 0, rn = 0, en = 0;
-        if (i > lo) {
-            const R* nx = G.scr + (size_t)(i - 1) * 3 * kLanes;
-            dn = nx[0];
-            rn = nx[kLanes];
-            en = nx[2 * kLanes];
+    auto load = [&](int k, R& d, R& r, R& e) {
+        if (k >= lo) {
+            const R* row = G.scr + (size_t)idx(k) * 3 * kLanes;
+            d = row[0];
+            r = row[kLanes];
+            e = row[2 * kLanes];
         }
-        eliminate_node(G, sn[i], i, d, r, e, carry_d, carry_r);
-        d = dn;
-        r = rn;
-        e = en;
+    };
+    R d0 = 0, r0 = 0, e0 = 0, d1 = 0, r1 = 0, e1 = 0;
+    load(hi - 1, d0, r0, e0);
+    load(hi - 2, d1, r1, e1);
+    for (int k = hi - 1; k >= lo; --k) {
+        R d2 = 0, r2 = 0, e2 = 0;
+        load(k - 2, d2, r2, e2);
+        const int i = idx(k);
+        eliminate_node(G, nr[i], i, d0, r0, e0, carry_d, carry_r);
+        d0 = d1; r0 = r1; e0 = e1;
+        d1 = d2; r1 = r2; e1 = e2;
     }
 }
 
-// One node of the fused root -> leaf pass: back-substitution, V update
-// (BACKSUB), channel update at the new V, next-step assembly.
+// One node of the fused root -> leaf pass: back-substitution and V update
+// (BACKSUB), channel update at the new V, next-step assembly.  Every store
+// is issued after the channel code so that its loads (one round trip for all
+// of the node's rows) are not held back behind them.
 template <typename R, int MS, bool INIT, bool BACKSUB>
-__device__ __forceinline__ void update_node(const SimArgs<R>& A, const Group<R>& G, const SolveNode<R>& s,
+__device__ __forceinline__ void update_node(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n,
                                             int i, R dt, R dtn_inv, R istim_amp, bool rec_now,
-                                            float* trace, R& x_prev) {
-    const NodeInfo ni = A.info[i];
-    const NodeCoef<R> c = A.coef[i];
+                                            float* trace, R& x_prev, R& v_prev, const R* x_given) {
     R* vo = G.vbuf + (size_t)i * 2 * kLanes;
     R* o = G.scr + (size_t)i * 3 * kLanes;
-    R V;
+    R V, vc = 0, x = 0;
     if (INIT) {
         V = (R)A.v_init;
-        vo[0] = V;
-        vo[kLanes] = 0;
     } else if (BACKSUB) {
-        const R xp = (i == 0) ? (R)0 : (s.pslot < 0 ? x_prev : G.jx[(size_t)s.pslot * kLanes]);
-        const R x = o[0] - o[kLanes] * xp;
-        if (s.jslot >= 0) G.jx[(size_t)s.jslot * kLanes] = x;
-        x_prev = x;
         V = vo[0];
-        R vc = vo[kLanes];
+        vc = vo[kLanes];
+        if (x_given) {
+            x = *x_given;
+        } else {
+            const R r = o[0], c = o[kLanes];
+            const R xp = (i == 0) ? (R)0 : (n.pslot < 0 ? x_prev : G.jx[(size_t)n.pslot * kLanes]);
+            x = r - c * xp;
+        }
+        x_prev = x;
         kahan_add(V, vc, x);
-        vo[0] = V;
-        vo[kLanes] = vc;
     } else {
         V = vo[0];
     }
-    const R vp = INIT ? V : ((i == 0) ? V : G.vbuf[(size_t)ni.parent * 2 * kLanes]);
+    // parent's new V: the previous node's for a chain child of this pass
+    const R vp = INIT || i == 0 ? V
+                 : (BACKSUB && n.pslot < 0) ? v_prev : G.vbuf[(size_t)n.parent * 2 * kLanes];
+    v_prev = V;
     R I, Gm;
-    channels<R, MS, INIT>(ni.mask, V, dt, G.slab + (size_t)ni.srow * kLanes, G.ptab + (size_t)ni.prow * kLanes,
+    channels<R, MS, INIT>(n.mask, V, dt, G.slab + (size_t)n.srow * kLanes, G.ptab + (size_t)n.prow * kLanes,
                           I, Gm);
+    if (INIT || BACKSUB) {
+        vo[0] = V;
+        vo[kLanes] = vc;
+    }
+    if (BACKSUB && n.jslot >= 0) G.jx[(size_t)n.jslot * kLanes] = x;
     const R istim = (i == A.stim_node) ? istim_amp : (R)0;
     const R dvp = vp - V;
-    o[0] = Gm + c.cm * dtn_inv + c.dconst;
-    o[kLanes] = istim - I - c.a * dvp;
-    o[2 * kLanes] = c.b * dvp;
-    if (rec_now && ni.rec >= 0) trace[(size_t)ni.rec * A.n_inst_pad] = (float)V;
+    o[0] = Gm + n.cm * dtn_inv + n.dconst;
+    o[kLanes] = istim - I - n.a * dvp;
+    o[2 * kLanes] = n.b * dvp;
+    if (rec_now && n.rec >= 0) trace[(size_t)n.rec * A.n_inst_pad] = (float)V;
 }
 
 template <typename R>
@@ -288,10 +307,11 @@ __device__ __forceinline__ void step_inputs(const SimArgs<R>& A, const Group<R>&
 }
 
 template <typename R>
-__device__ __forceinline__ void stage_solve_topology(const SimArgs<R>& A, char* smem) {
-    SolveNode<R>* sn = (SolveNode<R>*)smem;
-    for (int i = threadIdx.x; i < A.n_nodes; i += blockDim.x) sn[i] = A.solve[i];
+__device__ __forceinline__ const NodeRec<R>* stage_nodes(const SimArgs<R>& A, char* smem) {
+    NodeRec<R>* nr = (NodeRec<R>*)smem;
+    for (int i = threadIdx.x; i < A.n_nodes; i += blockDim.x) nr[i] = A.nodes[i];
     __syncthreads();
+    return nr;
 }
 
 template <typename R, int MS>
@@ -304,82 +324,214 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
     bool rec_now;
     float* trace;
     step_inputs(A, G, 0, true, dt, dtn_inv, istim_amp, rec_now, trace);
-    R xd = 0;
-    const SolveNode<R> none{};
+    R xd = 0, vd = 0;
     for (int i = w; i < A.n_nodes; i += A.n_warps)
-        update_node<R, MS, true, false>(A, G, none, i, dt, dtn_inv, istim_amp, rec_now, trace, xd);
+        update_node<R, MS, true, false>(A, G, A.nodes[i], i, dt, dtn_inv, istim_amp, rec_now, trace, xd, vd,
+                                        nullptr);
     if (w == 0) A.bad[G.inst] = 0;
 }
 
-// Per timestep:
-//   S1  every warp: leaf -> root elimination of its subtrees (they hang off
-//       the top tree, so no two warps touch the same node; contributions of
-//       subtree roots go to the top parents' FP64 accumulators)
-//   S2  warp 0: elimination and back-substitution of the small top tree,
-//       V update of the top nodes
-//   S3  every warp: fused back-substitution + V update + channels + next-step
-//       assembly for its subtrees, then channels + assembly of its share of
-//       the top nodes
+// Segment item, S1: leaf -> root elimination of the spine r..l-1 after its
+// light subtrees, carrying each row's dependence on the lower separator's
+// dV (w, the coupling b_l x_l of row l-1 moved to the right-hand side);
+// then a root -> leaf pass that writes every spine node's solution as
+// dV_i = g_i + al_i dV_u + be_i dV_l, and the reduced coupling of l to u.
+template <typename R>
+__device__ __forceinline__ void eliminate_segment(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
+                                                  const DevComp& c) {
+    using M = Math<R>;
+    const int r = c.r, l = c.l, b = l - 1;
+    const NodeRec<R> nl = nr[l];
+    const R e_l = G.scr[(size_t)l * 3 * kLanes + 2 * kLanes];
+    R carry_d = 0, carry_r = 0, carry_w = 0;
+    R* sv = G.sepv + (size_t)c.lk * 4 * kLanes;
+    for (int i = b; i >= r; --i) {
+        const NodeRec<R> s = nr[i];
+        R* row = G.scr + (size_t)i * 3 * kLanes;
+        R d, rh;
+        const R e_i = row[2 * kLanes];
+        if (s.jslot >= 0) {
+            double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
+            d = (R)((double)row[0] + (double)carry_d + ja[0]);
+            rh = (R)((double)row[kLanes] + (double)carry_r + ja[kLanes]);
+            ja[0] = 0.0;
+            ja[kLanes] = 0.0;
+        } else {
+            d = row[0] + carry_d;
+            rh = row[kLanes] + carry_r;
+        }
+        R w = carry_w;
+        if (i == b) {
+            w = -nl.b;
+            rh += e_l;
+        }
+        const R inv = M::rc(d);
+        const R rr = rh * inv, cc = s.a * inv, om = w * inv;
+        row[0] = rr;
+        row[kLanes] = cc;
+        row[2 * kLanes] = om;
+        if (i > r) {
+            carry_d = -s.b * cc;
+            carry_r = e_i - s.b * rr;
+            carry_w = -s.b * om;
+        } else {
+            double* ja = G.jacc + (size_t)(2 * s.pslot) * kLanes;  // the upper separator
+            atomicAdd(ja, (double)(-s.b * cc));
+            atomicAdd(ja + kLanes, (double)(e_i - s.b * rr));
+            sv[kLanes] = s.b * om;  // B: row u's coupling to dV_l
+        }
+    }
+    R al = 0, be = 0, ga = 0;
+    for (int i = r; i <= b; ++i) {
+        R* row = G.scr + (size_t)i * 3 * kLanes;
+        const R rr = row[0], cc = row[kLanes], om = row[2 * kLanes];
+        if (i == r) {
+            al = -cc;
+            be = om;
+            ga = rr;
+        } else {
+            al = -cc * al;
+            be = om - cc * be;
+            ga = rr - cc * ga;
+        }
+        row[0] = ga;
+        row[kLanes] = al;
+        row[2 * kLanes] = be;
+    }
+    sv[0] = nl.a * al;                // A: row l's coupling to dV_u
+    sv[2 * kLanes] = nl.a * be;       // added to d_l
+    sv[3 * kLanes] = -nl.a * ga;      // added to rhs_l
+}
+
+// Warp-level work queue: lane 0 takes the next item, the warp shares it.
+__device__ __forceinline__ int next_item(int* ctr) {
+    int k = 0;
+    if ((threadIdx.x & 31) == 0) k = atomicAdd(ctr, 1);
+    return __shfl_sync(0xffffffffu, k, 0);
+}
+
+// Per timestep (three barriers):
+//   S1  all warps take items from a queue, largest first: leaf -> root
+//       elimination of plain subtrees and of segments (above); each item's
+//       contribution to its upper separator goes to that separator's FP64
+//       accumulator
+//   S2  warp 0 solves the skeleton (the separators, a few dozen nodes) with
+//       the reduced couplings of the segments, and updates their V
+//   S3  all warps take items again: back-substitution + V update + channel
+//       update + next-step assembly of every node of the item (a segment
+//       also does its lower separator's channels, which need the spine's new
+//       V); separators linked directly to the skeleton are items too
 template <typename R, int MS>
-__global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_advance(SimArgs<R> A, int t0, int n_steps) {
+__global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim_advance(SimArgs<R> A, int t0, int n_steps) {
     extern __shared__ __align__(128) char smem[];
+    __shared__ int ctr[2];
     const Group<R> G = group_of(A);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    stage_solve_topology(A, smem);
-    const SolveNode<R>* sn = (const SolveNode<R>*)smem;
-    const int s_lo = A.seg_off[w], s_hi = A.seg_off[w + 1];
-    const int c_lo = A.tch_off[w], c_hi = A.tch_off[w + 1];
+    const int w = threadIdx.x >> 5;
+    const NodeRec<R>* nr = stage_nodes(A, smem);
+    if (threadIdx.x == 0) { ctr[0] = 0; ctr[1] = 0; }
+    __syncthreads();
     int bad = 0;
+    const int n_items3 = A.n_comps + A.n_seps;
     for (int t = t0; t < t0 + n_steps; ++t) {
         // S1
-        for (int k = s_hi - 1; k >= s_lo; --k) {
-            const int2 sg = A.seg[k];
-            eliminate_range(G, sn, sg.x, sg.y);
+        if (threadIdx.x == 0) ctr[1] = 0;
+        for (int k = next_item(&ctr[0]); k < A.n_comps; k = next_item(&ctr[0])) {
+            const DevComp c = A.comps[k];
+            eliminate_list(G, nr, c.lo, c.hi, [](int q) { return q; });
+            if (c.l >= 0) eliminate_segment(A, G, nr, c);
         }
         __syncthreads();
-        // S2
+        // S2: skeleton
         if (w == 0) {
-            R carry_d = 0, carry_r = 0;
-            for (int k = A.n_top - 1; k >= 0; --k) {
-                const int i = A.top[k];
-                const R* row = G.scr + (size_t)i * 3 * kLanes;
-                eliminate_node(G, sn[i], i, row[0], row[kLanes], row[2 * kLanes], carry_d, carry_r);
+            using M = Math<R>;
+            for (int k = A.n_seps - 1; k >= 0; --k) {
+                const DevSep sp = A.seps[k];
+                const NodeRec<R> s = nr[sp.node];
+                R* row = G.scr + (size_t)sp.node * 3 * kLanes;
+                double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
+                R d = (R)((double)row[0] + ja[0]);
+                R rh = (R)((double)row[kLanes] + ja[kLanes]);
+                ja[0] = 0.0;
+                ja[kLanes] = 0.0;
+                R Acp = s.a, Bcp = s.b, e_up = row[2 * kLanes];
+                if (sp.seg >= 0) {
+                    const R* sv = G.sepv + (size_t)k * 4 * kLanes;
+                    Acp = sv[0];
+                    Bcp = sv[kLanes];
+                    d += sv[2 * kLanes];
+                    rh += sv[3 * kLanes];
+                    e_up = 0;  // the segment already folded this node's axial term in
+                }
+                if (k == 0) {
+                    row[0] = M::dv(rh, d);
+                    break;
+                }
+                const R inv = M::rc(d);
+                const R rr = rh * inv, cc = Acp * inv;
+                row[0] = rr;
+                row[kLanes] = cc;
+                double* jp = G.jacc + (size_t)(2 * nr[A.seps[sp.par].node].jslot) * kLanes;
+                jp[0] += (double)(-Bcp * cc);
+                jp[kLanes] += (double)(e_up - Bcp * rr);
             }
-            R x_prev = 0;
-            for (int k = 0; k < A.n_top; ++k) {
-                const int i = A.top[k];
-                const SolveNode<R> s = sn[i];
-                R* o = G.scr + (size_t)i * 3 * kLanes;
-                const R xp = (i == 0) ? (R)0 : (s.pslot < 0 ? x_prev : G.jx[(size_t)s.pslot * kLanes]);
-                const R x = o[0] - o[kLanes] * xp;
-                if (s.jslot >= 0) G.jx[(size_t)s.jslot * kLanes] = x;
-                x_prev = x;
-                R* vo = G.vbuf + (size_t)i * 2 * kLanes;
+            for (int k = 0; k < A.n_seps; ++k) {
+                const DevSep sp = A.seps[k];
+                const NodeRec<R> s = nr[sp.node];
+                const R* row = G.scr + (size_t)sp.node * 3 * kLanes;
+                R x;
+                if (k == 0) x = row[0];
+                else x = row[0] - row[kLanes] * G.jx[(size_t)nr[A.seps[sp.par].node].jslot * kLanes];
+                G.jx[(size_t)s.jslot * kLanes] = x;
+                R* vo = G.vbuf + (size_t)sp.node * 2 * kLanes;
                 R V = vo[0], vc = vo[kLanes];
                 kahan_add(V, vc, x);
                 vo[0] = V;
                 vo[kLanes] = vc;
-                if (i == 0 && !(fabs(V) < (R)1e6)) bad = 1;  // NaN / Inf / blow-up
+                if (k == 0 && !(fabs(V) < (R)1e6)) bad = 1;  // NaN / Inf / blow-up
             }
         }
         __syncthreads();
         // S3
+        if (threadIdx.x == 0) ctr[0] = 0;
         R dt, dtn_inv, istim_amp;
         bool rec_now;
         float* trace;
         step_inputs(A, G, t, false, dt, dtn_inv, istim_amp, rec_now, trace);
-        for (int k = s_lo; k < s_hi; ++k) {
-            const int2 sg = A.seg[k];
-            R x_prev = 0;
-            for (int i = sg.x; i < sg.y; ++i) {
-                if (i + 1 < sg.y) prefetch_node(A, G, i + 1, lane);
-                update_node<R, MS, false, true>(A, G, sn[i], i, dt, dtn_inv, istim_amp, rec_now, trace, x_prev);
+        for (int k = next_item(&ctr[1]); k < n_items3; k = next_item(&ctr[1])) {
+            if (k < A.n_comps) {
+                const DevComp c = A.comps[k];
+                R x_prev = 0, v_prev = 0;
+                if (c.l >= 0) {  // spine: dV from the separators' solution
+                    const R xu = G.jx[(size_t)nr[c.u].jslot * kLanes];
+                    const R xl = G.jx[(size_t)nr[c.l].jslot * kLanes];
+                    v_prev = G.vbuf[(size_t)c.u * 2 * kLanes];
+                    for (int i = c.r; i < c.l; ++i) {
+                        if (i + 2 < c.l) prefetch_node(G, nr[i + 2], i + 2);
+                        const R* row = G.scr + (size_t)i * 3 * kLanes;
+                        const R xi = row[0] + row[kLanes] * xu + row[2 * kLanes] * xl;
+                        update_node<R, MS, false, true>(A, G, nr[i], i, dt, dtn_inv, istim_amp, rec_now, trace,
+                                                        x_prev, v_prev, &xi);
+                    }
+                }
+                x_prev = 0;
+                for (int i = c.lo; i < c.hi; ++i) {
+                    if (i + 2 < c.hi) prefetch_node(G, nr[i + 2], i + 2);
+                    update_node<R, MS, false, true>(A, G, nr[i], i, dt, dtn_inv, istim_amp, rec_now, trace, x_prev,
+                                                    v_prev, nullptr);
+                }
+                if (c.l >= 0) {
+                    R xd = 0, vd = 0;
+                    update_node<R, MS, false, false>(A, G, nr[c.l], c.l, dt, dtn_inv, istim_amp, rec_now, trace,
+                                                     xd, vd, nullptr);
+                }
+            } else {
+                const DevSep sp = A.seps[k - A.n_comps];
+                if (sp.seg < 0) {
+                    R xd = 0, vd = 0;
+                    update_node<R, MS, false, false>(A, G, nr[sp.node], sp.node, dt, dtn_inv, istim_amp, rec_now,
+                                                     trace, xd, vd, nullptr);
+                }
             }
-        }
-        R xd = 0;
-        for (int k = c_lo; k < c_hi; ++k) {
-            const int i = A.tch[k];
-            update_node<R, MS, false, false>(A, G, sn[i], i, dt, dtn_inv, istim_amp, rec_now, trace, xd);
         }
         __syncthreads();
     }

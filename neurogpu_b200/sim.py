@@ -50,13 +50,30 @@ class Model:
                 "state_vars": sv.value, "param_reads": prd.value}
 
     def partition(self, n_warps: int) -> dict:
-        """The tree split a CTA of n_warps warps uses (see ngpu_model_partition)."""
+        """The tree split a CTA of n_warps warps uses, per node in this model's
+        numbering (see ngpu_model_partition)."""
         n = self.cell.n_nodes
-        top, own, js, ps = (np.zeros(n, dtype=np.int32) for _ in range(4))
+        sep, item, js, ps = (np.zeros(n, dtype=np.int32) for _ in range(4))
         nj = C.c_int32()
         _ffi.check("ngpu_model_partition", _ffi.lib().ngpu_model_partition(
-            self._h, int(n_warps), _ffi.ptr(top), _ffi.ptr(own), _ffi.ptr(js), _ffi.ptr(ps), C.byref(nj)))
-        return {"top": top.astype(bool), "owner": own, "jslot": js, "pslot": ps, "n_jslots": nj.value}
+            self._h, int(n_warps), _ffi.ptr(sep), _ffi.ptr(item), _ffi.ptr(js), _ffi.ptr(ps), C.byref(nj)))
+        return {"sep": sep.astype(bool), "item": item, "jslot": js, "pslot": ps, "n_jslots": nj.value}
+
+    def split_info(self, n_warps: int) -> dict:
+        """The split in the library's internal node order (ngpu_model_split_info)."""
+        n = self.cell.n_nodes
+        L = _ffi.lib()
+        nc, ns = C.c_int32(), C.c_int32()
+        _ffi.check("ngpu_model_split_info", L.ngpu_model_split_info(
+            self._h, int(n_warps), None, C.byref(nc), None, 0, C.byref(ns), None, 0, None, None))
+        perm = np.zeros(n, dtype=np.int32)
+        comps = np.zeros((max(1, nc.value), 6), dtype=np.int32)
+        seps = np.zeros((max(1, ns.value), 3), dtype=np.int32)
+        js, ps = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+        _ffi.check("ngpu_model_split_info", L.ngpu_model_split_info(
+            self._h, int(n_warps), _ffi.ptr(perm), C.byref(nc), _ffi.ptr(comps), nc.value, C.byref(ns),
+            _ffi.ptr(seps), ns.value, _ffi.ptr(js), _ffi.ptr(ps)))
+        return {"perm": perm, "comps": comps[:nc.value], "seps": seps[:ns.value], "jslot": js, "pslot": ps}
 
     def close(self) -> None:
         if self._h:
