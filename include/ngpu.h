@@ -127,6 +127,38 @@ int ngpu_sim_check(ngpu_sim *s, int32_t *n_bad, void *cuda_stream);
 /* Device pointer of the trace buffer, layout [n_samples][n_rec][n_inst_padded]. */
 int ngpu_sim_trace_device(ngpu_sim *s, const float **trace, int32_t *n_inst_padded);
 
+/*
+ * Allocation-free variant of ngpu_run.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory -- a host program that
+ * owns a fixed device-memory arena and budget and hands the library only
+ * slices of it, or a loop with latency limits that cannot take the device-wide
+ * synchronisation and unbounded time of cudaMalloc / cudaFree.  The run's
+ * internal buffers (node records, channel states, parameter table, solver
+ * scratch, trace) live in one file-scope __device__ array of 16 MiB inside
+ * the library, which every GPU that loads the library holds until exit.
+ * Nothing is allocated: no cudaMalloc, cudaFree or other allocating call.
+ *
+ *   params_dev, amps_dev, dts_dev, out_dev: the caller's DEVICE memory, in the
+ *     layouts of ngpu_run; rec_nodes: host array.  FP32 only.
+ *   Limits: at most 512 nodes, 256 instances (sets x stimuli), 16 recording
+ *     sites, and the run must fit the 16 MiB array (nodes x instances x
+ *     states plus the nt-sample trace); larger runs are rejected with
+ *     NGPU_E_INVALID and a message giving the bytes needed.
+ *   Work is enqueued on cuda_stream; the call returns once its small host
+ *     copies are done, before the simulation finishes.  Non-finite voltages
+ *     are not reported.
+ *   The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.  All calls share the array and find the
+ *     previous call's contents in it (each call resets what it relies on), so
+ *     calls that overlap on the GPU race: serialise them.
+ */
+int ngpu_run_static(ngpu_model *m, int32_t n_sets, const float *params_dev, int32_t n_stim,
+                    int32_t nt, const float *amps_dev, const float *dts_dev, int32_t stim_node,
+                    float stim_area_um2, int32_t n_rec, const int32_t *rec_nodes, float v_init,
+                    float *out_dev, void *cuda_stream);
+
 /* Kernel launches issued by this thread since the last call (for accounting). */
 int64_t ngpu_launch_count(int32_t reset);
 

@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
             "ngpu_sim_check": (C.c_int, [P, P, P]),
             "ngpu_sim_trace_device": (C.c_int, [P, P, P]),
             "ngpu_launch_count": (I64, [I32]),
+            "ngpu_run_static": (C.c_int, [P, I32, P, I32, I32, P, P, I32, F32, I32, P, F32, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

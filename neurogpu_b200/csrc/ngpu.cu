@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <type_traits>
@@ -921,3 +922,238 @@ int ngpu_run(ngpu_model* m, int32_t n_sets, const float* params, int32_t n_stim,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free entry point (ngpu_run_static).
+//
+// Some callers are not allowed to allocate device memory at all: an
+// application that hands this library a region of its own pre-allocated
+// device arena and runs under a fixed device-memory budget, or a host loop
+// with latency limits that cannot afford cudaMalloc / cudaFree (both can
+// synchronise the whole device and take unbounded time).  For them every
+// buffer of one simulation run -- node records, channel states, parameters
+// table, solver scratch, trace -- is carved out of the single file-scope
+// array below instead of being allocated.  Inputs and outputs stay in the
+// caller's own device memory.
+//
+// The array is a host-side stand-in in host code: its device address is
+// looked up with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on the device.  Every call shares the
+// array and leaves its contents behind; each call re-initialises what it
+// relies on.  Two calls whose work overlaps on the GPU (different streams,
+// or another thread) race on the array and must be serialised by the caller.
+// ===========================================================================
+namespace {
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // held by every GPU that loads the library
+constexpr int kStaticMaxNodes = 512;
+constexpr int kStaticMaxInstances = 256;
+constexpr int kStaticMaxRec = 16;
+constexpr int kStaticMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mu;
+static unsigned char* g_static_addr[kStaticMaxDevices] = {};
+
+// Device address of g_static_scratch on the current device (set-up on first use).
+static int static_scratch_address(unsigned char** out) {
+    int dev = -1;
+    NGPU_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices)
+        return fail(NGPU_E_INVALID, "device ordinal beyond the static-scratch table");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(NGPU_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        g_static_addr[dev] = (unsigned char*)p;
+    }
+    *out = g_static_addr[dev];
+    return NGPU_OK;
+}
+
+extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* params_dev, int32_t n_stim,
+                               int32_t nt, const float* amps_dev, const float* dts_dev, int32_t stim_node,
+                               float stim_area_um2, int32_t n_rec, const int32_t* rec_nodes, float v_init,
+                               float* out_dev, void* cuda_stream) {
+    if (!m || !params_dev || !amps_dev || !dts_dev || !rec_nodes || !out_dev)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: null argument");
+    const int N = m->n;
+    if (N > kStaticMaxNodes)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: at most " + std::to_string(kStaticMaxNodes) +
+                                        " nodes (model has " + std::to_string(N) + ")");
+    if (n_sets < 1 || n_stim < 1 || (int64_t)n_sets * n_stim > kStaticMaxInstances)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: 1 to " + std::to_string(kStaticMaxInstances) +
+                                        " instances (sets x stimuli)");
+    if (nt < 1) return fail(NGPU_E_INVALID, "ngpu_run_static: nt must be >= 1");
+    if (n_rec < 1 || n_rec > kStaticMaxRec)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: 1 to " + std::to_string(kStaticMaxRec) + " recording sites");
+    if (stim_node < 0 || stim_node >= N) return fail(NGPU_E_INVALID, "ngpu_run_static: stim_node out of range");
+    if (!(stim_area_um2 > 0.f) || !std::isfinite(stim_area_um2))
+        return fail(NGPU_E_INVALID, "ngpu_run_static: stimulus area must be positive");
+    if (!std::isfinite(v_init)) return fail(NGPU_E_INVALID, "ngpu_run_static: v_init must be finite");
+    for (int r = 0; r < n_rec; ++r)
+        if (rec_nodes[r] < 0 || rec_nodes[r] >= N)
+            return fail(NGPU_E_INVALID, "ngpu_run_static: recording node out of range");
+
+    // ---- host bookkeeping in fixed-size local arrays (one warp per group:
+    // the root is the only separator, its child subtrees the work items)
+    const int n_inst = n_sets * n_stim;
+    const int n_groups = (n_inst + kLanes - 1) / kLanes;
+    const int n_pad = n_groups * kLanes;
+    NodeRec<float> recs[kStaticMaxNodes];  // ~38 KB of stack in all
+    DevComp comps[kStaticMaxNodes];
+    int subn[kStaticMaxNodes], jslot[kStaticMaxNodes], pslot[kStaticMaxNodes];
+    int inst_stim[kStaticMaxInstances + kLanes];
+    int rec_col_of_node[kStaticMaxRec], rec_cols[kStaticMaxRec], n_rec_u = 0;
+    for (int r = 0; r < n_rec; ++r) {
+        const int node = m->inv[rec_nodes[r]];
+        int c = -1;
+        for (int k = 0; k < n_rec_u; ++k)
+            if (rec_col_of_node[k] == node) c = k;
+        if (c < 0) {
+            c = n_rec_u;
+            rec_col_of_node[n_rec_u++] = node;
+        }
+        rec_cols[r] = c;
+    }
+    for (int i = 0; i < N; ++i) subn[i] = 1;
+    for (int i = N - 1; i > 0; --i) subn[m->parent[i]] += subn[i];
+    int n_comps = 0;
+    for (int i = 1; i < N; ++i)
+        if (m->parent[i] == 0) comps[n_comps++] = {i, 0, -1, -1, i, i + subn[i]};
+    int nj = 0;
+    for (int i = 0; i < N; ++i) jslot[i] = -1;
+    jslot[0] = nj++;
+    for (int i = 1; i < N; ++i) {
+        const int p = m->parent[i];
+        if ((p != i - 1 || p == 0) && jslot[p] < 0) jslot[p] = nj++;
+    }
+    for (int i = 0; i < N; ++i) {
+        const int p = i > 0 ? m->parent[i] : -1;
+        pslot[i] = (i > 0 && (p != i - 1 || p == 0)) ? jslot[p] : -1;
+    }
+    for (int i = 0; i < N; ++i) {
+        NodeRec<float>& q = recs[i];
+        q.a = (float)m->a[i];
+        q.b = (float)m->b[i];
+        q.dconst = (float)m->dconst[i];
+        q.cm = (float)(m->cm[i] / 1000.0);
+        q.srow = m->info[i].srow;
+        q.parent = (int16_t)m->parent[i];
+        q.jslot = (int16_t)jslot[i];
+        q.pslot = (int16_t)pslot[i];
+        q.rec = -1;
+        q.mask = (uint16_t)m->mask[i];
+        q.prow = (uint16_t)m->info[i].prow;
+        q.srows = (uint16_t)m->rows[i].x;
+        q.prows = (uint16_t)m->rows[i].y;
+    }
+    for (int k = 0; k < n_rec_u; ++k) recs[rec_col_of_node[k]].rec = (int16_t)k;
+    for (int k = 0; k < n_pad; ++k) inst_stim[k] = std::min(k, n_inst - 1) % n_stim;
+    const DevSep root_sep = {0, -1, -1, 0};
+
+    // ---- carve the static array
+    const size_t G = (size_t)n_groups, L = kLanes;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off += (bytes + 255) & ~size_t(255);
+        return at;
+    };
+    const size_t o_recs = take(sizeof(NodeRec<float>) * N);
+    const size_t o_comps = take(sizeof(DevComp) * std::max(1, n_comps));
+    const size_t o_seps = take(sizeof(DevSep));
+    const size_t o_istim = take(sizeof(int) * n_pad);
+    const size_t o_bad = take(sizeof(int) * n_pad);
+    const size_t o_err = take(sizeof(int));
+    const size_t o_rowp = take(sizeof(int) * m->row_param.size());
+    const size_t o_rows = take(sizeof(int) * m->row_sec.size());
+    const size_t o_vbuf = take(G * N * 2 * L * sizeof(float));
+    const size_t o_slab = take(G * m->slab_rows * L * sizeof(float));
+    const size_t o_ptab = take(G * m->ptab_rows * L * sizeof(float));
+    const size_t o_scr = take(G * N * 3 * L * sizeof(float));
+    const size_t o_jacc = take(G * 2 * nj * L * sizeof(double));
+    const size_t o_jx = take(G * nj * L * sizeof(float));
+    const size_t o_sepv = take(G * 4 * L * sizeof(float));
+    const size_t o_trace = take((size_t)nt * n_rec_u * n_pad * sizeof(float));
+    if (off > kStaticScratchBytes)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: this run needs " + std::to_string(off) +
+                                        " bytes of device scratch; the static array holds " +
+                                        std::to_string(kStaticScratchBytes));
+    unsigned char* base = nullptr;
+    int rc = static_scratch_address(&base);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    NGPU_CUDA(cudaMemcpyAsync(base + o_recs, recs, sizeof(NodeRec<float>) * N, cudaMemcpyHostToDevice, st));
+    if (n_comps)
+        NGPU_CUDA(cudaMemcpyAsync(base + o_comps, comps, sizeof(DevComp) * n_comps, cudaMemcpyHostToDevice, st));
+    NGPU_CUDA(cudaMemcpyAsync(base + o_seps, &root_sep, sizeof(DevSep), cudaMemcpyHostToDevice, st));
+    NGPU_CUDA(cudaMemcpyAsync(base + o_istim, inst_stim, sizeof(int) * n_pad, cudaMemcpyHostToDevice, st));
+    NGPU_CUDA(cudaMemcpyAsync(base + o_rowp, m->row_param.data(), sizeof(int) * m->row_param.size(),
+                              cudaMemcpyHostToDevice, st));
+    NGPU_CUDA(cudaMemcpyAsync(base + o_rows, m->row_sec.data(), sizeof(int) * m->row_sec.size(),
+                              cudaMemcpyHostToDevice, st));
+    NGPU_CUDA(cudaMemsetAsync(base + o_err, 0, sizeof(int), st));  // left over from an earlier call
+    // the copies above read host stack memory: make sure they are done before returning
+    NGPU_CUDA(cudaStreamSynchronize(st));
+
+    SimArgs<float> A;
+    A.nodes = (const NodeRec<float>*)(base + o_recs);
+    A.n_nodes = N;
+    A.vbuf = (float*)(base + o_vbuf);
+    A.slab = (float*)(base + o_slab);
+    A.slab_rows = m->slab_rows;
+    A.ptab = (const float*)(base + o_ptab);
+    A.ptab_rows = m->ptab_rows;
+    A.scr = (float*)(base + o_scr);
+    A.jacc = (double*)(base + o_jacc);
+    A.jx = (float*)(base + o_jx);
+    A.n_jslots = nj;
+    A.amps = amps_dev;
+    A.dts = dts_dev;
+    A.nt = nt;
+    A.stim_node = m->inv[stim_node];
+    A.stim_scale = 100.0 / (double)stim_area_um2;
+    A.inst_stim = (const int*)(base + o_istim);
+    A.trace = (float*)(base + o_trace);
+    A.n_rec = n_rec_u;
+    A.rec_every = 1;
+    A.n_inst_pad = n_pad;
+    A.v_init = v_init;
+    A.bad = (int*)(base + o_bad);
+    A.err = (int*)(base + o_err);
+    A.n_warps = 1;
+    A.comps = (const DevComp*)(base + o_comps);
+    A.n_comps = n_comps;
+    A.seps = (const DevSep*)(base + o_seps);
+    A.n_seps = 1;
+    A.sepv = (float*)(base + o_sepv);
+
+    const size_t total = G * m->ptab_rows * L;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    k_gather_params<<<blocks, 256, 0, st>>>(params_dev, (const int*)(base + o_rowp), (const int*)(base + o_rows),
+                                              m->ptab_rows, m->n_params, m->n_sections, n_stim, n_inst, n_groups,
+                                              (float*)(base + o_ptab));
+    const size_t smem = SmemPlan<float>::bytes(N);
+    if (m->mechset == NGPU_MECHSET_TTPC) {
+        k_sim_init<float, 0><<<n_groups, kLanes, 0, st>>>(A);
+        k_sim_advance<float, 0><<<n_groups, kLanes, smem, st>>>(A, 0, nt);
+    } else {
+        k_sim_init<float, 1><<<n_groups, kLanes, 0, st>>>(A);
+        k_sim_advance<float, 1><<<n_groups, kLanes, smem, st>>>(A, 0, nt);
+    }
+    g_launches += 3;
+    NGPU_CUDA(cudaGetLastError());
+    // trace [sample][site][instance] -> out [instance][requested site][sample]
+    for (int r = 0; r < n_rec; ++r) {
+        dim3 grid((n_pad + 31) / 32, (nt + 31) / 32, 1), block(32, 8);
+        k_trace_transpose_site<<<grid, block, 0, st>>>(A.trace, nt, n_rec_u, rec_cols[r], n_pad, n_inst, n_rec, r,
+                                                       out_dev);
+        g_launches++;
+    }
+    NGPU_CUDA(cudaGetLastError());
+    return NGPU_OK;
+}

@@ -577,4 +577,24 @@ __global__ void k_trace_transpose(const float* __restrict__ trace, int n_samples
     }
 }
 
+// One recording site of the trace into a caller's [instance][site][sample]
+// array: out[(inst * out_sites + out_site) * n_samples + s] <-
+// trace[(s * n_rec + col) * n_inst_pad + inst].  Used by the allocation-free
+// entry point, which writes straight into the caller's buffer.
+__global__ void k_trace_transpose_site(const float* __restrict__ trace, int n_samples, int n_rec, int col,
+                                       int n_inst_pad, int n_inst, int out_sites, int out_site,
+                                       float* __restrict__ out) {
+    __shared__ float tile[32][33];
+    const int i0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int s = s0 + k, i = i0 + threadIdx.x;
+        if (s < n_samples && i < n_inst_pad) tile[k][threadIdx.x] = trace[((size_t)s * n_rec + col) * n_inst_pad + i];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int i = i0 + k, s = s0 + threadIdx.x;
+        if (i < n_inst && s < n_samples) out[((size_t)i * out_sites + out_site) * n_samples + s] = tile[threadIdx.x][k];
+    }
+}
+
 }  // namespace ngpu
