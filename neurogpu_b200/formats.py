@@ -1,0 +1,265 @@
+"""The reference's file formats at the simulation boundary.
+
+A reference run reads its whole problem from the Data/ directory
+(GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/Util.h:44-56) and writes one trace
+file; these readers / writers keep that contract so existing directories run
+unchanged:
+
+* BasicConstSegP.csv -- topology and per-node constants, one comma-terminated
+  line per field, written by NeuroGPU_Base/scripts/pyscripts/
+  create_auxilliary_data_3.py:229-271 and read by src/MainC.cu:335-551.
+* AllParams.csv (src/Util.cu:210-234): line 1 = NSets, then one row of
+  NCOMPS*NPARAMS values per set, parameter-major (param_macro,
+  src/CudaStuff.cu:212).  ParamsM.csv, the per-model default written by the
+  porting step, holds one set section-major (NPARAMS values per section).
+* Sim.csv (src/Util.cu:394-432): v_init, dt, NRecSites, RecSites.
+* Stim_meta.csv (src/Util.cu:337-358): NStimuli, Nt, comp, loc (1-based), area.
+* Stim_raw.csv / Stim_raw<dev>.csv: one row of Nt amplitudes (nA) per stimulus.
+* times.csv: Nt per-step dt (ms) -- the step dt the reference uses
+  (src/CudaStuff.cu:228-230).
+* VHotP<dev>.dat (src/Util.cu:458-476): int32 N, int32 3, N float64 values in
+  [set][stim][site][t] order.  RunTimes.csv: "NSets,ms".
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from .mechsets import MAINEN, TTPC, MechSet
+from .model import CellModel
+
+# BasicConstSegP.csv line numbers (1-based), create_auxilliary_data_3.py:229-264
+BCS_FIELDS = ("N", "NComps", "e", "f", "Ks", "SegToComp", "Cms", "NModels", "boolModel",
+              "SonNoVec", "Depth", "LognDepth", "nFathers", "nCallForFather", "RelStarts",
+              "RelEnds", "RelVec", "SegStartI", "SegEndI", "Fathers", "FIdxs", "CompDepth",
+              "CompFDepth", "CompByLevel32", "CompByFLevel32", "nLRel", "LRelStarts",
+              "LRelEnds", "nFLRel", "FLRelStarts", "FLRelEnds", "KsB")
+
+
+def _csv_line(line: str) -> np.ndarray:
+    vals = [v for v in line.strip().split(",") if v.strip()]
+    return np.array([float(v) for v in vals], dtype=np.float64)
+
+
+def read_basic_const_segp(path: str | os.PathLike) -> dict[str, np.ndarray]:
+    """All 32 fields of a BasicConstSegP.csv as float64 arrays."""
+    lines = Path(path).read_text().splitlines()
+    if len(lines) < len(BCS_FIELDS):
+        raise ValueError(f"{path}: expected {len(BCS_FIELDS)} lines, found {len(lines)}")
+    return {name: _csv_line(lines[k]) for k, name in enumerate(BCS_FIELDS)}
+
+
+def parent_from_ks(ks: np.ndarray) -> np.ndarray:
+    """Node-order parent vector from the reversed 1-based Ks field: the parent
+    of node i > 0 is N - Ks[N - i] (the kernel's parentIndex,
+    src/CudaStuff.cu:195); the root's is -1."""
+    n = ks.size
+    parent = np.full(n, -1, dtype=np.int32)
+    for i in range(1, n):
+        parent[i] = n - int(ks[n - i])
+    return parent
+
+
+def son_no_vec(parent: np.ndarray) -> np.ndarray:
+    """Child rank of every node under its parent, in node order, with the
+    root's set to 0 (create_auxilliary_data_3.py:72-84)."""
+    used = np.zeros(parent.size, dtype=np.int64)
+    out = np.zeros(parent.size, dtype=np.int64)
+    for i in range(parent.size):
+        p = 0 if i == 0 else parent[i]
+        used[p] += 1
+        out[i] = used[p]
+    out[0] = 0
+    return out
+
+
+def ancestor_table(ks: np.ndarray) -> np.ndarray:
+    """The pointer-jumping table FIdxs of the reference's back-substitution
+    (create_auxilliary_data_3.py:53-67): row k holds, for every reversed
+    1-based node index, the 1-based index of its 2^k-th ancestor (N+1 past the
+    root); rows stop before the table saturates."""
+    n = ks.size
+    father = np.concatenate([ks[1:], [n + 1, n + 1]]).astype(np.int64)
+    rows = []
+    for lev in range(1, int(np.ceil(np.log2(n))) + 3 + 1):
+        cur = np.arange(1, father.size + 1)
+        for _ in range(2 ** (lev - 1)):
+            cur = father[cur - 1]
+        rows.append(cur)
+    tab = np.array(rows)
+    ind = int(np.nonzero(np.all(tab == tab[-1], axis=1))[0][0]) + 1
+    if ind != 0:
+        tab = tab[:ind - 1, :]
+    return tab[:, :n]
+
+
+@dataclass
+class ReferenceModel:
+    """A reference Data/ directory turned into the library's inputs."""
+    cell: CellModel
+    params: np.ndarray          # [n_sets, n_params, n_sections] float32 (library mechanism set)
+    amps: np.ndarray            # [n_stim, nt] float32
+    dts: np.ndarray             # [nt] float32
+    stim_node: int              # 0-based node
+    stim_area: float            # um2 (float32 value)
+    rec_nodes: np.ndarray       # int32
+    v_init: float
+    raw: dict = field(default_factory=dict)
+
+
+def mechset_for(n_models: int, n_params: int) -> tuple[MechSet, list[int], list[int] | None]:
+    """Library mechanism set for a reference build, the library mechanism of
+    each of the file's boolModel rows, and (when the reference build's
+    parameter list differs) the library parameter index of each file
+    parameter."""
+    if n_params == TTPC.n_params and n_models == TTPC.n_mech:
+        return TTPC, list(range(TTPC.n_mech)), None
+    if n_params == MAINEN.n_params and n_models <= MAINEN.n_mech:
+        # the Mainen build writes 7 boolModel rows: ca cad kca km kv na pas
+        return MAINEN, list(range(n_models)), None
+    if n_params == 2 and n_models == 1:
+        # single-mechanism passive build (Figures/FigureS3_passive/CParsed): pas
+        return TTPC, [TTPC.mech_index("pas")], [TTPC.param_index("g_pas"), TTPC.param_index("e_pas")]
+    raise ValueError(f"no library mechanism set matches a build with {n_models} mechanisms "
+                     f"and {n_params} parameters")
+
+
+def cell_from_basic_const(bc: dict[str, np.ndarray], n_params: int) -> CellModel:
+    n = int(bc["N"][0])
+    ncomps = int(bc["NComps"][0])
+    nmod = int(bc["NModels"][0])
+    ms, mech_map, _ = mechset_for(nmod, n_params)
+    parent = parent_from_ks(bc["Ks"])
+    e, f = bc["e"], bc["f"]
+    a = f[::-1][:n].copy()        # the reference's f, reversed into node order
+    b = e[::-1][:n].copy()
+    a[0] = 0.0
+    b[0] = 0.0
+    bool_model = bc["boolModel"].reshape(nmod, n)
+    mask = np.zeros((ms.n_mech, n), dtype=np.uint8)
+    for row, k in enumerate(mech_map):
+        mask[k] = (bool_model[row] != 0)
+    cell = CellModel(parent=parent, a=a, b=b, cm=bc["Cms"].astype(np.float64).copy(),
+                     section=bc["SegToComp"].astype(np.int32), n_sections=ncomps,
+                     mechset=ms, mech_mask=mask)
+    cell.validate()
+    return cell
+
+
+def read_params_csv(path: str | os.PathLike, n_comps: int, n_params: int, has_count: bool) -> np.ndarray:
+    """AllParams.csv (has_count: first line = NSets, rows parameter-major) or
+    ParamsM.csv (one section-major row) -> [n_sets, n_params, n_comps] float32
+    in the file's own parameter order."""
+    lines = [ln for ln in Path(path).read_text().splitlines() if ln.strip()]
+    if has_count:
+        n_sets = int(float(lines[0].split(",")[0]))
+        rows = lines[1:1 + n_sets]
+    else:
+        rows = lines
+    out = np.zeros((len(rows), n_params, n_comps), dtype=np.float32)
+    for k, ln in enumerate(rows):
+        v = _csv_line(ln)[:n_params * n_comps]
+        if v.size != n_params * n_comps:
+            raise ValueError(f"{path}: row {k} has {v.size} values, expected {n_params * n_comps}")
+        out[k] = v.reshape(n_params, n_comps) if has_count else v.reshape(n_comps, n_params).T
+    return out
+
+
+def write_allparams_csv(path: str | os.PathLike, params: np.ndarray) -> None:
+    """AllParams.csv in the reference's format (NeuroGPU_Base/scripts/
+    template/extractModel_mappings.py:326-330): the set count, then one
+    '%.5E, '-separated row per set."""
+    with open(path, "w") as fh:
+        fh.write(f"{params.shape[0]},\n")
+        for p in params.reshape(params.shape[0], -1):
+            fh.write(", ".join(f"{x:.5E}" for x in p) + ",\n")
+
+
+def map_params(file_params: np.ndarray, n_models: int, ms_params: int) -> np.ndarray:
+    """File parameter order -> library mechanism-set order."""
+    ms, _, pmap = mechset_for(n_models, file_params.shape[1])
+    if pmap is None:
+        return file_params
+    out = np.zeros((file_params.shape[0], ms.n_params, file_params.shape[2]), dtype=np.float32)
+    for j, k in enumerate(pmap):
+        out[:, k, :] = file_params[:, j, :]
+    return out
+
+
+def read_sim_csv(path: str | os.PathLike) -> tuple[float, float, np.ndarray]:
+    lines = [ln for ln in Path(path).read_text().splitlines() if ln.strip()]
+    v_init = float(_csv_line(lines[0])[0])
+    dt = float(_csv_line(lines[1])[0])
+    n_rec = int(_csv_line(lines[2])[0])
+    rec = _csv_line(lines[3])[:n_rec].astype(np.int32) if n_rec else np.zeros(0, np.int32)
+    return v_init, dt, rec
+
+
+def read_stim_meta(path: str | os.PathLike) -> tuple[int, int, int, float]:
+    """(n_stim, nt, loc as a 0-based node, area)."""
+    v = [float(ln.split(",")[0]) for ln in Path(path).read_text().splitlines() if ln.strip()]
+    return int(v[0]), int(v[1]), int(v[3]) - 1, float(np.float32(v[4]))
+
+
+def read_rows(path: str | os.PathLike, n_rows: int, n_cols: int) -> np.ndarray:
+    lines = [ln for ln in Path(path).read_text().splitlines() if ln.strip()]
+    out = np.zeros((n_rows, n_cols), dtype=np.float32)
+    for k in range(n_rows):
+        v = _csv_line(lines[k])[:n_cols]
+        out[k, :v.size] = v
+    return out
+
+
+def read_data_dir(data: str | os.PathLike, stim_index: int | None = None,
+                  params_file: str | None = None) -> ReferenceModel:
+    """Everything a reference run reads from its Data/ directory.  stim_index:
+    the device / stimulus number the reference appends to Stim_raw (argv[1],
+    src/Util.cu:359-364); None reads Stim_raw.csv."""
+    d = Path(data)
+    bc = read_basic_const_segp(d / "BasicConstSegP.csv")
+    n_comps = int(bc["NComps"][0])
+    n_models = int(bc["NModels"][0])
+    n_nodes = int(bc["N"][0])
+    if params_file is None:
+        params_file = "AllParams.csv" if (d / "AllParams.csv").exists() and \
+            not (d / "AllParams.csv").read_text().startswith("version https://git-lfs") else "ParamsM.csv"
+    has_count = Path(params_file).name.startswith("AllParams")
+    # parameter count of the build: the row length over NComps
+    first = [ln for ln in (d / params_file).read_text().splitlines() if ln.strip()]
+    row = first[1] if has_count else first[0]
+    n_params = _csv_line(row).size // n_comps
+    fparams = read_params_csv(d / params_file, n_comps, n_params, has_count)
+    cell = cell_from_basic_const(bc, n_params)
+    params = map_params(fparams, n_models, n_params)
+    v_init, _, rec = read_sim_csv(d / "Sim.csv")
+    n_stim, nt, loc, area = read_stim_meta(d / "Stim_meta.csv")
+    raw_name = "Stim_raw.csv" if stim_index is None else f"Stim_raw{stim_index}.csv"
+    amps = read_rows(d / raw_name, n_stim, nt)
+    dts = read_rows(d / "times.csv", 1, nt)[0]
+    if not (0 <= loc < n_nodes):
+        raise ValueError(f"stimulus location {loc + 1} outside the {n_nodes}-node tree")
+    return ReferenceModel(cell, params, amps, dts, loc, area, rec, v_init,
+                          raw={"basic_const": bc, "file_params": fparams})
+
+
+def write_vhot(path: str | os.PathLike, traces: np.ndarray) -> None:
+    """VHotP<dev>.dat: int32 count, int32 3, then float64 values."""
+    flat = np.ascontiguousarray(traces, dtype=np.float64).reshape(-1)
+    with open(path, "wb") as fh:
+        np.array([flat.size, 3], dtype=np.int32).tofile(fh)
+        flat.tofile(fh)
+
+
+def read_vhot(path: str | os.PathLike) -> np.ndarray:
+    """nrnMread of Figures/Figure4_DEAP/neurogpu_multistim_evaluator_par.py:
+    42-46 (the type word is ignored, values are float64)."""
+    with open(path, "rb") as fh:
+        n, _typ = np.fromfile(fh, dtype=np.int32, count=2)
+        return np.fromfile(fh, dtype=np.float64, count=int(n))
+
+
+def write_run_times(path: str | os.PathLike, n_sets: int, ms: float) -> None:
+    Path(path).write_text(f"{n_sets},{ms:f}\n")
