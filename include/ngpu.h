@@ -62,6 +62,11 @@ int ngpu_mechset_info(int32_t mechset, int32_t *n_mech, int32_t *n_params);
  *               read reversed from BasicConstSegP.csv lines 3-4).
  *   cm[n]       uF/cm2;  section[n]: node -> parameter section (SegToComp)
  *   mech_mask   [n_mech][n] 0/1, the reference's boolModel (line 9)
+ * Nodes joined by an edge whose absolute conductance exceeds 1e7 times the
+ * median edge's (near zero-area compartments of NEURON exports) are merged
+ * into one internal node; callers keep addressing every node in their own
+ * numbering (a merged node's voltage is its group's).  The environment
+ * variable NGPU_CONTRACT=0 disables the merge (diagnostics).
  */
 int ngpu_model_create(int32_t n_nodes, const int32_t *parent, const double *a, const double *b,
                       const double *cm, const int32_t *section, int32_t n_sections,
@@ -71,6 +76,19 @@ int ngpu_model_destroy(ngpu_model *m);
 int ngpu_model_layout(const ngpu_model *m, int32_t *state_rows, int32_t *param_rows,
                       int32_t *n_jslots, int64_t *state_vars, int64_t *param_reads);
 
+/* Node bookkeeping after stiff-edge merging: internal node count, the
+ * caller's node count, node_internal[n_caller] (caller node -> internal
+ * node) and density_scale[n_caller] (caller node's area over its internal
+ * node's area; a stimulus current density on a merged node is scaled by it).
+ * No counterpart in the reference, which keeps every node.  Any pointer may
+ * be NULL. */
+int ngpu_model_nodes(const ngpu_model *m, int32_t *n_internal, int32_t *n_caller, int32_t *node_internal,
+                     double *density_scale);
+/* The merged model in internal order: parent[n_internal], a, b, cm (the
+ * coefficients the kernels use).  For tests and tools; any pointer may be
+ * NULL. */
+int ngpu_model_arrays(const ngpu_model *m, int32_t *parent, double *a, double *b, double *cm);
+
 /* Introspection of the tree split used by a CTA of n_warps warps, per node in
  * the caller's numbering: sep_flag (1 = separator, solved by warp 0 in the
  * skeleton), item (work item holding the node, -1 for separators), junction
@@ -78,7 +96,8 @@ int ngpu_model_layout(const ngpu_model *m, int32_t *state_rows, int32_t *param_r
 int ngpu_model_partition(const ngpu_model *m, int32_t n_warps, int32_t *sep_flag, int32_t *item,
                          int32_t *jslot, int32_t *pslot, int32_t *n_jslots);
 /* The same split in the library's internal node order (heavy-first depth
- * first): perm[n] maps internal -> caller's node; comps[6*k] = (root, upper
+ * first): perm[n_internal] maps internal -> caller's node (a merged node's
+ * representative); comps[6*k] = (root, upper
  * separator, lower separator or -1, its separator index, light range lo, hi);
  * seps[3*k] = (node, skeleton parent index, linking item or -1); jslot/pslot
  * per internal node.  For tests and tools. */

@@ -107,11 +107,116 @@ struct ngpu_model {
     std::vector<int> row_param, row_sec;
     int slab_rows = 0, ptab_rows = 0;
     int64_t state_vars = 0, param_reads = 0;
-    std::vector<double> dconst;
     std::vector<int> weight;        // per-node channel cost
     std::vector<int2> rows;         // (state rows, parameter rows) per node
-    std::vector<int> perm, inv;     // internal node -> caller's node, and back
+    std::vector<int> perm, inv;     // internal node -> caller's node (group representative), group -> internal
+    // stiff-edge contraction (see contract_stiff_edges)
+    int n_caller = 0;                    // nodes in the caller's numbering
+    std::vector<int> node_internal;      // caller node -> internal node
+    std::vector<double> density_scale;   // caller node -> area(node) / area(its internal node)
 };
+
+namespace {
+
+// Stiff-edge contraction.
+//
+// Exports of NEURON models can hold compartments of near-zero area, whose
+// per-area axial couplings reach 1e21 while ordinary ones are 1e-4 .. 10.
+// Such compartments are tied to their neighbours so tightly that their
+// voltages agree far below FP32 (or FP64) resolution, yet each step's
+// right-hand side multiplies their voltage differences, rounding included,
+// by those couplings, and the rounding noise leaks into the rest of the
+// cell.  Nodes joined by such edges are therefore merged into one node
+// before anything else (the voltage difference across a merged edge is the
+// edge current over a conductance >= 1e7 times the median one).
+//
+// Rows are per unit membrane area, so the relative areas follow from the
+// coefficients themselves: row i holds a_i = -G_i / area_i, its parent's row
+// b_i = -G_i / area_parent, hence area_i / area_parent = b_i / a_i and the
+// edge's absolute conductance G_i = |a_i| area_i.  A merged group keeps one
+// row, normalised to the area of its representative (the member with
+// channels, or else the largest); the others contribute capacitance only
+// (sum of cm area) and their couplings are rescaled to the representative's
+// area.  Two members with channels are never merged, since the kernel
+// computes one channel set per node.
+struct Contraction {
+    std::vector<int> group;        // caller node -> group (groups numbered by first member)
+    std::vector<int> rep, top;     // group -> representative / top member (caller numbering)
+    std::vector<double> area;      // caller node -> area relative to the root
+    int n_groups = 0;
+};
+
+constexpr double kStiffRatio = 1e7;
+
+static Contraction contract_stiff_edges(int n, const int32_t* parent, const double* a, const double* b,
+                                        const std::vector<uint32_t>& mask, bool enabled) {
+    Contraction C;
+    C.area.assign(n, 1.0);
+    std::vector<double> G(n, 0.0);
+    std::vector<char> ok(n, 0);
+    for (int i = 1; i < n; ++i) {
+        const double r = b[i] / a[i];
+        if (std::isfinite(r) && r > 0.0 && std::isfinite(C.area[parent[i]] * r)) {
+            C.area[i] = C.area[parent[i]] * r;
+            G[i] = std::fabs(a[i]) * C.area[i];
+            ok[i] = G[i] > 0.0 && std::isfinite(G[i]);
+        } else {
+            C.area[i] = C.area[parent[i]];
+        }
+    }
+    std::vector<int> up(n);
+    for (int i = 0; i < n; ++i) up[i] = i;
+    std::vector<int> chan(n, -1);  // per set root: its member with channels
+    for (int i = 0; i < n; ++i)
+        if (mask[i]) chan[i] = i;
+    auto find = [&](int x) {
+        while (up[x] != x) x = up[x] = up[up[x]];
+        return x;
+    };
+    if (enabled && n > 2) {
+        std::vector<double> gs;
+        for (int i = 1; i < n; ++i)
+            if (ok[i]) gs.push_back(G[i]);
+        if (!gs.empty()) {
+            std::nth_element(gs.begin(), gs.begin() + gs.size() / 2, gs.end());
+            const double thr = kStiffRatio * gs[gs.size() / 2];
+            std::vector<int> stiff;
+            for (int i = 1; i < n; ++i)
+                if (ok[i] && G[i] > thr) stiff.push_back(i);
+            std::stable_sort(stiff.begin(), stiff.end(), [&](int x, int y) { return G[x] > G[y]; });
+            for (int i : stiff) {
+                int x = find(i), y = find(parent[i]);
+                if (x == y || (chan[x] >= 0 && chan[y] >= 0)) continue;
+                if (y > x) std::swap(x, y);  // keep the smaller caller index as the set root
+                up[x] = y;
+                if (chan[y] < 0) chan[y] = chan[x];
+            }
+        }
+    }
+    C.group.assign(n, -1);
+    std::vector<int> gid_of_root(n, -1);
+    for (int i = 0; i < n; ++i) {
+        const int r = find(i);
+        if (gid_of_root[r] < 0) {
+            gid_of_root[r] = C.n_groups++;
+            C.top.push_back(i);  // first member in a parent-before-child order is the top
+            C.rep.push_back(-1);
+        }
+        C.group[i] = gid_of_root[r];
+    }
+    for (int i = 0; i < n; ++i) {
+        const int g = C.group[i];
+        const int r = find(i);
+        if (chan[r] >= 0) {
+            C.rep[g] = chan[r];
+        } else if (C.rep[g] < 0 || C.area[i] > C.area[C.rep[g]]) {
+            C.rep[g] = i;
+        }
+    }
+    return C;
+}
+
+}  // namespace
 
 // Split of the tree for one CTA of W warps (see sim_kernels.cuh).  Nodes are
 // already in heavy-first depth-first order (model creation reorders them), so
@@ -389,14 +494,41 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
     }
     if (n_nodes > 32767) return fail(NGPU_E_INVALID, "at most 32767 nodes per morphology");
     if (NM > 16) return fail(NGPU_E_INVALID, "at most 16 mechanisms per set");
+    std::vector<uint32_t> maskc(n_nodes, 0u);
+    for (int k = 0; k < NM; ++k)
+        for (int i = 0; i < n_nodes; ++i)
+            if (mech_mask[(size_t)k * n_nodes + i]) maskc[i] |= (1u << k);
+    // Stiff edges merged first; the tree below is the merged one (groups,
+    // numbered parent-before-child), with rows normalised to each group's
+    // representative.  NGPU_CONTRACT=0 keeps every node (diagnostics).
+    const char* cev = getenv("NGPU_CONTRACT");
+    const Contraction Ct = contract_stiff_edges(n_nodes, parent, a, b, maskc, !(cev && cev[0] == '0'));
+    const int n_caller = n_nodes;
+    n_nodes = Ct.n_groups;
+    std::vector<int32_t> parent_g(n_nodes), section_g(n_nodes);
+    std::vector<double> a_g(n_nodes), b_g(n_nodes), cm_g(n_nodes, 0.0);
+    std::vector<uint32_t> mask0(n_nodes);
+    for (int g = 0; g < n_nodes; ++g) {
+        const int t = Ct.top[g], r = Ct.rep[g];
+        const double ar = Ct.area[r];
+        parent_g[g] = g == 0 ? -1 : Ct.group[parent[t]];
+        section_g[g] = section[r];
+        mask0[g] = maskc[r];
+        // row g's coupling to its parent, per the representative's area; the
+        // parent row's entry, per the parent group's representative's area
+        a_g[g] = g == 0 ? a[0] : a[t] * (Ct.area[t] / ar);
+        b_g[g] = g == 0 ? b[0] : b[t] * (Ct.area[parent[t]] / Ct.area[Ct.rep[parent_g[g]]]);
+    }
+    for (int i = 0; i < n_caller; ++i) cm_g[Ct.group[i]] += cm[i] * (Ct.area[i] / Ct.area[Ct.rep[Ct.group[i]]]);
+    parent = parent_g.data();
+    a = a_g.data();
+    b = b_g.data();
+    cm = cm_g.data();
+    section = section_g.data();
     // Internal node order: heavy-first depth-first (children by decreasing
     // channel-cost subtree weight), so heavy paths are runs of consecutive
     // nodes.  Any Hines order the caller gives is accepted; stimulus and
     // recording nodes are mapped through the permutation.
-    std::vector<uint32_t> mask0(n_nodes, 0u);
-    for (int k = 0; k < NM; ++k)
-        for (int i = 0; i < n_nodes; ++i)
-            if (mech_mask[(size_t)k * n_nodes + i]) mask0[i] |= (1u << k);
     std::vector<int64_t> subw(n_nodes, 0);
     for (int i = n_nodes - 1; i >= 0; --i) {
         int wt = 12;
@@ -422,9 +554,18 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
     }
     ngpu_model* m = new (std::nothrow) ngpu_model();
     if (!m) return fail(NGPU_E_NOMEM, "host allocation failed");
-    m->perm = order;
+    m->perm.assign(n_nodes, 0);
+    for (int i = 0; i < n_nodes; ++i) m->perm[i] = Ct.rep[order[i]];
     m->inv.assign(n_nodes, 0);
     for (int i = 0; i < n_nodes; ++i) m->inv[order[i]] = i;
+    m->n_caller = n_caller;
+    m->node_internal.assign(n_caller, 0);
+    m->density_scale.assign(n_caller, 1.0);
+    for (int j = 0; j < n_caller; ++j) {
+        const int g = Ct.group[j];
+        m->node_internal[j] = m->inv[g];
+        m->density_scale[j] = Ct.area[j] / Ct.area[Ct.rep[g]];
+    }
     m->n = n_nodes;
     m->n_sections = n_sections;
     m->mechset = mechset;
@@ -447,18 +588,13 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
     }
     for (int i = 0; i < n_nodes; ++i) {
         if ((m->mask[i] & sd.needs_ca_dyn) && !(m->mask[i] & sd.ca_dyn_bit)) {
-            const int o = order[i];
+            const int o = m->perm[i];
             delete m;
             return fail(NGPU_E_INVALID, "node " + std::to_string(o) +
                                             " has a calcium current without calcium dynamics "
                                             "(its reversal potential would be infinite)");
         }
     }
-    // constant part of the diagonal
-    m->dconst.assign(n_nodes, 0.0);
-    for (int i = 0; i < n_nodes; ++i) m->dconst[i] = -m->a[i];
-    m->dconst[0] = 0.0;  // the root has no parent coupling
-    for (int i = 1; i < n_nodes; ++i) m->dconst[m->parent[i]] -= m->b[i];
     // state and parameter rows
     std::map<std::pair<int, uint32_t>, int> prow_of;
     m->info.resize(n_nodes);
@@ -523,6 +659,29 @@ int ngpu_model_layout(const ngpu_model* m, int32_t* state_rows, int32_t* param_r
     return NGPU_OK;
 }
 
+int ngpu_model_nodes(const ngpu_model* m, int32_t* n_internal, int32_t* n_caller, int32_t* node_internal,
+                     double* density_scale) {
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    if (n_internal) *n_internal = m->n;
+    if (n_caller) *n_caller = m->n_caller;
+    for (int j = 0; j < m->n_caller; ++j) {
+        if (node_internal) node_internal[j] = m->node_internal[j];
+        if (density_scale) density_scale[j] = m->density_scale[j];
+    }
+    return NGPU_OK;
+}
+
+int ngpu_model_arrays(const ngpu_model* m, int32_t* parent, double* a, double* b, double* cm) {
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    for (int i = 0; i < m->n; ++i) {
+        if (parent) parent[i] = m->parent[i];
+        if (a) a[i] = m->a[i];
+        if (b) b[i] = m->b[i];
+        if (cm) cm[i] = m->cm[i];
+    }
+    return NGPU_OK;
+}
+
 int ngpu_model_partition(const ngpu_model* m, int32_t n_warps, int32_t* sep_flag, int32_t* item,
                          int32_t* jslot, int32_t* pslot, int32_t* n_jslots) {
     if (!m) return fail(NGPU_E_INVALID, "null model");
@@ -536,8 +695,8 @@ int ngpu_model_partition(const ngpu_model* m, int32_t n_warps, int32_t* sep_flag
             for (int i = c.r; i < c.l; ++i) owner[i] = (int)k;
         for (int i = c.light_lo; i < c.light_hi; ++i) owner[i] = (int)k;
     }
-    for (int j = 0; j < m->n; ++j) {  // j: node in the caller's numbering
-        const int i = m->inv[j];
+    for (int j = 0; j < m->n_caller; ++j) {  // j: node in the caller's numbering
+        const int i = m->node_internal[j];
         if (sep_flag) sep_flag[j] = sep[i];
         if (item) item[j] = owner[i];
         if (jslot) jslot[j] = P.jslot[i];
@@ -714,7 +873,7 @@ int ngpu_sim_set_stimulus(ngpu_sim* s, int32_t nt, const float* amps, const floa
                           int32_t stim_node, float stim_area_um2, int32_t on_device) {
     if (!s || !amps || !dts) return fail(NGPU_E_INVALID, "null sim or stimulus arrays");
     if (nt < 1) return fail(NGPU_E_INVALID, "nt must be >= 1");
-    if (stim_node < 0 || stim_node >= s->m->n) return fail(NGPU_E_INVALID, "stim_node out of range");
+    if (stim_node < 0 || stim_node >= s->m->n_caller) return fail(NGPU_E_INVALID, "stim_node out of range");
     if (!(stim_area_um2 > 0.f) || !std::isfinite(stim_area_um2))
         return fail(NGPU_E_INVALID, "stimulus area must be positive");
     if (!on_device) {
@@ -735,8 +894,9 @@ int ngpu_sim_set_stimulus(ngpu_sim* s, int32_t nt, const float* amps, const floa
     NGPU_CUDA(cudaMemcpy(s->d_amps, amps, sizeof(float) * (size_t)nt * s->n_stim, kind));
     NGPU_CUDA(cudaMemcpy(s->d_dts, dts, sizeof(float) * (size_t)nt, kind));
     s->nt = nt;
-    s->stim_node = s->m->inv[stim_node];
-    s->stim_scale = 100.0 / (double)stim_area_um2;
+    s->stim_node = s->m->node_internal[stim_node];
+    // density over the internal node's area (differs only for a merged node)
+    s->stim_scale = 100.0 / (double)stim_area_um2 * s->m->density_scale[stim_node];
     s->has_stim = true;
     s->initialized = false;
     return NGPU_OK;
@@ -749,18 +909,19 @@ int ngpu_sim_set_recording(ngpu_sim* s, int32_t n_rec, const int32_t* rec_nodes,
     std::vector<int> uniq;
     std::vector<int> cols(n_rec);
     for (int r = 0; r < n_rec; ++r) {
-        if (rec_nodes[r] < 0 || rec_nodes[r] >= s->m->n)
+        if (rec_nodes[r] < 0 || rec_nodes[r] >= s->m->n_caller)
             return fail(NGPU_E_INVALID, "recording node out of range");
-        auto it = std::find(uniq.begin(), uniq.end(), rec_nodes[r]);
+        const int node = s->m->node_internal[rec_nodes[r]];  // merged nodes share one column
+        auto it = std::find(uniq.begin(), uniq.end(), node);
         if (it == uniq.end()) {
             cols[r] = (int)uniq.size();
-            uniq.push_back(rec_nodes[r]);
+            uniq.push_back(node);
         } else {
             cols[r] = (int)(it - uniq.begin());
         }
     }
     s->rec_nodes.assign(n_rec, 0);
-    for (int r = 0; r < n_rec; ++r) s->rec_nodes[r] = s->m->inv[rec_nodes[r]];
+    for (int r = 0; r < n_rec; ++r) s->rec_nodes[r] = s->m->node_internal[rec_nodes[r]];
     s->rec_cols = cols;
     s->n_rec_unique = (int)uniq.size();
     s->rec_every = rec_every;
@@ -786,7 +947,6 @@ int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
             using RT = std::remove_reference_t<decltype(q.a)>;
             q.a = (RT)m->a[i];
             q.b = (RT)m->b[i];
-            q.dconst = (RT)m->dconst[i];
             q.cm = (RT)(m->cm[i] / 1000.0);
             q.srow = m->info[i].srow;
             q.parent = (int16_t)m->parent[i];
@@ -990,12 +1150,13 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     if (nt < 1) return fail(NGPU_E_INVALID, "ngpu_run_static: nt must be >= 1");
     if (n_rec < 1 || n_rec > kStaticMaxRec)
         return fail(NGPU_E_INVALID, "ngpu_run_static: 1 to " + std::to_string(kStaticMaxRec) + " recording sites");
-    if (stim_node < 0 || stim_node >= N) return fail(NGPU_E_INVALID, "ngpu_run_static: stim_node out of range");
+    if (stim_node < 0 || stim_node >= m->n_caller)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: stim_node out of range");
     if (!(stim_area_um2 > 0.f) || !std::isfinite(stim_area_um2))
         return fail(NGPU_E_INVALID, "ngpu_run_static: stimulus area must be positive");
     if (!std::isfinite(v_init)) return fail(NGPU_E_INVALID, "ngpu_run_static: v_init must be finite");
     for (int r = 0; r < n_rec; ++r)
-        if (rec_nodes[r] < 0 || rec_nodes[r] >= N)
+        if (rec_nodes[r] < 0 || rec_nodes[r] >= m->n_caller)
             return fail(NGPU_E_INVALID, "ngpu_run_static: recording node out of range");
 
     // ---- host bookkeeping in fixed-size local arrays (one warp per group:
@@ -1009,7 +1170,7 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     int inst_stim[kStaticMaxInstances + kLanes];
     int rec_col_of_node[kStaticMaxRec], rec_cols[kStaticMaxRec], n_rec_u = 0;
     for (int r = 0; r < n_rec; ++r) {
-        const int node = m->inv[rec_nodes[r]];
+        const int node = m->node_internal[rec_nodes[r]];
         int c = -1;
         for (int k = 0; k < n_rec_u; ++k)
             if (rec_col_of_node[k] == node) c = k;
@@ -1039,7 +1200,6 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
         NodeRec<float>& q = recs[i];
         q.a = (float)m->a[i];
         q.b = (float)m->b[i];
-        q.dconst = (float)m->dconst[i];
         q.cm = (float)(m->cm[i] / 1000.0);
         q.srow = m->info[i].srow;
         q.parent = (int16_t)m->parent[i];
@@ -1115,8 +1275,8 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     A.amps = amps_dev;
     A.dts = dts_dev;
     A.nt = nt;
-    A.stim_node = m->inv[stim_node];
-    A.stim_scale = 100.0 / (double)stim_area_um2;
+    A.stim_node = m->node_internal[stim_node];
+    A.stim_scale = 100.0 / (double)stim_area_um2 * m->density_scale[stim_node];
     A.inst_stim = (const int*)(base + o_istim);
     A.trace = (float*)(base + o_trace);
     A.n_rec = n_rec_u;

@@ -23,14 +23,25 @@
 // junction, or a subtree root) adds it to an FP64 junction accumulator of
 // its parent.
 //
+// Excess form.  A row is not stored with its diagonal d_i but with its
+// excess x_i = d_i + (sum of the row's off-diagonal couplings): at assembly
+// the grounded part g_i + cm_i/dt, later plus what eliminated children leak
+// to ground.  The diagonal is rebuilt as x_i - a_i (- the spine's coupling to
+// a lower separator) when the row is eliminated, and a child passes
+// -b_c x_c / d_c to its parent's excess.  Every update is then a sum of
+// nonnegative terms (the couplings a, b are negative), so FP32 keeps its
+// relative precision even where couplings differ by twenty orders of
+// magnitude, as between the near zero-area compartments of NEURON exports and
+// ordinary ones; the textbook update d_p - b_c a_c / d_c cancels there.
+//
 // Storage per group of 32 instances (rows of 32 elements, one per lane):
 //   vbuf   [N][2]  V and its Kahan compensation
 //   slab   channel state rows, per node in mechanism order
 //   ptab   parameter rows per distinct (section, mechanism set) pair
-//   scr    [N][3]  (d, rhs, e) after assembly, e = b_i (V_p - V_i) the
+//   scr    [N][3]  (x, rhs, e) after assembly, e = b_i (V_p - V_i) the
 //                  parent-row axial term; (r, c, -) after elimination with
-//                  dV_i = r_i - c_i dV_parent
-//   jacc   [J][2]  FP64 (d, rhs) accumulators of junction parents
+//                  dV_i = r_i - c_i dV_parent (spines: (r, c, w), below)
+//   jacc   [J][2]  FP64 (excess, rhs) accumulators of junction parents
 //   jx     [J]     dV of junction parents for their far children
 #pragma once
 #include "channels_mainen.cuh"
@@ -46,12 +57,11 @@ constexpr int kMaxWarps = 8;   // 256 threads; with 3 CTAs per SM the 85-registe
 #endif
 
 // Per-node record, identical for every instance; staged in shared memory
-// once per launch (36 bytes in FP32).
+// once per launch (32 bytes in FP32).
 template <typename R>
 struct NodeRec {
     R a;        // row i, column parent(i)
     R b;        // row parent(i), column i
-    R dconst;   // -a_i - sum over children c of b_c
     R cm;       // cm_i / 1000  (uF/cm2 -> mA/cm2/mV per 1/ms)
     int32_t srow;    // first channel-state row in slab
     int16_t parent;  // -1 for the root
@@ -108,7 +118,7 @@ struct SimArgs {
     int n_comps;
     const DevSep* seps;    // skeleton, ascending node index
     int n_seps;
-    R* sepv;               // [n_seps][4] rows per group: A, B, dd, drhs of segment links
+    R* sepv;               // [n_seps][4] rows per group: A, B, excess, rhs terms of segment links
 };
 
 template <typename R, int MS, bool INIT>
@@ -177,43 +187,43 @@ __device__ __forceinline__ void prefetch_node(const Group<R>& G, const NodeRec<R
     }
 }
 
-// Elimination of node i given its (d, rhs, e); updates the chain carry or the
+// Elimination of node i given its (x, rhs, e); updates the chain carry or the
 // parent's FP64 junction accumulator, writes (r, c).
 template <typename R>
-__device__ __forceinline__ void eliminate_node(const Group<R>& G, const NodeRec<R>& s, int i, R d0, R r0,
-                                               R e0, R& carry_d, R& carry_r) {
+__device__ __forceinline__ void eliminate_node(const Group<R>& G, const NodeRec<R>& s, int i, R x0, R r0,
+                                               R e0, R& carry_x, R& carry_r) {
     using M = Math<R>;
-    R d, r;
+    R x, r;
     if (s.jslot >= 0) {
         double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
-        d = (R)((double)d0 + (double)carry_d + ja[0]);
+        x = (R)((double)x0 + (double)carry_x + ja[0]);
         r = (R)((double)r0 + (double)carry_r + ja[kLanes]);
         ja[0] = 0.0;
         ja[kLanes] = 0.0;
     } else {
-        d = d0 + carry_d;
+        x = x0 + carry_x;
         r = r0 + carry_r;
     }
     R* out = G.scr + (size_t)i * 3 * kLanes;
-    if (i == 0) {  // root: dV_0 = rhs_0 / d_0
-        out[0] = M::dv(r, d);
+    if (i == 0) {  // root: no coupling left, d_0 = x_0
+        out[0] = M::dv(r, x);
         out[kLanes] = 0;
-        carry_d = carry_r = 0;
+        carry_x = carry_r = 0;
         return;
     }
-    const R inv = M::rc(d);
+    const R inv = M::rc(x - s.a);
     const R rr = r * inv, cc = s.a * inv;
     out[0] = rr;
     out[kLanes] = cc;
-    const R cd = -s.b * cc, cr = e0 - s.b * rr;  // e0: parent-row axial term
+    const R cx = -s.b * (x * inv), cr = e0 - s.b * rr;  // e0: parent-row axial term
     if (s.pslot < 0) {
-        carry_d = cd;
+        carry_x = cx;
         carry_r = cr;
     } else {
         double* ja = G.jacc + (size_t)(2 * s.pslot) * kLanes;
-        atomicAdd(ja, (double)cd);
+        atomicAdd(ja, (double)cx);
         atomicAdd(ja + kLanes, (double)cr);
-        carry_d = 0;
+        carry_x = 0;
         carry_r = 0;
     }
 }
@@ -223,25 +233,25 @@ __device__ __forceinline__ void eliminate_node(const Group<R>& G, const NodeRec<
 template <typename R, typename Idx>
 __device__ __forceinline__ void eliminate_list(const Group<R>& G, const NodeRec<R>* nr, int lo, int hi, Idx idx) {
     if (hi <= lo) return;
-    R carry_d = 0, carry_r = 0;
-    auto load = [&](int k, R& d, R& r, R& e) {
+    R carry_x = 0, carry_r = 0;
+    auto load = [&](int k, R& x, R& r, R& e) {
         if (k >= lo) {
             const R* row = G.scr + (size_t)idx(k) * 3 * kLanes;
-            d = row[0];
+            x = row[0];
             r = row[kLanes];
             e = row[2 * kLanes];
         }
     };
-    R d0 = 0, r0 = 0, e0 = 0, d1 = 0, r1 = 0, e1 = 0;
-    load(hi - 1, d0, r0, e0);
-    load(hi - 2, d1, r1, e1);
+    R x0 = 0, r0 = 0, e0 = 0, x1 = 0, r1 = 0, e1 = 0;
+    load(hi - 1, x0, r0, e0);
+    load(hi - 2, x1, r1, e1);
     for (int k = hi - 1; k >= lo; --k) {
-        R d2 = 0, r2 = 0, e2 = 0;
-        load(k - 2, d2, r2, e2);
+        R x2 = 0, r2 = 0, e2 = 0;
+        load(k - 2, x2, r2, e2);
         const int i = idx(k);
-        eliminate_node(G, nr[i], i, d0, r0, e0, carry_d, carry_r);
-        d0 = d1; r0 = r1; e0 = e1;
-        d1 = d2; r1 = r2; e1 = e2;
+        eliminate_node(G, nr[i], i, x0, r0, e0, carry_x, carry_r);
+        x0 = x1; r0 = r1; e0 = e1;
+        x1 = x2; r1 = r2; e1 = e2;
     }
 }
 
@@ -287,7 +297,7 @@ __device__ __forceinline__ void update_node(const SimArgs<R>& A, const Group<R>&
     if (BACKSUB && n.jslot >= 0) G.jx[(size_t)n.jslot * kLanes] = x;
     const R istim = (i == A.stim_node) ? istim_amp : (R)0;
     const R dvp = vp - V;
-    o[0] = Gm + n.cm * dtn_inv + n.dconst;
+    o[0] = Gm + n.cm * dtn_inv;  // the row's excess: its grounded conductance
     o[kLanes] = istim - I - n.a * dvp;
     o[2 * kLanes] = n.b * dvp;
     if (rec_now && n.rec >= 0) trace[(size_t)n.rec * A.n_inst_pad] = (float)V;
@@ -332,10 +342,15 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
 }
 
 // Segment item, S1: leaf -> root elimination of the spine r..l-1 after its
-// light subtrees, carrying each row's dependence on the lower separator's
-// dV (w, the coupling b_l x_l of row l-1 moved to the right-hand side);
-// then a root -> leaf pass that writes every spine node's solution as
-// dV_i = g_i + al_i dV_u + be_i dV_l, and the reduced coupling of l to u.
+// light subtrees.  Each spine row also couples to the lower separator's dV
+// (w: b_l of row l-1, then the fill-in carried up the spine), so its diagonal
+// is x - a + w and the row solves as dV_i = r_i - c_i dV_parent + w_i dV_l
+// (stored as (r, c, w) for S3).  The same sweep accumulates what separator
+// l needs for the skeleton, dV_{l-1} = gamma + alpha dV_u + beta dV_l
+// expanded down the spine: alpha (row l's coupling to u), gamma (its
+// right-hand side) and delta = 1 - alpha - beta, the fraction of dV_{l-1}
+// that leaks to ground along the spine, which becomes l's excess.  delta is
+// summed from the rows' leak fractions x_i / d_i, never as 1 - alpha - beta.
 template <typename R>
 __device__ __forceinline__ void eliminate_segment(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
                                                   const DevComp& c) {
@@ -343,21 +358,22 @@ __device__ __forceinline__ void eliminate_segment(const SimArgs<R>& A, const Gro
     const int r = c.r, l = c.l, b = l - 1;
     const NodeRec<R> nl = nr[l];
     const R e_l = G.scr[(size_t)l * 3 * kLanes + 2 * kLanes];
-    R carry_d = 0, carry_r = 0, carry_w = 0;
+    R carry_x = 0, carry_r = 0, carry_w = 0;
+    R P = 1, gam = 0, del = 0;  // P: product of -c over the rows below
     R* sv = G.sepv + (size_t)c.lk * 4 * kLanes;
     for (int i = b; i >= r; --i) {
         const NodeRec<R> s = nr[i];
         R* row = G.scr + (size_t)i * 3 * kLanes;
-        R d, rh;
+        R x, rh;
         const R e_i = row[2 * kLanes];
         if (s.jslot >= 0) {
             double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
-            d = (R)((double)row[0] + (double)carry_d + ja[0]);
+            x = (R)((double)row[0] + (double)carry_x + ja[0]);
             rh = (R)((double)row[kLanes] + (double)carry_r + ja[kLanes]);
             ja[0] = 0.0;
             ja[kLanes] = 0.0;
         } else {
-            d = row[0] + carry_d;
+            x = row[0] + carry_x;
             rh = row[kLanes] + carry_r;
         }
         R w = carry_w;
@@ -365,42 +381,28 @@ __device__ __forceinline__ void eliminate_segment(const SimArgs<R>& A, const Gro
             w = -nl.b;
             rh += e_l;
         }
-        const R inv = M::rc(d);
-        const R rr = rh * inv, cc = s.a * inv, om = w * inv;
+        const R inv = M::rc(x - s.a + w);
+        const R rr = rh * inv, cc = s.a * inv, om = w * inv, lam = x * inv;
         row[0] = rr;
         row[kLanes] = cc;
         row[2 * kLanes] = om;
+        gam += rr * P;
+        del += lam * P;
+        P *= -cc;
         if (i > r) {
-            carry_d = -s.b * cc;
+            carry_x = -s.b * lam;
             carry_r = e_i - s.b * rr;
             carry_w = -s.b * om;
         } else {
             double* ja = G.jacc + (size_t)(2 * s.pslot) * kLanes;  // the upper separator
-            atomicAdd(ja, (double)(-s.b * cc));
+            atomicAdd(ja, (double)(-s.b * lam));
             atomicAdd(ja + kLanes, (double)(e_i - s.b * rr));
             sv[kLanes] = s.b * om;  // B: row u's coupling to dV_l
         }
     }
-    R al = 0, be = 0, ga = 0;
-    for (int i = r; i <= b; ++i) {
-        R* row = G.scr + (size_t)i * 3 * kLanes;
-        const R rr = row[0], cc = row[kLanes], om = row[2 * kLanes];
-        if (i == r) {
-            al = -cc;
-            be = om;
-            ga = rr;
-        } else {
-            al = -cc * al;
-            be = om - cc * be;
-            ga = rr - cc * ga;
-        }
-        row[0] = ga;
-        row[kLanes] = al;
-        row[2 * kLanes] = be;
-    }
-    sv[0] = nl.a * al;                // A: row l's coupling to dV_u
-    sv[2 * kLanes] = nl.a * be;       // added to d_l
-    sv[3 * kLanes] = -nl.a * ga;      // added to rhs_l
+    sv[0] = nl.a * P;              // A: row l's coupling to dV_u (alpha = P)
+    sv[2 * kLanes] = -nl.a * del;  // added to l's excess
+    sv[3 * kLanes] = -nl.a * gam;  // added to rhs_l
 }
 
 // Warp-level work queue: lane 0 takes the next item, the warp shares it.
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim
                 const NodeRec<R> s = nr[sp.node];
                 R* row = G.scr + (size_t)sp.node * 3 * kLanes;
                 double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
-                R d = (R)((double)row[0] + ja[0]);
+                R x = (R)((double)row[0] + ja[0]);
                 R rh = (R)((double)row[kLanes] + ja[kLanes]);
                 ja[0] = 0.0;
                 ja[kLanes] = 0.0;
@@ -458,20 +460,20 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim
                     const R* sv = G.sepv + (size_t)k * 4 * kLanes;
                     Acp = sv[0];
                     Bcp = sv[kLanes];
-                    d += sv[2 * kLanes];
+                    x += sv[2 * kLanes];
                     rh += sv[3 * kLanes];
                     e_up = 0;  // the segment already folded this node's axial term in
                 }
                 if (k == 0) {
-                    row[0] = M::dv(rh, d);
+                    row[0] = M::dv(rh, x);
                     break;
                 }
-                const R inv = M::rc(d);
+                const R inv = M::rc(x - Acp);
                 const R rr = rh * inv, cc = Acp * inv;
                 row[0] = rr;
                 row[kLanes] = cc;
                 double* jp = G.jacc + (size_t)(2 * nr[A.seps[sp.par].node].jslot) * kLanes;
-                jp[0] += (double)(-Bcp * cc);
+                jp[0] += (double)(-Bcp * (x * inv));
                 jp[kLanes] += (double)(e_up - Bcp * rr);
             }
             for (int k = 0; k < A.n_seps; ++k) {
@@ -501,14 +503,15 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim
             if (k < A.n_comps) {
                 const DevComp c = A.comps[k];
                 R x_prev = 0, v_prev = 0;
-                if (c.l >= 0) {  // spine: dV from the separators' solution
-                    const R xu = G.jx[(size_t)nr[c.u].jslot * kLanes];
+                if (c.l >= 0) {  // spine: dV_i = r_i - c_i dV_parent + w_i dV_l, from separator u down
+                    R xp = G.jx[(size_t)nr[c.u].jslot * kLanes];
                     const R xl = G.jx[(size_t)nr[c.l].jslot * kLanes];
                     v_prev = G.vbuf[(size_t)c.u * 2 * kLanes];
                     for (int i = c.r; i < c.l; ++i) {
                         if (i + 2 < c.l) prefetch_node(G, nr[i + 2], i + 2);
                         const R* row = G.scr + (size_t)i * 3 * kLanes;
-                        const R xi = row[0] + row[kLanes] * xu + row[2 * kLanes] * xl;
+                        const R xi = row[0] - row[kLanes] * xp + row[2 * kLanes] * xl;
+                        xp = xi;
                         update_node<R, MS, false, true>(A, G, nr[i], i, dt, dtn_inv, istim_amp, rec_now, trace,
                                                         x_prev, v_prev, &xi);
                     }

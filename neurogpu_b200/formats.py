@@ -44,6 +44,56 @@ def _csv_line(line: str) -> np.ndarray:
     return np.array([float(v) for v in vals], dtype=np.float64)
 
 
+def ref_atof(tok: str) -> np.float32:
+    """One AllParams.csv value parsed the way the reference parses it
+    (src/Util.cu:143-185, myatof): mantissa digits accumulated in float32
+    (each step computed in double and rounded), divided in float32 by the
+    float32 power of ten of the fraction digits, then divided or multiplied by
+    the C int 10**exp (32-bit, wrapping).  It can land one ulp away from a
+    correctly rounded parse, so a drop-in reader must reproduce it to see the
+    reference's parameters bit for bit.  A nonzero exponent without a sign is
+    rejected: the reference reads an uninitialised sign there."""
+    s = tok.lstrip()
+    n = len(s)
+    i = 0
+    sign = np.float32(-1.0 if s[:1] == "-" else 1.0)
+    if s[:1] in ("+", "-") and n:
+        i = 1
+    val, pw = np.float32(0.0), np.float32(1.0)
+    while i < n and s[i].isdigit():
+        val = np.float32(10.0 * float(val) + (ord(s[i]) - 48))
+        i += 1
+    if i < n and s[i] == ".":
+        i += 1
+    while i < n and s[i].isdigit():
+        val = np.float32(10.0 * float(val) + (ord(s[i]) - 48))
+        pw = np.float32(10.0 * float(pw))
+        i += 1
+    if i < n and s[i] in "eE":
+        i += 1
+    esign = None
+    if i < n and s[i] in "+-":
+        esign = s[i]
+        i += 1
+    exp = 0
+    while i < n and s[i].isdigit():
+        exp = 10 * exp + (ord(s[i]) - 48)
+        i += 1
+    if esign is None and exp != 0:
+        raise ValueError(f"value {tok!r}: exponent without a sign")
+    p10 = 1
+    for _ in range(exp):
+        p10 = (p10 * 10 + 2 ** 31) % 2 ** 32 - 2 ** 31
+    q = sign * np.float32(val / pw)
+    return np.float32(q / np.float32(p10)) if esign == "-" else np.float32(q * np.float32(p10))
+
+
+def _ref_atof_line(line: str) -> np.ndarray:
+    toks = [t for t in line.split(",") if t.strip()]
+    uniq, inv = np.unique(np.array(toks), return_inverse=True)
+    return np.array([ref_atof(t) for t in uniq], dtype=np.float32)[inv]
+
+
 def read_basic_const_segp(path: str | os.PathLike) -> dict[str, np.ndarray]:
     """All 32 fields of a BasicConstSegP.csv as float64 arrays."""
     lines = Path(path).read_text().splitlines()
@@ -150,9 +200,10 @@ def cell_from_basic_const(bc: dict[str, np.ndarray], n_params: int) -> CellModel
 
 
 def read_params_csv(path: str | os.PathLike, n_comps: int, n_params: int, has_count: bool) -> np.ndarray:
-    """AllParams.csv (has_count: first line = NSets, rows parameter-major) or
-    ParamsM.csv (one section-major row) -> [n_sets, n_params, n_comps] float32
-    in the file's own parameter order."""
+    """AllParams.csv (has_count: first line = NSets, rows parameter-major,
+    values parsed like the reference's myatof) or ParamsM.csv (one
+    section-major row) -> [n_sets, n_params, n_comps] float32 in the file's
+    own parameter order."""
     lines = [ln for ln in Path(path).read_text().splitlines() if ln.strip()]
     if has_count:
         n_sets = int(float(lines[0].split(",")[0]))
@@ -161,7 +212,7 @@ def read_params_csv(path: str | os.PathLike, n_comps: int, n_params: int, has_co
         rows = lines
     out = np.zeros((len(rows), n_params, n_comps), dtype=np.float32)
     for k, ln in enumerate(rows):
-        v = _csv_line(ln)[:n_params * n_comps]
+        v = (_ref_atof_line(ln) if has_count else _csv_line(ln))[:n_params * n_comps]
         if v.size != n_params * n_comps:
             raise ValueError(f"{path}: row {k} has {v.size} values, expected {n_params * n_comps}")
         out[k] = v.reshape(n_params, n_comps) if has_count else v.reshape(n_comps, n_params).T

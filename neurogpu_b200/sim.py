@@ -59,9 +59,30 @@ class Model:
             self._h, int(n_warps), _ffi.ptr(sep), _ffi.ptr(item), _ffi.ptr(js), _ffi.ptr(ps), C.byref(nj)))
         return {"sep": sep.astype(bool), "item": item, "jslot": js, "pslot": ps, "n_jslots": nj.value}
 
+    def nodes(self) -> dict:
+        """Stiff-edge merging (ngpu_model_nodes): internal node count, the
+        internal node of every node of this model, and each node's area over
+        its internal node's area."""
+        n = self.cell.n_nodes
+        ni = C.c_int32()
+        node_internal = np.zeros(n, dtype=np.int32)
+        scale = np.zeros(n, dtype=np.float64)
+        _ffi.check("ngpu_model_nodes", _ffi.lib().ngpu_model_nodes(
+            self._h, C.byref(ni), None, _ffi.ptr(node_internal), _ffi.ptr(scale)))
+        return {"n_internal": ni.value, "node_internal": node_internal, "density_scale": scale}
+
+    def arrays(self) -> dict:
+        """The merged model in internal order (ngpu_model_arrays)."""
+        n = self.nodes()["n_internal"]
+        par = np.zeros(n, dtype=np.int32)
+        a, b, cm = (np.zeros(n, dtype=np.float64) for _ in range(3))
+        _ffi.check("ngpu_model_arrays", _ffi.lib().ngpu_model_arrays(
+            self._h, _ffi.ptr(par), _ffi.ptr(a), _ffi.ptr(b), _ffi.ptr(cm)))
+        return {"parent": par, "a": a, "b": b, "cm": cm}
+
     def split_info(self, n_warps: int) -> dict:
         """The split in the library's internal node order (ngpu_model_split_info)."""
-        n = self.cell.n_nodes
+        n = self.nodes()["n_internal"]
         L = _ffi.lib()
         nc, ns = C.c_int32(), C.c_int32()
         _ffi.check("ngpu_model_split_info", L.ngpu_model_split_info(

@@ -10,6 +10,9 @@
 #   _ref/neuroGPU_ttpc512  the reference's fused GPU simulator, unmodified,
 #                          for sm_100a (its own Makefile uses -dc -O3 per file,
 #                          GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/Makefile:154)
+#   _ref/ref_atof          the reference's AllParams value parser (Util.cu,
+#                          myatof) behind oracle/ref_atof_main.cpp (stdin
+#                          tokens -> float bits)
 #
 # Test infrastructure only.  _ref/ is git-ignored but travels with the repo
 # snapshot, so the GPU box uses these prebuilt files.
@@ -48,5 +51,7 @@ if command -v nvcc >/dev/null 2>&1; then
         objs+=("$OUT/ref_$f.o")
     done
     nvcc "${GEN[@]}" -o "$OUT/neuroGPU_ttpc512" "${objs[@]}"
+    nvcc "${GEN[@]}" -O2 -c "$HERE/ref_atof_main.cpp" -o "$OUT/atof_main.o"
+    nvcc "${GEN[@]}" -o "$OUT/ref_atof" "$OUT/atof_main.o" "$OUT/ref_Util.o"
 fi
 echo "build_ref.sh: built into $OUT"

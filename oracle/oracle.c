@@ -1,7 +1,12 @@
 /*
  * CPU oracle for the NeuroGPU simulation step -- TEST INFRASTRUCTURE ONLY
  * (the checker; see oracle.h).  Compiled twice: ONG_REAL=double -> *_f64,
- * ONG_REAL=float -> *_f32.
+ * ONG_REAL=float -> *_f32.  The f32 build keeps the reference's storage
+ * split (U/Util.h:7-9): voltages, gating states, parameters and channel
+ * arithmetic in float (MYFTYPE), the tree matrix and its solve in double
+ * (MYSECONDFTYPE).  It does not reproduce the double promotions inside the
+ * reference's generated channel expressions; it is a precision probe, the
+ * f64 build is the parity reference.
  *
  * Every function below restates the reference's arithmetic; each cites the
  * file:line it follows.  Paths are relative to the reference project:
@@ -392,7 +397,7 @@ double ong_node_current_f64(int ms, const unsigned char *mask, double v, const d
  *   currents at v+0.001 and v              :262-267
  *   g=(I(v+eps)-I(v))/eps; rhs=Istim-I;
  *   D=g+cm/(1000 dt)-f; axial terms        :268-291
- *   Hines forward elimination              :31-69
+ *   Hines forward elimination              :31-69 (in excess form, below)
  *   back-substitution                      :72-104
  *   v += dV                                :298-301
  *   cnexp gate / Ca updates at the new v   :324-326
@@ -409,8 +414,8 @@ static void run_instance(const ong_model *m, const float *pset, const float *amp
     real *V = (real *)calloc((size_t)N, sizeof(real));
     real *S = (real *)calloc((size_t)N * SW, sizeof(real));
     real *P = (real *)calloc((size_t)N * NP, sizeof(real));
-    real *d = (real *)calloc((size_t)N, sizeof(real));
-    real *rhs = (real *)calloc((size_t)N, sizeof(real));
+    double *d = (double *)calloc((size_t)N, sizeof(double));    /* U/CudaStuff.cu:179-180: */
+    double *rhs = (double *)calloc((size_t)N, sizeof(double));  /* D, rhs are MYSECONDFTYPE */
     real *tmp = (real *)calloc((size_t)SW, sizeof(real));
     unsigned char *mk = (unsigned char *)calloc((size_t)N * NM, 1);
     for (int i = 0; i < N; ++i) {
@@ -440,27 +445,36 @@ static void run_instance(const ong_model *m, const float *pset, const float *amp
                 I = node_current(ms, k, V[i], p, s, &g, 1);
             }
             real istim = (i == stim_node) ? (real)(100.0 * (double)amp[t] / stim_area) : (real)0;
-            rhs[i] = istim - I;
-            d[i] = g + (real)m->cm[i] / (dt * (real)1000) - (real)m->a[i];
+            rhs[i] = (double)istim - (double)I;
+            /* the row's excess: its grounded conductance g + cm/(1000 dt) */
+            d[i] = (double)g + (double)(real)((real)m->cm[i] / (dt * (real)1000));
         }
         for (int i = 1; i < N; ++i) {
             int p = m->parent[i];
             real dv = V[p] - V[i];
-            rhs[i] -= (real)m->a[i] * dv;
-            rhs[p] += (real)m->b[i] * dv;
-            d[p] -= (real)m->b[i];
+            rhs[i] -= m->a[i] * (double)dv;
+            rhs[p] += m->b[i] * (double)dv;
         }
-        for (int i = N - 1; i >= 1; --i) { /* leaf -> root elimination */
+        /* leaf -> root elimination in excess form: row i's diagonal is its
+         * excess minus its coupling a_i (children already folded in); the
+         * child hands -b_i x_i / d_i to the parent's excess and -b_i rhs_i / d_i
+         * to its right-hand side.  Algebraically the reference's update
+         * u_p -= f e / u_i (U/CudaStuff.cu:31-69), without its cancellation of
+         * nearly equal diagonal terms, which costs ~1e-5 relative in FP64 on
+         * trees that join near zero-area compartments (couplings ~1e21) to
+         * ordinary ones. */
+        for (int i = N - 1; i >= 1; --i) {
             int p = m->parent[i];
-            real f = (real)m->b[i] / d[i];
-            d[p] -= f * (real)m->a[i];
-            rhs[p] -= f * rhs[i];
+            double di = d[i] - m->a[i];
+            d[p] += -m->b[i] * (d[i] / di);
+            rhs[p] += -m->b[i] * (rhs[i] / di);
+            d[i] = di;
         }
         rhs[0] /= d[0];
         for (int i = 1; i < N; ++i) /* root -> leaf back-substitution */
-            rhs[i] = (rhs[i] - (real)m->a[i] * rhs[m->parent[i]]) / d[i];
+            rhs[i] = (rhs[i] - m->a[i] * rhs[m->parent[i]]) / d[i];
         for (int i = 0; i < N; ++i) {
-            V[i] += rhs[i];
+            V[i] += (real)rhs[i];
             node_deriv(ms, mk + (size_t)i * NM, dt, V[i], P + (size_t)i * NP, S + (size_t)i * SW);
         }
     }

@@ -10,6 +10,9 @@ results).
      mainen384/ Figures/FigureS4_mainen/Data/{BasicConstSegP.csv, ParamsM.csv,
                 Sim.csv, Stim_meta.csv, Stim_raw.csv, times.csv} + Fmatrix.csv
      passive384/ Figures/FigureS3_passive/Data/{same} + Fmatrix.csv
+3. Feeds a seeded set of number tokens (and every value of the shipped
+   AllParams) to the reference's own AllParams parser (oracle/_ref/ref_atof)
+   and stores tokens and resulting float32 bits in atof_vectors.npz.
 2. Evaluates the reference's OWN channel functions (built from its sources by
    oracle/build_ref.sh into oracle/_ref/libref_{ttpc,mainen}.so) on a seeded
    grid of voltages / states / parameters, mechanism by mechanism, and stores
@@ -91,7 +94,26 @@ def channel_vectors() -> None:
             G=np.array([r[8] for r in recs], dtype=np.float32))
 
 
+def atof_vectors() -> None:
+    import subprocess
+    exe = ROOT / "oracle" / "_ref" / "ref_atof"
+    if not exe.exists():
+        raise SystemExit("oracle/_ref/ref_atof is not built: run oracle/build_ref.sh first")
+    rng = np.random.default_rng(77)
+    toks = []
+    for _ in range(4000):
+        x = float(np.float32(rng.choice([1, -1]) * 10 ** rng.uniform(-9, 4)))
+        toks.append(str(rng.choice([f"{x:.5E}", f"{x:.5e}", f"{x:.9e}", f"{x:.3f}", f" {x:.6e}"])))
+    toks += [t.strip() for t in (HERE / "ttpc512" / "AllParams_reference.csv").read_text().split(",")[1:]
+             if t.strip()]
+    out = subprocess.run([str(exe)], input="\n".join(toks) + "\n", capture_output=True, text=True,
+                         check=True).stdout.split()
+    bits = np.array([int(h, 16) for h in out], dtype=np.uint32)
+    np.savez_compressed(HERE / "atof_vectors.npz", tokens=np.array(toks), bits=bits)
+
+
 if __name__ == "__main__":
     copy_models()
     channel_vectors()
+    atof_vectors()
     print("golden fixtures written to", HERE)

@@ -114,3 +114,17 @@ def test_oracle_runs_shipped_models(oracle):
                          m.v_init)
         assert np.all(np.isfinite(out))
         assert abs(out[0, 0, 0, 99] - m.v_init) < 15.0
+
+
+def test_allparams_parse_matches_reference_parser():
+    """AllParams values parse to the reference parser's float32 bits
+    (src/Util.cu:143-185), which differ from a correctly rounded parse for a
+    sizeable share of tokens."""
+    from neurogpu_b200.formats import ref_atof
+    z = np.load(GOLD / "atof_vectors.npz")
+    got = np.array([ref_atof(str(t)) for t in z["tokens"]], dtype=np.float32).view(np.uint32)
+    assert np.array_equal(got, z["bits"])
+    rounded = np.array([np.float32(float(t)) for t in z["tokens"]], dtype=np.float32).view(np.uint32)
+    assert np.count_nonzero(rounded != z["bits"]) > 0.05 * z["bits"].size
+    with pytest.raises(ValueError):
+        ref_atof("1.5e3")
