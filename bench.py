@@ -40,7 +40,7 @@ METRIC = "compartment-steps/s (TTPC-like x4096)"
 UNIT = "compartment-steps/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-TRAFFIC_FILE = ROOT / "profiles" / "ttpc_like_sim_advance.md"
+TRAFFIC_FILE = ROOT / "profiles" / "k_sim_advance_ttpc_like_x4096.md"
 
 
 def parse_args():
