@@ -48,6 +48,10 @@ typedef struct ngpu_sim ngpu_sim;
 
 const char *ngpu_last_error(void);
 int ngpu_abi_version(void);
+/* Device selection for the calling thread (the reference binary takes its
+ * GPU from argv[1], U/kernel.cu:24-31). */
+int ngpu_device_count(int32_t *n);
+int ngpu_set_device(int32_t device);
 /* Mechanism set description: number of mechanisms / parameters. */
 int ngpu_mechset_info(int32_t mechset, int32_t *n_mech, int32_t *n_params);
 

@@ -48,6 +48,8 @@ def lib() -> C.CDLL:
             "ngpu_model_layout": (C.c_int, [P, P, P, P, P, P]),
             "ngpu_model_partition": (C.c_int, [P, I32, P, P, P, P, P]),
             "ngpu_model_nodes": (C.c_int, [P, P, P, P, P]),
+            "ngpu_device_count": (C.c_int, [P]),
+            "ngpu_set_device": (C.c_int, [I32]),
             "ngpu_model_arrays": (C.c_int, [P, P, P, P, P]),
             "ngpu_model_split_info": (C.c_int, [P, I32, P, P, P, I32, P, P, I32, P, P]),
             "ngpu_run": (C.c_int, [P, I32, P, I32, I32, P, P, I32, F32, I32, P, F32, I32, P]),

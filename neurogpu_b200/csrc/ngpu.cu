@@ -460,6 +460,20 @@ int64_t ngpu_launch_count(int32_t reset) {
     return reset ? g_launches.exchange(0) : g_launches.load();
 }
 
+int ngpu_device_count(int32_t* n) {
+    int c = 0;
+    const cudaError_t e = cudaGetDeviceCount(&c);
+    if (n) *n = e == cudaSuccess ? c : 0;
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    return NGPU_OK;
+}
+
+int ngpu_set_device(int32_t device) {
+    const cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return NGPU_OK;
+}
+
 int ngpu_mechset_info(int32_t mechset, int32_t* n_mech, int32_t* n_params) {
     if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN)
         return fail(NGPU_E_INVALID, "unknown mechanism set");
