@@ -46,6 +46,21 @@ NGPU_HD R efun(R z) {
     if (fabs(z) < (R)1e-2) return (R)1 - z * ((R)0.5 - z * (R)(1.0 / 12.0));
     return Math<R>::dv(z, Math<R>::ex(z) - (R)1);
 }
+// efun(z) and efun(-z) from one exponential: efun(-z) = efun(z) e^z, with the
+// series 1 -+ z/2 + z^2/12 near 0.  The alpha/beta pairs of NaTa_t, NaTs2_t
+// and Nap_Et2's activation are efun of opposite arguments.
+template <typename R>
+NGPU_HD void efun_pair(R z, R& pos, R& neg) {
+    if (fabs(z) < (R)1e-2) {
+        const R c = z * z * (R)(1.0 / 12.0);
+        pos = (R)1 - z * (R)0.5 + c;
+        neg = (R)1 + z * (R)0.5 + c;
+        return;
+    }
+    const R e = Math<R>::ex(z);
+    pos = Math<R>::dv(z, e - (R)1);
+    neg = pos * e;
+}
 // 1/(1 + e^z)
 template <typename R>
 NGPU_HD R sigm(R z) {
@@ -124,8 +139,10 @@ struct TTPCRates {
     static NGPU_HD void nap(R v, R& mi, R& mr, R& hi, R& hr) {
         mi = sigm((v + (R)52.6) * (R)(-1.0 / 4.6));
         if (v == (R)-38.0) v = v + (R)0.0001;
-        R ma = (R)(0.182 * 6.0) * efun(-(v + (R)38) * (R)(1.0 / 6.0));
-        R mb = (R)(0.124 * 6.0) * efun((v + (R)38) * (R)(1.0 / 6.0));
+        R ep, en;
+        efun_pair((v + (R)38) * (R)(1.0 / 6.0), ep, en);
+        R ma = (R)(0.182 * 6.0) * en;
+        R mb = (R)(0.124 * 6.0) * ep;
         mr = qt * (R)(1.0 / 6.0) * (ma + mb);
         if (v == (R)-17.0) v = v + (R)0.0001;
         if (v == (R)-64.4) v = v + (R)0.0001;
@@ -137,12 +154,15 @@ struct TTPCRates {
     // AllModels.cu:152-169 (NaTa_t: th_m=-38, th_h=-66), :170-187 (NaTs2_t: -32, -60)
     static NGPU_HD void nat(R v, R thm, R thh, R& mi, R& mr, R& hi, R& hr) {
         if (v == thm) v = v + (R)0.0001;
-        R ma = (R)(0.182 * 6.0) * efun(-(v - thm) * (R)(1.0 / 6.0));
-        R mb = (R)(0.124 * 6.0) * efun((v - thm) * (R)(1.0 / 6.0));
+        R ep, en;
+        efun_pair((v - thm) * (R)(1.0 / 6.0), ep, en);
+        R ma = (R)(0.182 * 6.0) * en;
+        R mb = (R)(0.124 * 6.0) * ep;
         mi = ab_gate(ma, mb, qt, &mr);
         if (v == thh) v = v + (R)0.0001;
-        R ha = (R)(0.015 * 6.0) * efun((v - thh) * (R)(1.0 / 6.0));
-        R hb = (R)(0.015 * 6.0) * efun(-(v - thh) * (R)(1.0 / 6.0));
+        efun_pair((v - thh) * (R)(1.0 / 6.0), ep, en);
+        R ha = (R)(0.015 * 6.0) * ep;
+        R hb = (R)(0.015 * 6.0) * en;
         hi = ab_gate(ha, hb, qt, &hr);
     }
     // AllModels.cu:188-193

@@ -127,6 +127,21 @@ __device__ __forceinline__ void channels(uint32_t mk, R v, R dt, R* st, const fl
     else mainen_node<R, INIT>(mk, v, dt, st, pr, I, G);
 }
 
+// The per-step channel update as one out-of-line function: the kernel calls
+// it from three places (spine nodes, light subtrees, separators), and one
+// shared copy keeps the instruction cache warm where warps at different
+// nodes run different mechanisms.  (I, G) come back in registers.
+template <typename R>
+struct CurrentG {
+    R I, G;
+};
+template <typename R, int MS>
+__device__ __noinline__ CurrentG<R> channels_step(uint32_t mk, R v, R dt, R* st, const float* pr) {
+    CurrentG<R> o;
+    channels<R, MS, false>(mk, v, dt, st, pr, o.I, o.G);
+    return o;
+}
+
 // v + x with running compensation c (Kahan); the round-to-nearest intrinsics
 // keep the compiler from re-associating the correction away.
 __device__ __forceinline__ void kahan_add(float& v, float& c, float x) {
@@ -288,8 +303,15 @@ __device__ __forceinline__ void update_node(const SimArgs<R>& A, const Group<R>&
                  : (BACKSUB && n.pslot < 0) ? v_prev : G.vbuf[(size_t)n.parent * 2 * kLanes];
     v_prev = V;
     R I, Gm;
-    channels<R, MS, INIT>(n.mask, V, dt, G.slab + (size_t)n.srow * kLanes, G.ptab + (size_t)n.prow * kLanes,
-                          I, Gm);
+    if constexpr (INIT) {
+        channels<R, MS, true>(n.mask, V, dt, G.slab + (size_t)n.srow * kLanes, G.ptab + (size_t)n.prow * kLanes,
+                              I, Gm);
+    } else {
+        const CurrentG<R> ig = channels_step<R, MS>(n.mask, V, dt, G.slab + (size_t)n.srow * kLanes,
+                                                   G.ptab + (size_t)n.prow * kLanes);
+        I = ig.I;
+        Gm = ig.G;
+    }
     if (INIT || BACKSUB) {
         vo[0] = V;
         vo[kLanes] = vc;
