@@ -45,6 +45,7 @@ enum { NGPU_FP32 = 0, NGPU_FP64 = 1 };
 
 typedef struct ngpu_model ngpu_model;
 typedef struct ngpu_sim ngpu_sim;
+typedef struct ngpu_batch ngpu_batch;
 
 const char *ngpu_last_error(void);
 int ngpu_abi_version(void);
@@ -141,6 +142,33 @@ int ngpu_sim_set_recording(ngpu_sim *s, int32_t n_rec, const int32_t *rec_nodes,
 int ngpu_sim_init(ngpu_sim *s, float v_init, void *cuda_stream);
 /* Steps [t0, t0 + n_steps) of the stimulus, enqueued on cuda_stream. */
 int ngpu_sim_advance(ngpu_sim *s, int32_t t0, int32_t n_steps, void *cuda_stream);
+
+/* As ngpu_sim_create with the CTA's warp count chosen by the caller (1..8;
+ * 0 = the library's choice from the morphology size).  The warp count sets
+ * how the tree is split over the CTA's warps; an autotuner picks it per
+ * morphology by timing. */
+int ngpu_sim_create_ex(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
+                       ngpu_sim **out);
+
+/*
+ * Several simulations in one launch (morphologies of different sizes, one
+ * mechanism set and precision): CTAs are dealt to the members in order, each
+ * runs its member's groups exactly as a separate launch would (bitwise the
+ * same results).  Members keep their own parameters, stimuli, recordings and
+ * traces (ngpu_sim_get_trace).  Up to 16 members.  The reference runs one
+ * morphology per process (U/CudaStuff.cu:518-587); no counterpart.
+ *   ngpu_batch_init       ngpu_sim_init of every member, one launch
+ *   ngpu_batch_advance    ngpu_sim_advance of every member, one launch
+ *   ngpu_batch_run_graph  init + ceil(nt/chunk) advance launches captured once
+ *                         as a CUDA graph on `cuda_stream` (non-default) and
+ *                         replayed; the capture is reused while the members'
+ *                         buffers, nt, chunk and stream are unchanged.
+ */
+int ngpu_batch_create(ngpu_sim *const *sims, int32_t n, ngpu_batch **out);
+int ngpu_batch_destroy(ngpu_batch *b);
+int ngpu_batch_init(ngpu_batch *b, float v_init, void *cuda_stream);
+int ngpu_batch_advance(ngpu_batch *b, int32_t t0, int32_t n_steps, void *cuda_stream);
+int ngpu_batch_run_graph(ngpu_batch *b, float v_init, int32_t nt, int32_t chunk, void *cuda_stream);
 /* Number of recorded samples per (instance, site): ceil(nt / rec_every). */
 int ngpu_sim_n_samples(const ngpu_sim *s);
 /* out [n_sets][n_stim][n_rec][n_samples]; on_device != 0: device pointer. */

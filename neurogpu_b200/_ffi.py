@@ -54,6 +54,12 @@ def lib() -> C.CDLL:
             "ngpu_model_split_info": (C.c_int, [P, I32, P, P, P, I32, P, P, I32, P, P]),
             "ngpu_run": (C.c_int, [P, I32, P, I32, I32, P, P, I32, F32, I32, P, F32, I32, P]),
             "ngpu_sim_create": (C.c_int, [P, I32, I32, I32, P]),
+            "ngpu_sim_create_ex": (C.c_int, [P, I32, I32, I32, I32, P]),
+            "ngpu_batch_create": (C.c_int, [P, I32, P]),
+            "ngpu_batch_destroy": (C.c_int, [P]),
+            "ngpu_batch_init": (C.c_int, [P, F32, P]),
+            "ngpu_batch_advance": (C.c_int, [P, I32, I32, P]),
+            "ngpu_batch_run_graph": (C.c_int, [P, F32, I32, I32, P]),
             "ngpu_sim_destroy": (C.c_int, [P]),
             "ngpu_sim_set_params": (C.c_int, [P, P, I32]),
             "ngpu_sim_set_stimulus": (C.c_int, [P, I32, P, P, I32, F32, I32]),

@@ -187,6 +187,21 @@ def hh_active(n_sets: int = 1024, t_stop: float = 500.0, dt: float = 0.025, n_co
                     np.array([0], dtype=np.int32), -70.0, mult, seed)
 
 
+def uneven_batch(n_sets: int = 8192, sizes=(200, 800, 1500, 3000), t_stop: float = 500.0, dt: float = 0.025,
+                 seed: int = 4, levels=(0.1, 0.2, 0.4, 0.7, 1.0)) -> list[Workload]:
+    """An uneven batch: seeded HH-type trees of the given compartment counts
+    (the hh_active channel set and parameter sampling), n_sets split evenly
+    over them, five step protocols shared by all (one instance = one set x
+    one protocol)."""
+    per = n_sets // len(sizes)
+    out = []
+    for k, n in enumerate(sizes):
+        w = hh_active(n_sets=per, t_stop=t_stop, dt=dt, n_comp=n, seed=seed * 100 + k, levels=levels)
+        w.name = f"uneven_{n}"
+        out.append(w)
+    return out
+
+
 # ----------------------------------------------------------------------- 3
 TTPC_REGIONS = ("soma", "axon", "basal", "trunk", "oblique", "tuft")
 TTPC_MECHS = {

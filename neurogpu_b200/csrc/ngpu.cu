@@ -374,6 +374,7 @@ struct ngpu_sim {
     float* d_amps = nullptr;
     float* d_dts = nullptr;
     float* d_trace = nullptr;
+    size_t trace_bytes = 0;
     float* d_tmp_out = nullptr;
     size_t tmp_out_bytes = 0;
     // stimulus / recording (internal node numbering)
@@ -761,7 +762,14 @@ static void sim_free(ngpu_sim* s) {
 
 int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision,
                     ngpu_sim** out) {
+    return ngpu_sim_create_ex(m, n_sets, n_stim, precision, 0, out);
+}
+
+int ngpu_sim_create_ex(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
+                       ngpu_sim** out) {
     if (!out) return fail(NGPU_E_INVALID, "out is null");
+    if (n_warps < 0 || n_warps > kMaxWarps)
+        return fail(NGPU_E_INVALID, "n_warps must be 0 (automatic) or 1.." + std::to_string(kMaxWarps));
     *out = nullptr;
     if (!m) return fail(NGPU_E_INVALID, "null model");
     if (n_sets < 1 || n_stim < 1) return fail(NGPU_E_INVALID, "need n_sets >= 1 and n_stim >= 1");
@@ -789,6 +797,7 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
     // warps per CTA and the tree split over them
     int W = std::min(8, std::max(1, m->n / 48));
     if (const char* ev = getenv("NGPU_WARPS")) W = std::max(1, std::min(kMaxWarps, atoi(ev)));
+    if (n_warps > 0) W = n_warps;
     W = std::min(W, m->n);
     s->n_warps = W;
     s->part = make_partition(m, W);
@@ -943,12 +952,14 @@ int ngpu_sim_set_recording(ngpu_sim* s, int32_t n_rec, const int32_t* rec_nodes,
     return NGPU_OK;
 }
 
-int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
+// Host side of an initialisation: node records with this run's split and
+// recording columns, the trace buffer (kept when its size is unchanged, so
+// the device addresses a captured graph holds stay valid), the error flags.
+static int sim_prepare_init(ngpu_sim* s, float v_init, cudaStream_t st) {
     if (!s) return fail(NGPU_E_INVALID, "null sim");
     if (!s->has_params) return fail(NGPU_E_STATE, "set_params must precede init");
     if (!s->has_stim) return fail(NGPU_E_STATE, "set_stimulus must precede init");
     if (!std::isfinite(v_init)) return fail(NGPU_E_INVALID, "v_init must be finite");
-    cudaStream_t st = (cudaStream_t)cuda_stream;
     const ngpu_model* m = s->m;
     // node records with this run's split and recording columns
     std::vector<int> uniq(s->n_rec_unique, -1);
@@ -983,13 +994,24 @@ int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
         NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
     }
     s->n_samples = (s->nt + s->rec_every - 1) / s->rec_every;
-    if (s->d_trace) cudaFree(s->d_trace);
-    s->d_trace = nullptr;
-    int rc = NGPU_OK;
-    s->d_trace = (float*)dmalloc(sizeof(float) * (size_t)s->n_samples * s->n_rec_unique * s->n_pad, &rc);
-    if (!s->d_trace) return rc;
+    const size_t tbytes = sizeof(float) * (size_t)s->n_samples * s->n_rec_unique * s->n_pad;
+    if (!s->d_trace || s->trace_bytes != tbytes) {
+        if (s->d_trace) cudaFree(s->d_trace);
+        s->d_trace = nullptr;
+        int rc = NGPU_OK;
+        s->d_trace = (float*)dmalloc(tbytes, &rc);
+        if (!s->d_trace) return rc;
+        s->trace_bytes = tbytes;
+    }
     NGPU_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(int) * s->n_pad, st));
     s->v_init = v_init;
+    return NGPU_OK;
+}
+
+int ngpu_sim_init(ngpu_sim* s, float v_init, void* cuda_stream) {
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const int rc = sim_prepare_init(s, v_init, st);
+    if (rc != NGPU_OK) return rc;
     cudaError_t e = s->precision == NGPU_FP64 ? launch_init<double>(s, st) : launch_init<float>(s, st);
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("init launch: ") + cudaGetErrorString(e));
     s->initialized = true;
@@ -1006,6 +1028,211 @@ int ngpu_sim_advance(ngpu_sim* s, int32_t t0, int32_t n_steps, void* cuda_stream
     cudaError_t e = s->precision == NGPU_FP64 ? launch_advance<double>(s, t0, n_steps, st)
                                               : launch_advance<float>(s, t0, n_steps, st);
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("advance launch: ") + cudaGetErrorString(e));
+    return NGPU_OK;
+}
+
+}  // extern "C"
+
+// ---- several simulations in one launch ------------------------------------
+struct ngpu_batch {
+    std::vector<ngpu_sim*> sims;
+    int precision = 0, mechset = 0, threads = 0, total_ctas = 0;
+    size_t smem = 0;
+    // a captured run (init + chunked advances), reused while its arguments hold
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> graph_key;
+    int graph_kernels = 0;  // kernels one replay launches
+};
+
+template <typename R>
+static BatchArgs<R> make_batch_args(ngpu_batch* b) {
+    BatchArgs<R> B;
+    memset((void*)&B, 0, sizeof(B));
+    B.n = (int)b->sims.size();
+    int c = 0;
+    for (int k = 0; k < B.n; ++k) {
+        B.sim[k] = make_args<R>(b->sims[k]);
+        B.cta0[k] = c;
+        c += b->sims[k]->n_groups;
+    }
+    B.cta0[B.n] = c;
+    return B;
+}
+
+template <typename R>
+static cudaError_t launch_batch(ngpu_batch* b, bool init, int t0, int n, cudaStream_t st) {
+    const BatchArgs<R> B = make_batch_args<R>(b);
+    cudaError_t e;
+    if (b->mechset == NGPU_MECHSET_TTPC) {
+        if (init) {
+            k_batch_init<R, 0><<<b->total_ctas, b->threads, 0, st>>>(B);
+        } else {
+            e = cudaFuncSetAttribute(k_batch_advance<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+            if (e != cudaSuccess) return e;
+            k_batch_advance<R, 0><<<b->total_ctas, b->threads, b->smem, st>>>(B, t0, n);
+        }
+    } else {
+        if (init) {
+            k_batch_init<R, 1><<<b->total_ctas, b->threads, 0, st>>>(B);
+        } else {
+            e = cudaFuncSetAttribute(k_batch_advance<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+            if (e != cudaSuccess) return e;
+            k_batch_advance<R, 1><<<b->total_ctas, b->threads, b->smem, st>>>(B, t0, n);
+        }
+    }
+    g_launches++;
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_batch_any(ngpu_batch* b, bool init, int t0, int n, cudaStream_t st) {
+    return b->precision == NGPU_FP64 ? launch_batch<double>(b, init, t0, n, st)
+                                     : launch_batch<float>(b, init, t0, n, st);
+}
+
+static void batch_drop_graph(ngpu_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->graph_key.clear();
+}
+
+extern "C" {
+
+int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
+    if (!out) return fail(NGPU_E_INVALID, "out is null");
+    *out = nullptr;
+    if (!sims || n < 1 || n > kMaxBatch)
+        return fail(NGPU_E_INVALID, "a batch holds 1.." + std::to_string(kMaxBatch) + " simulations");
+    for (int k = 0; k < n; ++k) {
+        if (!sims[k]) return fail(NGPU_E_INVALID, "null simulation in the batch");
+        for (int j = 0; j < k; ++j)
+            if (sims[j] == sims[k]) return fail(NGPU_E_INVALID, "a simulation appears twice in the batch");
+        if (sims[k]->precision != sims[0]->precision)
+            return fail(NGPU_E_INVALID, "a batch needs one precision");
+        if (sims[k]->m->mechset != sims[0]->m->mechset)
+            return fail(NGPU_E_INVALID, "a batch needs one mechanism set");
+    }
+    ngpu_batch* b = new (std::nothrow) ngpu_batch();
+    if (!b) return fail(NGPU_E_NOMEM, "host allocation failed");
+    b->sims.assign(sims, sims + n);
+    b->precision = sims[0]->precision;
+    b->mechset = sims[0]->m->mechset;
+    int W = 1;
+    for (ngpu_sim* s : b->sims) {
+        W = std::max(W, s->n_warps);
+        b->total_ctas += s->n_groups;
+        b->smem = std::max(b->smem, b->precision == NGPU_FP64 ? SmemPlan<double>::bytes(s->m->n)
+                                                             : SmemPlan<float>::bytes(s->m->n));
+    }
+    b->threads = kLanes * W;
+    *out = b;
+    return NGPU_OK;
+}
+
+int ngpu_batch_destroy(ngpu_batch* b) {
+    if (b) batch_drop_graph(b);
+    delete b;
+    return NGPU_OK;
+}
+
+static int batch_check_steps(ngpu_batch* b, int t0, int n) {
+    for (ngpu_sim* s : b->sims) {
+        if (!s->initialized) return fail(NGPU_E_STATE, "init must precede advance");
+        if (t0 < 0 || n < 0 || (int64_t)t0 + n > s->nt)
+            return fail(NGPU_E_INVALID, "step range outside a member's stimulus");
+    }
+    return NGPU_OK;
+}
+
+int ngpu_batch_init(ngpu_batch* b, float v_init, void* cuda_stream) {
+    if (!b) return fail(NGPU_E_INVALID, "null batch");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    for (ngpu_sim* s : b->sims) {
+        const int rc = sim_prepare_init(s, v_init, st);
+        if (rc != NGPU_OK) return rc;
+    }
+    const cudaError_t e = launch_batch_any(b, true, 0, 0, st);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("batch init launch: ") + cudaGetErrorString(e));
+    for (ngpu_sim* s : b->sims) s->initialized = true;
+    return NGPU_OK;
+}
+
+int ngpu_batch_advance(ngpu_batch* b, int32_t t0, int32_t n_steps, void* cuda_stream) {
+    if (!b) return fail(NGPU_E_INVALID, "null batch");
+    const int rc = batch_check_steps(b, t0, n_steps);
+    if (rc != NGPU_OK) return rc;
+    if (n_steps == 0) return NGPU_OK;
+    const cudaError_t e = launch_batch_any(b, false, t0, n_steps, (cudaStream_t)cuda_stream);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("batch advance launch: ") + cudaGetErrorString(e));
+    return NGPU_OK;
+}
+
+int ngpu_batch_run_graph(ngpu_batch* b, float v_init, int32_t nt, int32_t chunk, void* cuda_stream) {
+    if (!b) return fail(NGPU_E_INVALID, "null batch");
+    if (nt < 1 || chunk < 1) return fail(NGPU_E_INVALID, "need nt >= 1 and chunk >= 1");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    for (ngpu_sim* s : b->sims) {
+        const int rc = sim_prepare_init(s, v_init, st);
+        if (rc != NGPU_OK) return rc;
+        if (nt > s->nt) return fail(NGPU_E_INVALID, "nt beyond a member's stimulus");
+    }
+    // the graph bakes in every launch argument: reuse it only for the same ones
+    std::vector<unsigned char> key;
+    auto add = [&](const void* p, size_t bytes) {
+        const unsigned char* c = (const unsigned char*)p;
+        key.insert(key.end(), c, c + bytes);
+    };
+    if (b->precision == NGPU_FP64) {
+        const BatchArgs<double> B = make_batch_args<double>(b);
+        add(&B, sizeof(B));
+    } else {
+        const BatchArgs<float> B = make_batch_args<float>(b);
+        add(&B, sizeof(B));
+    }
+    add(&nt, sizeof(nt));
+    add(&chunk, sizeof(chunk));
+    add(&st, sizeof(st));
+    if (!b->exec || key != b->graph_key) {
+        batch_drop_graph(b);
+        // set the shared-memory attribute outside the capture
+        cudaError_t e = cudaSuccess;
+        if (b->precision == NGPU_FP64)
+            e = b->mechset == NGPU_MECHSET_TTPC
+                    ? cudaFuncSetAttribute(k_batch_advance<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem)
+                    : cudaFuncSetAttribute(k_batch_advance<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+        else
+            e = b->mechset == NGPU_MECHSET_TTPC
+                    ? cudaFuncSetAttribute(k_batch_advance<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem)
+                    : cudaFuncSetAttribute(k_batch_advance<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+        if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("batch attribute: ") + cudaGetErrorString(e));
+        if (!st) return fail(NGPU_E_INVALID, "graph capture needs a non-default stream");
+        e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+        const auto before = g_launches.load();
+        cudaError_t le = launch_batch_any(b, true, 0, 0, st);
+        for (int t0 = 0; le == cudaSuccess && t0 < nt; t0 += chunk)
+            le = launch_batch_any(b, false, t0, std::min(chunk, nt - t0), st);
+        b->graph_kernels = (int)(g_launches.load() - before);
+        g_launches -= b->graph_kernels;  // captured, not run
+        e = cudaStreamEndCapture(st, &b->graph);
+        if (le != cudaSuccess || e != cudaSuccess) {
+            batch_drop_graph(b);
+            return fail(NGPU_E_CUDA, std::string("graph capture: ") +
+                                         cudaGetErrorString(le != cudaSuccess ? le : e));
+        }
+        e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        if (e != cudaSuccess) {
+            batch_drop_graph(b);
+            return fail(NGPU_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        b->graph_key = key;
+    }
+    const cudaError_t e = cudaGraphLaunch(b->exec, st);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+    g_launches += b->graph_kernels;
+    for (ngpu_sim* s : b->sims) s->initialized = true;
     return NGPU_OK;
 }
 

@@ -165,8 +165,8 @@ struct Group {  // per-CTA pointers (lane offset included)
 };
 
 template <typename R>
-__device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A) {
-    const int g = blockIdx.x, lane = threadIdx.x & 31;
+__device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A, int g) {
+    const int lane = threadIdx.x & 31;
     const size_t N = (size_t)A.n_nodes;
     Group<R> p;
     p.vbuf = A.vbuf + (size_t)g * N * 2 * kLanes + lane;
@@ -346,10 +346,13 @@ __device__ __forceinline__ const NodeRec<R>* stage_nodes(const SimArgs<R>& A, ch
     return nr;
 }
 
+// Initial state of group g: channels at steady state for v_init, the first
+// step's rows, sample 0.  Nodes are independent here, so any number of warps
+// shares them.
 template <typename R, int MS>
-__global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
-    const Group<R> G = group_of(A);
-    const int w = threadIdx.x >> 5;
+__device__ __forceinline__ void init_body(const SimArgs<R>& A, int g) {
+    const Group<R> G = group_of(A, g);
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (w == 0)
         for (int j = 0; j < 2 * A.n_jslots; ++j) G.jacc[(size_t)j * kLanes] = 0.0;
     R dt, dtn_inv, istim_amp;
@@ -357,10 +360,15 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
     float* trace;
     step_inputs(A, G, 0, true, dt, dtn_inv, istim_amp, rec_now, trace);
     R xd = 0, vd = 0;
-    for (int i = w; i < A.n_nodes; i += A.n_warps)
+    for (int i = w; i < A.n_nodes; i += nw)
         update_node<R, MS, true, false>(A, G, A.nodes[i], i, dt, dtn_inv, istim_amp, rec_now, trace, xd, vd,
                                         nullptr);
     if (w == 0) A.bad[G.inst] = 0;
+}
+
+template <typename R, int MS>
+__global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
+    init_body<R, MS>(A, blockIdx.x);
 }
 
 // Segment item, S1: leaf -> root elimination of the spine r..l-1 after its
@@ -445,11 +453,12 @@ __device__ __forceinline__ int next_item(int* ctr) {
 //       update + next-step assembly of every node of the item (a segment
 //       also does its lower separator's channels, which need the spine's new
 //       V); separators linked directly to the skeleton are items too
+// n_steps timesteps of group g; the items are shared by however many warps
+// the CTA has (the split was sized for A.n_warps).
 template <typename R, int MS>
-__global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim_advance(SimArgs<R> A, int t0, int n_steps) {
-    extern __shared__ __align__(128) char smem[];
-    __shared__ int ctr[2];
-    const Group<R> G = group_of(A);
+__device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0, int n_steps, char* smem,
+                                             int* ctr) {
+    const Group<R> G = group_of(A, g);
     const int w = threadIdx.x >> 5;
     const NodeRec<R>* nr = stage_nodes(A, smem);
     if (threadIdx.x == 0) { ctr[0] = 0; ctr[1] = 0; }
@@ -561,6 +570,46 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim
         __syncthreads();
     }
     if (w == 0 && bad) A.bad[G.inst] = 1;
+}
+
+template <typename R, int MS>
+__global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim_advance(SimArgs<R> A, int t0, int n_steps) {
+    extern __shared__ __align__(128) char smem[];
+    __shared__ int ctr[2];
+    advance_body<R, MS>(A, blockIdx.x, t0, n_steps, smem, ctr);
+}
+
+// Several simulations (morphologies of different sizes, one mechanism set)
+// in one launch: CTAs [cta0[k], cta0[k+1]) run the groups of simulation k.
+// The arguments live in the kernel's parameter space (__grid_constant__), so
+// a CTA reads its simulation's fields through the constant cache.
+constexpr int kMaxBatch = 16;
+template <typename R>
+struct BatchArgs {
+    SimArgs<R> sim[kMaxBatch];
+    int cta0[kMaxBatch + 1];
+    int n;
+};
+
+__device__ __forceinline__ int batch_member(const int* cta0, int n) {
+    int k = 0;
+    while (k + 1 < n && (int)blockIdx.x >= cta0[k + 1]) ++k;
+    return k;
+}
+
+template <typename R, int MS>
+__global__ void __launch_bounds__(kLanes * kMaxWarps) k_batch_init(const __grid_constant__ BatchArgs<R> B) {
+    const int k = batch_member(B.cta0, B.n);
+    init_body<R, MS>(B.sim[k], blockIdx.x - B.cta0[k]);
+}
+
+template <typename R, int MS>
+__global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS)
+    k_batch_advance(const __grid_constant__ BatchArgs<R> B, int t0, int n_steps) {
+    extern __shared__ __align__(128) char smem[];
+    __shared__ int ctr[2];
+    const int k = batch_member(B.cta0, B.n);
+    advance_body<R, MS>(B.sim[k], blockIdx.x - B.cta0[k], t0, n_steps, smem, ctr);
 }
 
 // Parameter table: ptab[g][row][lane] = params[set][row_param[row]][row_sec[row]]

@@ -111,13 +111,16 @@ class Model:
 class Simulator:
     """Resident simulation of n_sets x n_stim instances of one model."""
 
-    def __init__(self, model: Model | CellModel, n_sets: int, n_stim: int, precision: str = "fp32"):
+    def __init__(self, model: Model | CellModel, n_sets: int, n_stim: int, precision: str = "fp32",
+                 n_warps: int = 0):
+        """n_warps: warps per CTA (1..8), 0 = the library's choice; see
+        neurogpu_b200.autotune for timing-based selection."""
         self.model = model if isinstance(model, Model) else Model(model)
         self.n_sets, self.n_stim = int(n_sets), int(n_stim)
         self.precision = precision
         h = C.c_void_p()
-        _ffi.check("ngpu_sim_create", _ffi.lib().ngpu_sim_create(
-            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], C.byref(h)))
+        _ffi.check("ngpu_sim_create_ex", _ffi.lib().ngpu_sim_create_ex(
+            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], int(n_warps), C.byref(h)))
         self._h = h
         self.nt = 0
         self.n_rec = 1
@@ -210,3 +213,39 @@ def run(cell: CellModel | Model, params, amps, dts, stim_node: int, stim_area_um
         int(stim_node), float(stim_area_um2), r.size, _ffi.ptr(r), float(v_init),
         _PREC[precision], _ffi.ptr(out)))
     return out
+
+
+class Batch:
+    """Several Simulators (different morphologies, one mechanism set and
+    precision) advanced by single launches (ngpu_batch_*).  Each member
+    keeps its own parameters, stimulus, recording and trace."""
+
+    def __init__(self, sims: list[Simulator]):
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(self.sims))(*[s._h for s in self.sims])
+        h = C.c_void_p()
+        _ffi.check("ngpu_batch_create", _ffi.lib().ngpu_batch_create(arr, len(self.sims), C.byref(h)))
+        self._h = h
+
+    def init(self, v_init: float, stream=None) -> None:
+        _ffi.check("ngpu_batch_init", _ffi.lib().ngpu_batch_init(self._h, float(v_init), _stream_ptr(stream)))
+
+    def advance(self, t0: int, n_steps: int, stream=None) -> None:
+        _ffi.check("ngpu_batch_advance", _ffi.lib().ngpu_batch_advance(
+            self._h, int(t0), int(n_steps), _stream_ptr(stream)))
+
+    def run_graph(self, v_init: float, nt: int, chunk: int, stream) -> None:
+        """init + every advance chunk as one CUDA graph on a non-default stream."""
+        _ffi.check("ngpu_batch_run_graph", _ffi.lib().ngpu_batch_run_graph(
+            self._h, float(v_init), int(nt), int(chunk), _stream_ptr(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _ffi.lib().ngpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
