@@ -213,6 +213,22 @@ int ngpu_run_static(ngpu_model *m, int32_t n_sets, const float *params_dev, int3
 /* Kernel launches issued by this thread since the last call (for accounting). */
 int64_t ngpu_launch_count(int32_t reset);
 
+/*
+ * BF16 tensor-core GEMM (tcgen05) of the surrogate network, device pointers:
+ *   D[M][N] = A[M][K] . B[N][K]^T, A and B bf16 row-major (K contiguous),
+ *   K a multiple of 64, lda/ldb multiples of 8, 16-byte aligned; fp32
+ *   accumulation.  epilogue: 0 out_f32 = D; 1 z = D + bias: out_f32 = z,
+ *   out_bf16 = gelu(z) (tanh form) and its transpose out_bf16_t[n][m];
+ *   2 out_f32 = D + bias; 3 dz = D * gelu'(zin): out_bf16 = dz and
+ *   out_bf16_t = dz^T.  bn: the N tile (32, 64, 128, 256).  A wait that
+ *   exceeds its bound sets a device flag read (and cleared) by
+ *   ngpu_gemm_error.  No counterpart in the reference.
+ */
+int ngpu_gemm_bf16_tn(const void *A, const void *B, int32_t M, int32_t N, int32_t K, int32_t lda, int32_t ldb,
+                      int32_t epilogue, int32_t bn, float *out_f32, void *out_bf16, void *out_bf16_t, int32_t ldo,
+                      int32_t ldt, const float *bias, const float *zin, void *cuda_stream);
+int ngpu_gemm_error(int32_t *flag);
+
 #ifdef __cplusplus
 }
 #endif

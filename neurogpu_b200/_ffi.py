@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
             "ngpu_batch_init": (C.c_int, [P, F32, P]),
             "ngpu_batch_advance": (C.c_int, [P, I32, I32, P]),
             "ngpu_batch_run_graph": (C.c_int, [P, F32, I32, I32, P]),
+            "ngpu_gemm_bf16_tn": (C.c_int, [P, P, I32, I32, I32, I32, I32, I32, I32, P, P, P, I32, I32, P, P, P]),
+            "ngpu_gemm_error": (C.c_int, [P]),
             "ngpu_sim_destroy": (C.c_int, [P]),
             "ngpu_sim_set_params": (C.c_int, [P, P, I32]),
             "ngpu_sim_set_stimulus": (C.c_int, [P, I32, P, P, I32, F32, I32]),

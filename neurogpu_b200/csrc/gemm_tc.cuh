@@ -1,0 +1,262 @@
+// BF16 tensor-core GEMM for the surrogate network (tcgen05, sm_100a).
+//
+//   D[M][N] = A[M][K] . B[N][K]^T     (A, B bf16, both K-major; D fp32 in TMEM)
+//
+// One CTA of 128 threads computes a 128 x BN tile.  K advances in tiles of
+// 64: all threads copy the next A / B tiles into a two-stage shared-memory
+// ring with cp.async (rows past M read as zeros) while the previous tile's
+// MMAs run; one thread issues four tcgen05.mma (K = 16 each) per tile and
+// commits them to that stage's mbarrier, which the copy into the stage waits
+// on before overwriting it.  The accumulator lives in tensor memory (BN fp32
+// columns x 128 lanes); after the last commit each warp reads its 32 lanes
+// with tcgen05.ld and applies the epilogue.
+//
+// Shared-memory operand layout (no swizzle, K-major canonical layout): an
+// 8-row x 16-byte core matrix is 128 contiguous bytes; core matrices along K
+// are LBO = 128 bytes apart, blocks of 8 rows SBO = 8 x 128 = 1024 bytes
+// apart, so one 64-wide K tile of 128 rows is 16 KB.  Descriptor fields
+// (start >> 4, LBO >> 4 at bit 16, SBO >> 4 at bit 32, version 1 at bit 46,
+// swizzle 0 at bit 61) and the kind::f16 instruction descriptor (F32
+// accumulator, BF16 A and B, K-major both, N >> 3 at bit 17, M >> 4 at
+// bit 24) follow the PTX ISA's tcgen05 matrix and instruction descriptors.
+//
+// Every wait is bounded: past the limit the kernel records an error in
+// *err, skips the epilogue and still frees its tensor memory.
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace ngpu {
+
+constexpr int kGemmThreads = 128;
+constexpr int kGemmBM = 128;
+constexpr int kGemmBK = 64;
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+enum GemmEpilogue : int {
+    kEpiStore = 0,      // out_f32[m][n] = D
+    kEpiBiasGelu = 1,   // z = D + bias[n]: out_f32 = z, out_bf16 = gelu(z), out_bf16_t[n][m] = gelu(z)
+    kEpiBias = 2,       // out_f32[m][n] = D + bias[n]
+    kEpiGeluGrad = 3,   // dz = D * gelu'(zin[m][n]): out_bf16 = dz, out_bf16_t[n][m] = dz
+};
+
+struct GemmArgs {
+    const __nv_bfloat16* A;  // [M][lda]
+    const __nv_bfloat16* B;  // [N][ldb]
+    int M, N, K, lda, ldb;
+    float* out_f32;          // [M][ldo]
+    __nv_bfloat16* out_bf16; // [M][ldo]
+    __nv_bfloat16* out_bf16_t;  // [N][ldt]
+    int ldo, ldt;
+    const float* bias;       // [N]
+    const float* zin;        // [M][ldo]
+    int* err;
+};
+
+__device__ __forceinline__ float gelu_tanh(float z) {
+    const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+    return 0.5f * z * (1.0f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_tanh_grad(float z) {
+    const float z2 = z * z;
+    const float u = 0.7978845608028654f * (z + 0.044715f * z2 * z);
+    const float t = tanhf(u);
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z2);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    const uint64_t lbo = 128 >> 4, sbo = 1024 >> 4;
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+template <int BN>
+__device__ __forceinline__ constexpr uint32_t umma_idesc() {
+    return (1u << 4)                      // D: F32
+           | (1u << 7) | (1u << 10)       // A, B: BF16
+           | ((uint32_t)(BN >> 3) << 17)  // N
+           | ((uint32_t)(kGemmBM >> 4) << 24);  // M = 128
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// true when the phase completed, false after kSpinLimit polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    const int n = valid ? 16 : 0;  // 0: fill with zeros
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+
+// Copy one 64-wide K tile of `rows` rows (row r of the tile at src + r * ld)
+// into the core-matrix layout at dst; rows >= rows_valid read as zeros.
+template <int ROWS>
+__device__ __forceinline__ void load_tile(uint32_t dst, const __nv_bfloat16* src, int ld, int rows_valid) {
+    constexpr int kVec = ROWS * (kGemmBK / 8);  // 16-byte vectors
+#pragma unroll
+    for (int v = threadIdx.x; v < kVec; v += kGemmThreads) {
+        const int row = v >> 3, kg = v & 7;
+        const uint32_t off = (uint32_t)((row >> 3) * 1024 + kg * 128 + (row & 7) * 16);
+        const bool ok = row < rows_valid;
+        const __nv_bfloat16* p = src + (size_t)(ok ? row : 0) * ld + kg * 8;
+        cp_async16(dst + off, p, ok);
+    }
+}
+
+template <int BN>
+struct GemmSmem {
+    alignas(1024) unsigned char a[2][kGemmBM * kGemmBK * 2];
+    alignas(1024) unsigned char b[2][BN * kGemmBK * 2];
+    alignas(8) uint64_t bar[2];
+    uint32_t tmem;
+};
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
+    static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "BN: a multiple of 16 in [32, 256]");
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // align the ring to 1024 bytes (descriptor base offset 0)
+    GemmSmem<BN>& S = *reinterpret_cast<GemmSmem<BN>*>(
+        (void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
+    constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // power of two >= 32 for BN in {32, 64, 128, 256}
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&S.bar[0]), 1);
+        mbar_init(smem_u32(&S.bar[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = S.tmem;
+
+    const int KT = g.K / kGemmBK;
+    const int rows_a = min(kGemmBM, g.M - m0), rows_b = min(BN, g.N - n0);
+    const __nv_bfloat16* Ab = g.A + (size_t)m0 * g.lda;
+    const __nv_bfloat16* Bb = g.B + (size_t)n0 * g.ldb;
+    uint32_t phase[2] = {0, 0};
+    bool ok = true;
+
+    load_tile<kGemmBM>(smem_u32(S.a[0]), Ab, g.lda, rows_a);
+    load_tile<BN>(smem_u32(S.b[0]), Bb, g.ldb, rows_b);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt & 1;
+        if (kt + 1 < KT) {
+            const int sn = (kt + 1) & 1;
+            if (kt >= 1) {  // the MMAs of tile kt-1 read stage sn
+                ok = ok && mbar_wait(smem_u32(&S.bar[sn]), phase[sn]);
+                phase[sn] ^= 1;
+            }
+            load_tile<kGemmBM>(smem_u32(S.a[sn]), Ab + (size_t)(kt + 1) * kGemmBK, g.lda, rows_a);
+            load_tile<BN>(smem_u32(S.b[sn]), Bb + (size_t)(kt + 1) * kGemmBK, g.ldb, rows_b);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async data -> tensor core reads
+        __syncthreads();
+        if (threadIdx.x == 0 && ok) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(S.a[s]), sb = smem_u32(S.b[s]);
+#pragma unroll
+            for (int k = 0; k < kGemmBK / 16; ++k) {  // K = 16 per MMA: two core matrices along K
+                const uint64_t da = umma_desc(sa + k * 256), db = umma_desc(sb + k * 256);
+                const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(umma_idesc<BN>()), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&S.bar[s]))
+                         : "memory");
+        }
+        __syncthreads();
+    }
+    // the last commit covers every MMA this thread issued
+    if (KT > 0) {
+        const int s = (KT - 1) & 1;
+        ok = ok && mbar_wait(smem_u32(&S.bar[s]), phase[s]);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    ok = __syncthreads_and(ok);
+
+    if (ok) {
+        const int m = m0 + warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(trow + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < g.M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= g.N) continue;
+                    const float d = __uint_as_float(r[j]);
+                    if constexpr (EPI == kEpiStore) {
+                        g.out_f32[(size_t)m * g.ldo + n] = d;
+                    } else if constexpr (EPI == kEpiBias) {
+                        g.out_f32[(size_t)m * g.ldo + n] = d + g.bias[n];
+                    } else if constexpr (EPI == kEpiBiasGelu) {
+                        const float z = d + g.bias[n];
+                        const __nv_bfloat16 h = __float2bfloat16_rn(gelu_tanh(z));
+                        g.out_f32[(size_t)m * g.ldo + n] = z;
+                        g.out_bf16[(size_t)m * g.ldo + n] = h;
+                        g.out_bf16_t[(size_t)n * g.ldt + m] = h;
+                    } else {  // kEpiGeluGrad
+                        const float dz = d * gelu_tanh_grad(g.zin[(size_t)m * g.ldo + n]);
+                        const __nv_bfloat16 h = __float2bfloat16_rn(dz);
+                        g.out_bf16[(size_t)m * g.ldo + n] = h;
+                        g.out_bf16_t[(size_t)n * g.ldt + m] = h;
+                    }
+                }
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicExch(g.err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+template <int BN>
+constexpr size_t gemm_smem_bytes() {
+    return sizeof(GemmSmem<BN>) + 1024;
+}
+
+}  // namespace ngpu

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/ngpu.h"
+#include "gemm_tc.cuh"
 #include "sim_kernels.cuh"
 
 using namespace ngpu;
@@ -1556,5 +1557,72 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
         g_launches++;
     }
     NGPU_CUDA(cudaGetLastError());
+    return NGPU_OK;
+}
+
+// ---- BF16 tensor-core GEMM (surrogate network) -------------------------------
+static __device__ int g_gemm_err;
+
+template <int BN, int EPI>
+static cudaError_t launch_gemm_bn(const GemmArgs& g, cudaStream_t st) {
+    const size_t smem = gemm_smem_bytes<BN>();
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tn<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + BN - 1) / BN);
+    k_gemm_bf16_tn<BN, EPI><<<grid, kGemmThreads, smem, st>>>(g);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+template <int EPI>
+static cudaError_t launch_gemm_epi(const GemmArgs& g, int bn, cudaStream_t st) {
+    switch (bn) {
+        case 32: return launch_gemm_bn<32, EPI>(g, st);
+        case 64: return launch_gemm_bn<64, EPI>(g, st);
+        case 128: return launch_gemm_bn<128, EPI>(g, st);
+        default: return launch_gemm_bn<256, EPI>(g, st);
+    }
+}
+
+extern "C" int ngpu_gemm_bf16_tn(const void* A, const void* B, int32_t M, int32_t N, int32_t K, int32_t lda,
+                                 int32_t ldb, int32_t epilogue, int32_t bn, float* out_f32, void* out_bf16,
+                                 void* out_bf16_t, int32_t ldo, int32_t ldt, const float* bias, const float* zin,
+                                 void* cuda_stream) {
+    if (!A || !B) return fail(NGPU_E_INVALID, "gemm: null operand");
+    if (M < 1 || N < 1 || K < kGemmBK || K % kGemmBK)
+        return fail(NGPU_E_INVALID, "gemm: need M, N >= 1 and K a positive multiple of 64");
+    if (lda < K || ldb < K || lda % 8 || ldb % 8)
+        return fail(NGPU_E_INVALID, "gemm: leading dimensions must be >= K and multiples of 8");
+    if (((uintptr_t)A | (uintptr_t)B) & 15) return fail(NGPU_E_INVALID, "gemm: operands must be 16-byte aligned");
+    if (bn != 32 && bn != 64 && bn != 128 && bn != 256) return fail(NGPU_E_INVALID, "gemm: bn must be 32, 64, 128 or 256");
+    const bool need_f32 = epilogue == kEpiStore || epilogue == kEpiBias || epilogue == kEpiBiasGelu;
+    const bool need_bf16 = epilogue == kEpiBiasGelu || epilogue == kEpiGeluGrad;
+    if ((need_f32 && !out_f32) || (need_bf16 && (!out_bf16 || !out_bf16_t)) ||
+        ((epilogue == kEpiBias || epilogue == kEpiBiasGelu) && !bias) || (epilogue == kEpiGeluGrad && !zin))
+        return fail(NGPU_E_INVALID, "gemm: missing output / bias / pre-activation for the epilogue");
+    if (ldo < N || (need_bf16 && ldt < M)) return fail(NGPU_E_INVALID, "gemm: output leading dimension too small");
+    int* err = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&err, g_gemm_err);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("gemm: ") + cudaGetErrorString(e));
+    GemmArgs g{(const __nv_bfloat16*)A, (const __nv_bfloat16*)B, M, N, K, lda, ldb, out_f32,
+               (__nv_bfloat16*)out_bf16, (__nv_bfloat16*)out_bf16_t, ldo, ldt, bias, zin, err};
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    switch (epilogue) {
+        case kEpiStore: e = launch_gemm_epi<kEpiStore>(g, bn, st); break;
+        case kEpiBiasGelu: e = launch_gemm_epi<kEpiBiasGelu>(g, bn, st); break;
+        case kEpiBias: e = launch_gemm_epi<kEpiBias>(g, bn, st); break;
+        case kEpiGeluGrad: e = launch_gemm_epi<kEpiGeluGrad>(g, bn, st); break;
+        default: return fail(NGPU_E_INVALID, "gemm: unknown epilogue");
+    }
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("gemm launch: ") + cudaGetErrorString(e));
+    return NGPU_OK;
+}
+
+extern "C" int ngpu_gemm_error(int32_t* flag) {
+    int v = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_gemm_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_gemm_err, &zero, sizeof(int));
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("gemm error flag: ") + cudaGetErrorString(e));
+    if (flag) *flag = v;
     return NGPU_OK;
 }
