@@ -56,7 +56,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-sets", type=int, default=16)
     ap.add_argument("--cpu-sample-steps", type=int, default=400)
-    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch"],
+    ap.add_argument("--ga-pop", type=int, default=8192)
+    ap.add_argument("--ga-gens", type=int, default=20)
+    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga"],
                     help="uneven_batch: 8192 sets over 200/800/1500/3000-compartment trees x 5 protocols, "
                          "one launch per chunk, the run captured as a CUDA graph (auxiliary line)")
     return ap.parse_args()
@@ -282,10 +284,42 @@ def run_uneven(args):
     batch.close()
 
 
+def run_ga(args):
+    """Config-5 line: GA time-to-score, surrogate-screened vs plain, on one
+    GPU.  Both fit the same 12 parameters of the 500-node HH-type cell to a
+    target's features over 3 step protocols (500 ms, dt 0.025 ms); the plain
+    GA simulates every offspring, the screened GA only the surrogate's top
+    10 % (its wall time includes simulating its training set and training
+    the network).  value = the screened GA's time to reach the plain GA's
+    final best score (s)."""
+    from neurogpu_b200 import ga
+    prob = ga.FitProblem()
+    plain = ga.run_plain(prob, args.ga_pop, args.ga_gens, seed=1)
+    sims_plain = prob.sim_count
+    prob.sim_count = 0
+    scr = ga.run_screened(prob, args.ga_pop, args.ga_gens, seed=1)
+    target = plain.best[-1]
+    t_scr = scr.time_to(target)
+    print(json.dumps({
+        "metric": "GA time-to-score (surrogate-screened vs plain)", "value": t_scr, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.ga_gens, "warmup": 0, "dtype": "f32 sim, bf16 net",
+        "data": "synthetic (seeded)", "vs_baseline": None,
+        "config": {"workload": "ga", "population": args.ga_pop, "generations": args.ga_gens,
+                   "model": "hh 500 compartments, 12 parameters, 3 protocols x 500 ms", "screen_keep": 0.1},
+        "plain": {"final_best": target, "seconds": plain.time[-1], "simulations": sims_plain,
+                  "best_per_generation": plain.best},
+        "screened": {"final_best": scr.best[-1], "seconds": scr.time[-1], "simulations": prob.sim_count,
+                     "best_per_generation": scr.best, "time_per_generation": scr.time,
+                     "surrogate_error_per_generation": [(g, round(e, 4), k) for g, e, k in scr.notes]},
+        "time_ratio": None if t_scr is None else t_scr / plain.time[-1]}))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ga":
+        return run_ga(args)
     if args.workload == "uneven_batch":
         return run_uneven(args)
     import torch
