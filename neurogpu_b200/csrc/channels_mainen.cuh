@@ -32,8 +32,8 @@ struct Mainen {
 };
 
 // One node, three phases (load every row / compute / store), as ttpc_node.
-template <typename R, bool INIT>
-NGPU_HD void mainen_node(uint32_t mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,
+template <typename R, bool INIT, typename MK>
+NGPU_HD void mainen_node(MK mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,
                          R& G) {
     using M = Math<R>;
     constexpr int S = 32;

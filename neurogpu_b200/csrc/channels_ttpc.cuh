@@ -190,8 +190,8 @@ struct TTPCRates {
 //            CaDynamics update)
 // st: the node's first state row (row stride 32 elements); pr: its first
 // parameter row.  Returns I (mA/cm2) and G = dI/dv.
-template <typename R, bool INIT>
-NGPU_HD void ttpc_node(uint32_t mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,
+template <typename R, bool INIT, typename MK>
+NGPU_HD void ttpc_node(MK mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,
                        R& G) {
     using Q = TTPCRates<R>;
     using M = Math<R>;

@@ -981,8 +981,10 @@ static int sim_prepare_init(ngpu_sim* s, float v_init, cudaStream_t st) {
             q.rec = (int16_t)rec[i];
             q.mask = (uint16_t)m->mask[i];
             q.prow = (uint16_t)m->info[i].prow;
-            q.srows = (uint16_t)m->rows[i].x;
-            q.prows = (uint16_t)m->rows[i].y;
+            q.srows = (uint8_t)m->rows[i].x;
+            q.prows = (uint8_t)m->rows[i].y;
+            q.cls = (uint8_t)node_class(m->mechset, (uint32_t)m->mask[i]);
+            q.pad_ = 0;
         }
     };
     if (s->precision == NGPU_FP64) {
@@ -1450,8 +1452,10 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
         q.rec = -1;
         q.mask = (uint16_t)m->mask[i];
         q.prow = (uint16_t)m->info[i].prow;
-        q.srows = (uint16_t)m->rows[i].x;
-        q.prows = (uint16_t)m->rows[i].y;
+        q.srows = (uint8_t)m->rows[i].x;
+        q.prows = (uint8_t)m->rows[i].y;
+        q.cls = (uint8_t)node_class(m->mechset, (uint32_t)m->mask[i]);
+        q.pad_ = 0;
     }
     for (int k = 0; k < n_rec_u; ++k) recs[rec_col_of_node[k]].rec = (int16_t)k;
     for (int k = 0; k < n_pad; ++k) inst_stim[k] = std::min(k, n_inst - 1) % n_stim;

@@ -52,6 +52,15 @@ template <> struct Math<double> {
     static NGPU_HD double one_minus_exp_neg(double z) { return -expm1(-z); }
 };
 
+// Index of the lowest set bit of m (m != 0).
+NGPU_HD int low_bit(uint32_t m) {
+#ifdef __CUDA_ARCH__
+    return __ffs((int)m) - 1;
+#else
+    return __builtin_ctz(m);
+#endif
+}
+
 // cnexp update of a first-order gate: x += (1 - exp(-dt/tau)) (xinf - x).
 template <typename R>
 NGPU_HD R cnexp(R x, R xinf, R tau, R dt) {

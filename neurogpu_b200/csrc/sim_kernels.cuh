@@ -13,15 +13,19 @@
 // the new V (:324-326), channel currents (:262-267) and the assembly of the
 // next step's diagonal and right-hand side (:268-291).
 //
-// The tree is split once on the host into a small "top tree" (containing the
-// root) and subtrees hanging off it, bin-packed over the CTA's W warps by
-// channel cost.  Subtrees are contiguous node ranges in Hines (depth-first)
-// order and independent given their top-tree parent, so elimination and
-// back-substitution of the subtrees run on all warps at once; warp 0 solves
-// only the top tree in between (S1 / S2 / S3 below).  A chain child hands its
-// elimination term to node i-1 in registers; any other child (branch
-// junction, or a subtree root) adds it to an FP64 junction accumulator of
-// its parent.
+// The tree is split once on the host into a skeleton of separator nodes
+// (containing the root) and work items hanging off it, sized by channel
+// cost for the CTA's W warps: plain subtrees, and segments (a heavy-path
+// spine between two separators plus the spine's light subtrees).  Items are
+// contiguous node ranges in Hines (depth-first, heavy-first) order and
+// independent given their separators, so all warps work on items at once and
+// warp 0 alone solves the skeleton in between (S2 / S3 in advance_body).
+// Within an item a warp makes two passes per step: root -> leaf,
+// back-substitution and V update; leaf -> root, each node's channel update,
+// its row for the next step and the row's elimination, so assembled rows
+// never leave registers.  A chain child hands its elimination term to node
+// i-1 in registers; any other child (branch junction, or an item root) adds
+// it to an FP64 junction accumulator of its parent.
 //
 // Excess form.  A row is not stored with its diagonal d_i but with its
 // excess x_i = d_i + (sum of the row's off-diagonal couplings): at assembly
@@ -38,15 +42,17 @@
 //   vbuf   [N][2]  V and its Kahan compensation
 //   slab   channel state rows, per node in mechanism order
 //   ptab   parameter rows per distinct (section, mechanism set) pair
-//   scr    [N][3]  (x, rhs, e) after assembly, e = b_i (V_p - V_i) the
-//                  parent-row axial term; (r, c, -) after elimination with
-//                  dV_i = r_i - c_i dV_parent (spines: (r, c, w), below)
+//   scr    [N][3]  eliminated rows (r, c, -) with dV_i = r_i - c_i dV_parent
+//                  (spines: (r, c, w), below); separators: their assembled
+//                  rows (x, rhs, e), e = b_i (V_p - V_i) the parent-row
+//                  axial term, for the skeleton solve
 //   jacc   [J][2]  FP64 (excess, rhs) accumulators of junction parents
 //   jx     [J]     dV of junction parents for their far children
 #pragma once
 #include "channels_mainen.cuh"
 #include "channels_ttpc.cuh"
 #include "ngpu_math.cuh"
+#include "node_classes.cuh"
 
 namespace ngpu {
 
@@ -70,8 +76,10 @@ struct NodeRec {
     int16_t rec;     // recording column or -1
     uint16_t mask;   // mechanism bits
     uint16_t prow;   // first parameter row
-    uint16_t srows;  // number of state rows
-    uint16_t prows;  // number of parameter rows
+    uint8_t srows;   // number of state rows
+    uint8_t prows;   // number of parameter rows
+    uint8_t cls;     // mechanism-set class (node_class)
+    uint8_t pad_;
 };
 
 // A work item of the split (see make_partition on the host): a plain
@@ -121,24 +129,44 @@ struct SimArgs {
     R* sepv;               // [n_seps][4] rows per group: A, B, excess, rhs terms of segment links
 };
 
-template <typename R, int MS, bool INIT>
-__device__ __forceinline__ void channels(uint32_t mk, R v, R dt, R* st, const float* pr, R& I, R& G) {
+// mk: the node's mechanism bits, a runtime value or a std::integral_constant
+// (then every mechanism test folds at compile time).
+template <typename R, int MS, bool INIT, typename MK>
+__device__ __forceinline__ void channels(MK mk, R v, R dt, R* st, const float* pr, R& I, R& G) {
     if constexpr (MS == 0) ttpc_node<R, INIT>(mk, v, dt, st, pr, I, G);
     else mainen_node<R, INIT>(mk, v, dt, st, pr, I, G);
 }
 
-// The per-step channel update as one out-of-line function: the kernel calls
-// it from three places (spine nodes, light subtrees, separators), and one
-// shared copy keeps the instruction cache warm where warps at different
-// nodes run different mechanisms.  (I, G) come back in registers.
+// Channel update of a node of mechanism-set class cls: class k < sizeof...(Ms)
+// runs the code specialised for mask Ms[k] (straight-line code in which the
+// compiler interleaves all of the node's gates); other nodes run the generic
+// code on their runtime mask.
+template <typename R, int MS, bool INIT, uint32_t M0, uint32_t... Ms>
+__device__ __forceinline__ void channels_cls(int cls, uint32_t mk, R v, R dt, R* st, const float* pr, R& I, R& G) {
+    if (cls == 0) {
+        channels<R, MS, INIT>(std::integral_constant<uint32_t, M0>{}, v, dt, st, pr, I, G);
+    } else if constexpr (sizeof...(Ms) > 0) {
+        channels_cls<R, MS, INIT, Ms...>(cls - 1, mk, v, dt, st, pr, I, G);
+    } else {
+        channels<R, MS, INIT>(mk, v, dt, st, pr, I, G);
+    }
+}
+template <typename R, int MS, bool INIT, uint32_t... Ms>
+__device__ __forceinline__ void channels_list(MaskList<Ms...>, int cls, uint32_t mk, R v, R dt, R* st,
+                                              const float* pr, R& I, R& G) {
+    channels_cls<R, MS, INIT, Ms...>(cls, mk, v, dt, st, pr, I, G);
+}
+
+// The per-step channel update.  (I, G) come back in registers.
 template <typename R>
 struct CurrentG {
     R I, G;
 };
 template <typename R, int MS>
-__device__ __noinline__ CurrentG<R> channels_step(uint32_t mk, R v, R dt, R* st, const float* pr) {
+__device__ __forceinline__ CurrentG<R> channels_step(int cls, uint32_t mk, R v, R dt, R* st, const float* pr) {
     CurrentG<R> o;
-    channels<R, MS, false>(mk, v, dt, st, pr, o.I, o.G);
+    if constexpr (MS == 0) channels_list<R, MS, false>(TTPCClasses{}, cls, mk, v, dt, st, pr, o.I, o.G);
+    else channels_list<R, MS, false>(MainenClasses{}, cls, mk, v, dt, st, pr, o.I, o.G);
     return o;
 }
 
@@ -191,41 +219,58 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// L2 prefetch of the rows the back-substitution pass reads for nodes
+// [i, i + n): (r, c, w) and (V, Kahan term), two contiguous blocks.
 template <typename R>
-__device__ __forceinline__ void prefetch_node(const Group<R>& G, const NodeRec<R>& n, int i) {
-    const int lane = threadIdx.x & 31;
-    if (lane == 0) {
-        prefetch_l2(G.scr - lane + (size_t)i * 3 * kLanes, 3 * kLanes * sizeof(R));
-        prefetch_l2(G.vbuf - lane + (size_t)i * 2 * kLanes, 2 * kLanes * sizeof(R));
-        if (n.srows) prefetch_l2(G.slab - lane + (size_t)n.srow * kLanes, n.srows * kLanes * sizeof(R));
-        if (n.prows) prefetch_l2(G.ptab - lane + (size_t)n.prow * kLanes, n.prows * kLanes * sizeof(float));
+__device__ __forceinline__ void prefetch_backsub(const Group<R>& G, int i, int n) {
+    if ((threadIdx.x & 31) == 0 && n > 0) {  // lane 0's pointers carry no lane offset
+        prefetch_l2(G.scr + (size_t)i * 3 * kLanes, (uint32_t)n * 3 * kLanes * sizeof(R));
+        prefetch_l2(G.vbuf + (size_t)i * 2 * kLanes, (uint32_t)n * 2 * kLanes * sizeof(R));
     }
 }
 
-// Elimination of node i given its (x, rhs, e); updates the chain carry or the
-// parent's FP64 junction accumulator, writes (r, c).
+// L2 prefetch of the rows node n's channel update reads: states and parameters.
+template <typename R>
+__device__ __forceinline__ void prefetch_channels(const Group<R>& G, const NodeRec<R>& n) {
+    if ((threadIdx.x & 31) == 0) {
+        if (n.srows) prefetch_l2(G.slab + (size_t)n.srow * kLanes, n.srows * kLanes * sizeof(R));
+        if (n.prows) prefetch_l2(G.ptab + (size_t)n.prow * kLanes, n.prows * kLanes * sizeof(float));
+    }
+}
+
+// A junction row: its FP64 sum with the chain carry and the accumulator of
+// its far children, which is cleared for the next step.  Out of line, so
+// that the other rows (most of them) do not issue this path predicated off.
+template <typename R>
+struct RowSum {
+    R x, r;
+};
+template <typename R>
+__device__ __forceinline__ RowSum<R> junction_sum(double* ja, R x0, R cx, R r0, R cr) {
+    RowSum<R> o;
+    o.x = (R)((double)x0 + (double)cx + ja[0]);
+    o.r = (R)((double)r0 + (double)cr + ja[kLanes]);
+    ja[0] = 0.0;
+    ja[kLanes] = 0.0;
+    return o;
+}
+
+// Elimination of a non-root node i given its (x, rhs, e); updates the chain
+// carry or the parent's FP64 junction accumulator, writes (r, c).
 template <typename R>
 __device__ __forceinline__ void eliminate_node(const Group<R>& G, const NodeRec<R>& s, int i, R x0, R r0,
                                                R e0, R& carry_x, R& carry_r) {
     using M = Math<R>;
     R x, r;
     if (s.jslot >= 0) {
-        double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
-        x = (R)((double)x0 + (double)carry_x + ja[0]);
-        r = (R)((double)r0 + (double)carry_r + ja[kLanes]);
-        ja[0] = 0.0;
-        ja[kLanes] = 0.0;
+        const RowSum<R> j = junction_sum(G.jacc + (size_t)(2 * s.jslot) * kLanes, x0, carry_x, r0, carry_r);
+        x = j.x;
+        r = j.r;
     } else {
         x = x0 + carry_x;
         r = r0 + carry_r;
     }
     R* out = G.scr + (size_t)i * 3 * kLanes;
-    if (i == 0) {  // root: no coupling left, d_0 = x_0
-        out[0] = M::dv(r, x);
-        out[kLanes] = 0;
-        carry_x = carry_r = 0;
-        return;
-    }
     const R inv = M::rc(x - s.a);
     const R rr = r * inv, cc = s.a * inv;
     out[0] = rr;
@@ -243,86 +288,68 @@ __device__ __forceinline__ void eliminate_node(const Group<R>& G, const NodeRec<
     }
 }
 
-// Leaf -> root elimination over the nodes idx(hi-1) .. idx(lo) of a list
-// (a node range or the top-tree list), with rows read two nodes ahead.
-template <typename R, typename Idx>
-__device__ __forceinline__ void eliminate_list(const Group<R>& G, const NodeRec<R>* nr, int lo, int hi, Idx idx) {
-    if (hi <= lo) return;
+// Leaf -> root elimination of the node range [lo, hi).  row(i, x, rhs, e)
+// supplies node i's assembled row: read back from scr (first step after
+// init), or assembled on the spot from the node's channel update.
+template <typename R, typename Row>
+__device__ __forceinline__ void eliminate_range(const Group<R>& G, const NodeRec<R>* nr, int lo, int hi, Row&& row) {
     R carry_x = 0, carry_r = 0;
-    auto load = [&](int k, R& x, R& r, R& e) {
-        if (k >= lo) {
-            const R* row = G.scr + (size_t)idx(k) * 3 * kLanes;
-            x = row[0];
-            r = row[kLanes];
-            e = row[2 * kLanes];
-        }
-    };
-    R x0 = 0, r0 = 0, e0 = 0, x1 = 0, r1 = 0, e1 = 0;
-    load(hi - 1, x0, r0, e0);
-    load(hi - 2, x1, r1, e1);
-    for (int k = hi - 1; k >= lo; --k) {
-        R x2 = 0, r2 = 0, e2 = 0;
-        load(k - 2, x2, r2, e2);
-        const int i = idx(k);
+    for (int i = hi - 1; i >= lo; --i) {
+        R x0, r0, e0;
+        row(i, x0, r0, e0);
         eliminate_node(G, nr[i], i, x0, r0, e0, carry_x, carry_r);
-        x0 = x1; r0 = r1; e0 = e1;
-        x1 = x2; r1 = r2; e1 = e2;
     }
 }
 
-// One node of the fused root -> leaf pass: back-substitution and V update
-// (BACKSUB), channel update at the new V, next-step assembly.  Every store
-// is issued after the channel code so that its loads (one round trip for all
-// of the node's rows) are not held back behind them.
-template <typename R, int MS, bool INIT, bool BACKSUB>
-__device__ __forceinline__ void update_node(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n,
-                                            int i, R dt, R dtn_inv, R istim_amp, bool rec_now,
-                                            float* trace, R& x_prev, R& v_prev, const R* x_given) {
-    R* vo = G.vbuf + (size_t)i * 2 * kLanes;
-    R* o = G.scr + (size_t)i * 3 * kLanes;
-    R V, vc = 0, x = 0;
-    if (INIT) {
-        V = (R)A.v_init;
-    } else if (BACKSUB) {
-        V = vo[0];
-        vc = vo[kLanes];
-        if (x_given) {
-            x = *x_given;
-        } else {
-            const R r = o[0], c = o[kLanes];
-            const R xp = (i == 0) ? (R)0 : (n.pslot < 0 ? x_prev : G.jx[(size_t)n.pslot * kLanes]);
-            x = r - c * xp;
-        }
-        x_prev = x;
-        kahan_add(V, vc, x);
-    } else {
-        V = vo[0];
-    }
-    // parent's new V: the previous node's for a chain child of this pass
-    const R vp = INIT || i == 0 ? V
-                 : (BACKSUB && n.pslot < 0) ? v_prev : G.vbuf[(size_t)n.parent * 2 * kLanes];
-    v_prev = V;
+// Channel update of node i at its new voltage V (INIT: steady state at V),
+// then the node's row for the next step: its excess x (the grounded
+// conductance g + cm/dt), right-hand side, and e = b_i (V_p - V_i), the
+// axial term of the parent's row.
+template <typename R, int MS, bool INIT>
+__device__ __forceinline__ void assemble_node(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n, int i,
+                                              R V, R vp, R dt, R dtn_inv, R istim_amp, R& x, R& rhs, R& e) {
     R I, Gm;
     if constexpr (INIT) {
-        channels<R, MS, true>(n.mask, V, dt, G.slab + (size_t)n.srow * kLanes, G.ptab + (size_t)n.prow * kLanes,
+        channels<R, MS, true>((uint32_t)n.mask, V, dt, G.slab + (size_t)n.srow * kLanes, G.ptab + (size_t)n.prow * kLanes,
                               I, Gm);
     } else {
-        const CurrentG<R> ig = channels_step<R, MS>(n.mask, V, dt, G.slab + (size_t)n.srow * kLanes,
+        const CurrentG<R> ig = channels_step<R, MS>(n.cls, n.mask, V, dt, G.slab + (size_t)n.srow * kLanes,
                                                    G.ptab + (size_t)n.prow * kLanes);
         I = ig.I;
         Gm = ig.G;
     }
-    if (INIT || BACKSUB) {
-        vo[0] = V;
-        vo[kLanes] = vc;
-    }
-    if (BACKSUB && n.jslot >= 0) G.jx[(size_t)n.jslot * kLanes] = x;
     const R istim = (i == A.stim_node) ? istim_amp : (R)0;
     const R dvp = vp - V;
-    o[0] = Gm + n.cm * dtn_inv;  // the row's excess: its grounded conductance
-    o[kLanes] = istim - I - n.a * dvp;
-    o[2 * kLanes] = n.b * dvp;
+    x = Gm + n.cm * dtn_inv;
+    rhs = istim - I - n.a * dvp;
+    e = n.b * dvp;
+}
+
+template <typename R>
+__device__ __forceinline__ void store_row(const Group<R>& G, int i, R x, R rhs, R e) {
+    R* o = G.scr + (size_t)i * 3 * kLanes;
+    o[0] = x;
+    o[kLanes] = rhs;
+    o[2 * kLanes] = e;
+}
+
+template <typename R>
+__device__ __forceinline__ void record(const SimArgs<R>& A, const NodeRec<R>& n, R V, bool rec_now, float* trace) {
     if (rec_now && n.rec >= 0) trace[(size_t)n.rec * A.n_inst_pad] = (float)V;
+}
+
+// Back-substitution result x = dV_i of node i: V update (Kahan), dV for the
+// node's far children, recording.
+template <typename R>
+__device__ __forceinline__ void backsub_node(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n, int i,
+                                             R x, bool rec_now, float* trace) {
+    R* vo = G.vbuf + (size_t)i * 2 * kLanes;
+    R V = vo[0], vc = vo[kLanes];
+    kahan_add(V, vc, x);
+    vo[0] = V;
+    vo[kLanes] = vc;
+    if (n.jslot >= 0) G.jx[(size_t)n.jslot * kLanes] = x;
+    record(A, n, V, rec_now, trace);
 }
 
 template <typename R>
@@ -346,93 +373,87 @@ __device__ __forceinline__ const NodeRec<R>* stage_nodes(const SimArgs<R>& A, ch
     return nr;
 }
 
-// Initial state of group g: channels at steady state for v_init, the first
-// step's rows, sample 0.  Nodes are independent here, so any number of warps
-// shares them.
-template <typename R, int MS>
-__device__ __forceinline__ void init_body(const SimArgs<R>& A, int g) {
-    const Group<R> G = group_of(A, g);
-    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (w == 0)
-        for (int j = 0; j < 2 * A.n_jslots; ++j) G.jacc[(size_t)j * kLanes] = 0.0;
-    R dt, dtn_inv, istim_amp;
-    bool rec_now;
-    float* trace;
-    step_inputs(A, G, 0, true, dt, dtn_inv, istim_amp, rec_now, trace);
-    R xd = 0, vd = 0;
-    for (int i = w; i < A.n_nodes; i += nw)
-        update_node<R, MS, true, false>(A, G, A.nodes[i], i, dt, dtn_inv, istim_amp, rec_now, trace, xd, vd,
-                                        nullptr);
-    if (w == 0) A.bad[G.inst] = 0;
-}
-
-template <typename R, int MS>
-__global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
-    init_body<R, MS>(A, blockIdx.x);
-}
-
-// Segment item, S1: leaf -> root elimination of the spine r..l-1 after its
-// light subtrees.  Each spine row also couples to the lower separator's dV
+// Segment item, leaf -> root elimination of the spine r..l-1 (after its
+// light subtrees).  Each spine row also couples to the lower separator's dV
 // (w: b_l of row l-1, then the fill-in carried up the spine), so its diagonal
 // is x - a + w and the row solves as dV_i = r_i - c_i dV_parent + w_i dV_l
-// (stored as (r, c, w) for S3).  The same sweep accumulates what separator
-// l needs for the skeleton, dV_{l-1} = gamma + alpha dV_u + beta dV_l
-// expanded down the spine: alpha (row l's coupling to u), gamma (its
-// right-hand side) and delta = 1 - alpha - beta, the fraction of dV_{l-1}
-// that leaks to ground along the spine, which becomes l's excess.  delta is
-// summed from the rows' leak fractions x_i / d_i, never as 1 - alpha - beta.
+// (stored as (r, c, w) for the back-substitution).  The same sweep
+// accumulates what separator l needs for the skeleton, dV_{l-1} = gamma +
+// alpha dV_u + beta dV_l expanded down the spine: alpha (row l's coupling to
+// u), gamma (its right-hand side) and delta = 1 - alpha - beta, the fraction
+// of dV_{l-1} that leaks to ground along the spine, which becomes l's
+// excess.  delta is summed from the rows' leak fractions x_i / d_i, never as
+// 1 - alpha - beta.
 template <typename R>
-__device__ __forceinline__ void eliminate_segment(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
-                                                  const DevComp& c) {
-    using M = Math<R>;
-    const int r = c.r, l = c.l, b = l - 1;
-    const NodeRec<R> nl = nr[l];
-    const R e_l = G.scr[(size_t)l * 3 * kLanes + 2 * kLanes];
-    R carry_x = 0, carry_r = 0, carry_w = 0;
-    R P = 1, gam = 0, del = 0;  // P: product of -c over the rows below
-    R* sv = G.sepv + (size_t)c.lk * 4 * kLanes;
-    for (int i = b; i >= r; --i) {
-        const NodeRec<R> s = nr[i];
-        R* row = G.scr + (size_t)i * 3 * kLanes;
-        R x, rh;
-        const R e_i = row[2 * kLanes];
-        if (s.jslot >= 0) {
-            double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
-            x = (R)((double)row[0] + (double)carry_x + ja[0]);
-            rh = (R)((double)row[kLanes] + (double)carry_r + ja[kLanes]);
-            ja[0] = 0.0;
-            ja[kLanes] = 0.0;
-        } else {
-            x = row[0] + carry_x;
-            rh = row[kLanes] + carry_r;
-        }
-        R w = carry_w;
-        if (i == b) {
-            w = -nl.b;
-            rh += e_l;
-        }
-        const R inv = M::rc(x - s.a + w);
-        const R rr = rh * inv, cc = s.a * inv, om = w * inv, lam = x * inv;
-        row[0] = rr;
-        row[kLanes] = cc;
-        row[2 * kLanes] = om;
-        gam += rr * P;
-        del += lam * P;
-        P *= -cc;
-        if (i > r) {
-            carry_x = -s.b * lam;
-            carry_r = e_i - s.b * rr;
-            carry_w = -s.b * om;
-        } else {
-            double* ja = G.jacc + (size_t)(2 * s.pslot) * kLanes;  // the upper separator
-            atomicAdd(ja, (double)(-s.b * lam));
-            atomicAdd(ja + kLanes, (double)(e_i - s.b * rr));
-            sv[kLanes] = s.b * om;  // B: row u's coupling to dV_l
-        }
+struct SpineCarry {
+    R x, r, w;    // chain carries (excess, right-hand side, coupling to dV_l)
+    R P, gam, del;  // P: product of -c over the rows below
+    __device__ __forceinline__ void reset() {
+        x = r = w = 0;
+        P = 1;
+        gam = del = 0;
     }
-    sv[0] = nl.a * P;              // A: row l's coupling to dV_u (alpha = P)
-    sv[2 * kLanes] = -nl.a * del;  // added to l's excess
-    sv[3 * kLanes] = -nl.a * gam;  // added to rhs_l
+};
+
+// One spine row i (rows are visited from b = l-1 down to r) with its row
+// (x0, r0, e_i); e_l: the lower separator's parent-row axial term; sv: the
+// segment link's rows (A, B, excess, rhs terms).
+template <typename R>
+__device__ __forceinline__ void eliminate_spine_row(const Group<R>& G, const NodeRec<R>& s, const NodeRec<R>& nl,
+                                                    int i, int b, int r, R x0, R r0, R e_i, R e_l,
+                                                    SpineCarry<R>& k, R* sv) {
+    using M = Math<R>;
+    R x, rh;
+    if (s.jslot >= 0) {
+        const RowSum<R> j = junction_sum(G.jacc + (size_t)(2 * s.jslot) * kLanes, x0, k.x, r0, k.r);
+        x = j.x;
+        rh = j.r;
+    } else {
+        x = x0 + k.x;
+        rh = r0 + k.r;
+    }
+    R w = k.w;
+    if (i == b) {
+        w = -nl.b;
+        rh += e_l;
+    }
+    const R inv = M::rc(x - s.a + w);
+    const R rr = rh * inv, cc = s.a * inv, om = w * inv, lam = x * inv;
+    R* out = G.scr + (size_t)i * 3 * kLanes;
+    out[0] = rr;
+    out[kLanes] = cc;
+    out[2 * kLanes] = om;
+    k.gam += rr * k.P;
+    k.del += lam * k.P;
+    k.P *= -cc;
+    if (i > r) {
+        k.x = -s.b * lam;
+        k.r = e_i - s.b * rr;
+        k.w = -s.b * om;
+    } else {
+        double* ja = G.jacc + (size_t)(2 * s.pslot) * kLanes;  // the upper separator
+        atomicAdd(ja, (double)(-s.b * lam));
+        atomicAdd(ja + kLanes, (double)(e_i - s.b * rr));
+        sv[kLanes] = s.b * om;  // B: row u's coupling to dV_l
+        sv[0] = nl.a * k.P;              // A: row l's coupling to dV_u (alpha = P)
+        sv[2 * kLanes] = -nl.a * k.del;  // added to l's excess
+        sv[3 * kLanes] = -nl.a * k.gam;  // added to rhs_l
+    }
+}
+
+// The spine of segment c, from rows supplied by row(i, x, rhs, e).
+template <typename R, typename Row>
+__device__ __forceinline__ void eliminate_segment(const Group<R>& G, const NodeRec<R>* nr, const DevComp& c, R e_l,
+                                                  Row&& row) {
+    const NodeRec<R> nl = nr[c.l];
+    SpineCarry<R> k;
+    k.reset();
+    R* sv = G.sepv + (size_t)c.lk * 4 * kLanes;
+    for (int i = c.l - 1; i >= c.r; --i) {
+        R x0, r0, e_i;
+        row(i, x0, r0, e_i);
+        eliminate_spine_row(G, nr[i], nl, i, c.l - 1, c.r, x0, r0, e_i, e_l, k, sv);
+    }
 }
 
 // Warp-level work queue: lane 0 takes the next item, the warp shares it.
@@ -442,19 +463,156 @@ __device__ __forceinline__ int next_item(int* ctr) {
     return __shfl_sync(0xffffffffu, k, 0);
 }
 
-// Per timestep (three barriers):
-//   S1  all warps take items from a queue, largest first: leaf -> root
-//       elimination of plain subtrees and of segments (above); each item's
-//       contribution to its upper separator goes to that separator's FP64
-//       accumulator
+// Initial state of group g: channels at steady state for v_init, the first
+// step's rows (nodes are independent here, so any number of warps shares
+// them), sample 0; then every item's elimination for the first step, from
+// the rows just stored, so that a launch of k_sim_advance starts on
+// eliminated rows.  ctr: a shared-memory work counter.
+template <typename R, int MS>
+__device__ __forceinline__ void init_body(const SimArgs<R>& A, int g, int* ctr) {
+    const Group<R> G = group_of(A, g);
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) *ctr = 0;
+    if (w == 0)
+        for (int j = 0; j < 2 * A.n_jslots; ++j) G.jacc[(size_t)j * kLanes] = 0.0;
+    R dt, dtn_inv, istim_amp;
+    bool rec_now;
+    float* trace;
+    step_inputs(A, G, 0, true, dt, dtn_inv, istim_amp, rec_now, trace);
+    const R V = (R)A.v_init;
+    for (int i = w; i < A.n_nodes; i += nw) {
+        const NodeRec<R> n = A.nodes[i];
+        R x, rhs, e;
+        assemble_node<R, MS, true>(A, G, n, i, V, V, dt, dtn_inv, istim_amp, x, rhs, e);
+        R* vo = G.vbuf + (size_t)i * 2 * kLanes;
+        vo[0] = V;
+        vo[kLanes] = 0;
+        store_row(G, i, x, rhs, e);
+        record(A, n, V, rec_now, trace);
+    }
+    if (w == 0) A.bad[G.inst] = 0;
+    __syncthreads();
+    auto row = [&](int i, R& x, R& rhs, R& e) {
+        const R* o = G.scr + (size_t)i * 3 * kLanes;
+        x = o[0];
+        rhs = o[kLanes];
+        e = o[2 * kLanes];
+    };
+    for (int k = next_item(ctr); k < A.n_comps; k = next_item(ctr)) {
+        const DevComp c = A.comps[k];
+        eliminate_range(G, A.nodes, c.lo, c.hi, row);
+        if (c.l >= 0) eliminate_segment(G, A.nodes, c, G.scr[(size_t)c.l * 3 * kLanes + 2 * kLanes], row);
+    }
+}
+
+template <typename R, int MS>
+__global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
+    __shared__ int ctr;
+    init_body<R, MS>(A, blockIdx.x, &ctr);
+}
+
+// Back-substitution pass of an item, root -> leaf: the spine of a segment
+// (dV_i = r_i - c_i dV_parent + w_i dV_l, from separator u down), then the
+// light nodes; V update of each node.  Rows are prefetched into L2 in
+// blocks of four nodes, four nodes ahead.
+template <typename R>
+__device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
+                                             const DevComp& c, bool rec_now, float* trace) {
+    constexpr int kBlk = 4;
+    if (c.l >= 0) {
+        R xp = G.jx[(size_t)nr[c.u].jslot * kLanes];
+        const R xl = G.jx[(size_t)nr[c.l].jslot * kLanes];
+        prefetch_backsub(G, c.r, min(kBlk, c.l - c.r));
+        for (int i = c.r; i < c.l; ++i) {
+            if (((i - c.r) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.l - i - kBlk));
+            const R* row = G.scr + (size_t)i * 3 * kLanes;
+            const R xi = row[0] - row[kLanes] * xp + row[2 * kLanes] * xl;
+            xp = xi;
+            backsub_node(A, G, nr[i], i, xi, rec_now, trace);
+        }
+    }
+    R x_prev = 0;
+    prefetch_backsub(G, c.lo, min(kBlk, c.hi - c.lo));
+    for (int i = c.lo; i < c.hi; ++i) {
+        if (((i - c.lo) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.hi - i - kBlk));
+        const NodeRec<R> n = nr[i];
+        const R* row = G.scr + (size_t)i * 3 * kLanes;
+        const R xp = n.pslot < 0 ? x_prev : G.jx[(size_t)n.pslot * kLanes];
+        const R x = row[0] - row[kLanes] * xp;
+        x_prev = x;
+        backsub_node(A, G, n, i, x, rec_now, trace);
+    }
+}
+
+// Channel pass of an item, leaf -> root: each node's channel update at its
+// new V and its next-step row, which is eliminated at once (children come
+// first in this order), so assembled rows stay in registers.  One loop
+// visits, in this order, the light nodes hi-1 .. lo, the separator sep (a
+// segment's lower separator, or a separator linked directly to the
+// skeleton: its row goes to the skeleton), and, for a segment (lk >= 0),
+// the spine sep-1 .. r.  Every channel update of a step goes through this
+// one loop, so the channel code is inlined once.
+template <typename R, int MS>
+__device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
+                                              int lo, int hi, int sep, int r, int lk, R dt, R dtn_inv,
+                                              R istim_amp) {
+    const int n_light = hi - lo;
+    const int n_sep = n_light + (sep >= 0 ? 1 : 0);
+    const int n = n_sep + (lk >= 0 ? sep - r : 0);
+    const int b = sep - 1;
+    auto node_at = [&](int p) { return p < n_light ? hi - 1 - p : (p < n_sep ? sep : b - (p - n_sep)); };
+    NodeRec<R> nl;
+    R* sv = nullptr;
+    if (lk >= 0) {
+        nl = nr[sep];
+        sv = G.sepv + (size_t)lk * 4 * kLanes;
+    }
+    SpineCarry<R> k;
+    k.reset();
+    R e_l = 0;
+    int vi = -1;  // node whose V was read last as a parent voltage
+    R vv = 0;
+    if (n > 0) prefetch_channels(G, nr[node_at(0)]);
+    if (n > 1) prefetch_channels(G, nr[node_at(1)]);
+    for (int p = 0; p < n; ++p) {
+        const int i = node_at(p);
+        const NodeRec<R> nd = nr[i];
+        if (p + 2 < n) prefetch_channels(G, nr[node_at(p + 2)]);
+        R V;
+        if (vi == i) V = vv;
+        else V = G.vbuf[(size_t)i * 2 * kLanes];
+        const R vp = i == 0 ? V : G.vbuf[(size_t)nd.parent * 2 * kLanes];
+        vi = nd.parent;
+        vv = vp;
+        R x, rhs, e;
+        assemble_node<R, MS, false>(A, G, nd, i, V, vp, dt, dtn_inv, istim_amp, x, rhs, e);
+        if (p < n_light) {
+            eliminate_node(G, nd, i, x, rhs, e, k.x, k.r);
+        } else if (p < n_sep) {
+            store_row(G, i, x, rhs, e);
+            e_l = e;
+            k.reset();
+        } else {
+            eliminate_spine_row(G, nd, nl, i, b, r, x, rhs, e, e_l, k, sv);
+        }
+    }
+}
+
+// Per timestep (two barriers):
 //   S2  warp 0 solves the skeleton (the separators, a few dozen nodes) with
-//       the reduced couplings of the segments, and updates their V
-//   S3  all warps take items again: back-substitution + V update + channel
-//       update + next-step assembly of every node of the item (a segment
-//       also does its lower separator's channels, which need the spine's new
-//       V); separators linked directly to the skeleton are items too
-// n_steps timesteps of group g; the items are shared by however many warps
-// the CTA has (the split was sized for A.n_warps).
+//       the reduced couplings of the segments, and updates (and records)
+//       their V
+//   S3  all warps take items from a queue, largest first: an item's
+//       back-substitution pass, then its channel pass (channel update,
+//       next-step assembly and elimination node by node, above); each
+//       item's contribution to its upper separator goes to that
+//       separator's FP64 accumulator.  Separators linked directly to the
+//       skeleton are items too (channel update and row for S2).
+// Between launches the rows are eliminated (k_sim_init eliminates the first
+// step's rows), so a run split into several launches performs the same
+// operations as one launch.  n_steps timesteps of group g; the items are
+// shared by however many warps the CTA has (the split was sized for
+// A.n_warps).
 template <typename R, int MS>
 __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0, int n_steps, char* smem,
                                              int* ctr) {
@@ -464,16 +622,16 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
     if (threadIdx.x == 0) { ctr[0] = 0; ctr[1] = 0; }
     __syncthreads();
     int bad = 0;
-    const int n_items3 = A.n_comps + A.n_seps;
+    const int n_items = A.n_comps + A.n_seps;
     for (int t = t0; t < t0 + n_steps; ++t) {
-        // S1
-        if (threadIdx.x == 0) ctr[1] = 0;
-        for (int k = next_item(&ctr[0]); k < A.n_comps; k = next_item(&ctr[0])) {
-            const DevComp c = A.comps[k];
-            eliminate_list(G, nr, c.lo, c.hi, [](int q) { return q; });
-            if (c.l >= 0) eliminate_segment(A, G, nr, c);
-        }
-        __syncthreads();
+        // this step's queue is ctr[t & 1]; the other counter was last used
+        // by the previous step's queue, which the barrier ended
+        int* const q = &ctr[t & 1];
+        if (threadIdx.x == 0) ctr[(t + 1) & 1] = 0;
+        R dt, dtn_inv, istim_amp;
+        bool rec_now;
+        float* trace;
+        step_inputs(A, G, t, false, dt, dtn_inv, istim_amp, rec_now, trace);
         // S2: skeleton
         if (w == 0) {
             using M = Math<R>;
@@ -520,52 +678,27 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
                 kahan_add(V, vc, x);
                 vo[0] = V;
                 vo[kLanes] = vc;
+                record(A, s, V, rec_now, trace);
                 if (k == 0 && !(fabs(V) < (R)1e6)) bad = 1;  // NaN / Inf / blow-up
             }
         }
         __syncthreads();
-        // S3
-        if (threadIdx.x == 0) ctr[0] = 0;
-        R dt, dtn_inv, istim_amp;
-        bool rec_now;
-        float* trace;
-        step_inputs(A, G, t, false, dt, dtn_inv, istim_amp, rec_now, trace);
-        for (int k = next_item(&ctr[1]); k < n_items3; k = next_item(&ctr[1])) {
+        // S3: items
+        for (int k = next_item(q); k < n_items; k = next_item(q)) {
+            int lo = 0, hi = 0, sep = -1, r = 0, lk = -1;
             if (k < A.n_comps) {
                 const DevComp c = A.comps[k];
-                R x_prev = 0, v_prev = 0;
-                if (c.l >= 0) {  // spine: dV_i = r_i - c_i dV_parent + w_i dV_l, from separator u down
-                    R xp = G.jx[(size_t)nr[c.u].jslot * kLanes];
-                    const R xl = G.jx[(size_t)nr[c.l].jslot * kLanes];
-                    v_prev = G.vbuf[(size_t)c.u * 2 * kLanes];
-                    for (int i = c.r; i < c.l; ++i) {
-                        if (i + 2 < c.l) prefetch_node(G, nr[i + 2], i + 2);
-                        const R* row = G.scr + (size_t)i * 3 * kLanes;
-                        const R xi = row[0] - row[kLanes] * xp + row[2 * kLanes] * xl;
-                        xp = xi;
-                        update_node<R, MS, false, true>(A, G, nr[i], i, dt, dtn_inv, istim_amp, rec_now, trace,
-                                                        x_prev, v_prev, &xi);
-                    }
-                }
-                x_prev = 0;
-                for (int i = c.lo; i < c.hi; ++i) {
-                    if (i + 2 < c.hi) prefetch_node(G, nr[i + 2], i + 2);
-                    update_node<R, MS, false, true>(A, G, nr[i], i, dt, dtn_inv, istim_amp, rec_now, trace, x_prev,
-                                                    v_prev, nullptr);
-                }
-                if (c.l >= 0) {
-                    R xd = 0, vd = 0;
-                    update_node<R, MS, false, false>(A, G, nr[c.l], c.l, dt, dtn_inv, istim_amp, rec_now, trace,
-                                                     xd, vd, nullptr);
-                }
+                backsub_item(A, G, nr, c, rec_now, trace);
+                lo = c.lo;
+                hi = c.hi;
+                sep = c.l;
+                r = c.r;
+                lk = c.lk;
             } else {
                 const DevSep sp = A.seps[k - A.n_comps];
-                if (sp.seg < 0) {
-                    R xd = 0, vd = 0;
-                    update_node<R, MS, false, false>(A, G, nr[sp.node], sp.node, dt, dtn_inv, istim_amp, rec_now,
-                                                     trace, xd, vd, nullptr);
-                }
+                if (sp.seg < 0) sep = sp.node;  // separators ending a segment are their segment's
             }
+            channels_item<R, MS>(A, G, nr, lo, hi, sep, r, lk, dt, dtn_inv, istim_amp);
         }
         __syncthreads();
     }
@@ -599,8 +732,9 @@ __device__ __forceinline__ int batch_member(const int* cta0, int n) {
 
 template <typename R, int MS>
 __global__ void __launch_bounds__(kLanes * kMaxWarps) k_batch_init(const __grid_constant__ BatchArgs<R> B) {
+    __shared__ int ctr;
     const int k = batch_member(B.cta0, B.n);
-    init_body<R, MS>(B.sim[k], blockIdx.x - B.cta0[k]);
+    init_body<R, MS>(B.sim[k], blockIdx.x - B.cta0[k], &ctr);
 }
 
 template <typename R, int MS>
