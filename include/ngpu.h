@@ -179,6 +179,26 @@ int ngpu_sim_check(ngpu_sim *s, int32_t *n_bad, void *cuda_stream);
 int ngpu_sim_trace_device(ngpu_sim *s, const float **trace, int32_t *n_inst_padded);
 
 /*
+ * Runtime specialisation of the advance kernel.  At initialisation an FP32
+ * simulation (or, at creation, an FP32 batch) gets a kernel compiled with
+ * NVRTC for its model's mechanism masks (up to 16): nodes with those masks
+ * run channel code in which the mask is a compile-time constant.  The
+ * reference regenerates and recompiles its simulator per model ahead of time
+ * (AllModels.cu / AllModels.cuh); no API counterpart.  Without NVRTC, after a
+ * failed compile, or with NGPU_JIT=0 in the environment, the ahead-of-time
+ * kernel runs (same results up to FP32 rounding order within a node).
+ *   ngpu_sim_classes  masks compiled for the kernel that runs s (0: the
+ *                     ahead-of-time kernel); valid after ngpu_sim_init
+ *   ngpu_jit_build    compile only (no device needed) for compute
+ *                     capability cc_major.cc_minor: the cubin's size
+ *   ngpu_jit_log      the last compile failure or reason for falling back
+ */
+int ngpu_sim_classes(const ngpu_sim *s, int32_t *n_classes);
+int ngpu_jit_build(int32_t mechset, const uint32_t *masks, int32_t n_masks, int32_t cc_major,
+                   int32_t cc_minor, int64_t *cubin_bytes);
+const char *ngpu_jit_log(void);
+
+/*
  * Allocation-free variant of ngpu_run.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory -- a host program that

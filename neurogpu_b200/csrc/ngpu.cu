@@ -22,6 +22,7 @@
 
 #include "../../include/ngpu.h"
 #include "gemm_tc.cuh"
+#include "ngpu_jit.h"
 #include "sim_kernels.cuh"
 
 using namespace ngpu;
@@ -351,6 +352,7 @@ static Partition make_partition(const ngpu_model* m, int W) {
     return P;
 }
 
+struct ngpu_batch;
 struct ngpu_sim {
     ngpu_model* m = nullptr;
     int n_sets = 0, n_stim = 0, n_inst = 0, n_groups = 0, n_pad = 0, precision = 0;
@@ -386,6 +388,10 @@ struct ngpu_sim {
     int n_rec_unique = 0, rec_every = 1, n_samples = 0;
     float v_init = -65.f;
     bool has_params = false, has_stim = false, initialized = false;
+    // runtime-specialised kernels the node records' classes refer to
+    // (nullptr: the ahead-of-time kernels, every node generic)
+    const ngpu_jit::Module* jit = nullptr;
+    ngpu_batch* batch = nullptr;  // the batch whose kernels this simulation's records follow
 };
 
 template <typename R>
@@ -441,6 +447,15 @@ static cudaError_t launch_advance(ngpu_sim* s, int t0, int n, cudaStream_t st) {
     const int threads = kLanes * s->n_warps;
     const size_t smem = SmemPlan<R>::bytes(s->m->n);
     cudaError_t e;
+    if (std::is_same<R, float>::value && s->jit) {
+        const void* k = (const void*)s->jit->advance;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        void* args[] = {(void*)&A, (void*)&t0, (void*)&n};
+        e = cudaLaunchKernel(k, dim3(s->n_groups), dim3(threads), args, smem, st);
+        g_launches++;
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     if (s->m->mechset == NGPU_MECHSET_TTPC) {
         e = cudaFuncSetAttribute(k_sim_advance<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -953,49 +968,27 @@ int ngpu_sim_set_recording(ngpu_sim* s, int32_t n_rec, const int32_t* rec_nodes,
     return NGPU_OK;
 }
 
-// Host side of an initialisation: node records with this run's split and
-// recording columns, the trace buffer (kept when its size is unchanged, so
-// the device addresses a captured graph holds stay valid), the error flags.
+// The mechanism masks a simulation's (or batch's) kernel is compiled for.
+static std::vector<uint32_t> model_masks(const ngpu_model* m) {
+    std::vector<uint32_t> v(m->mask.begin(), m->mask.end());
+    return v;
+}
+
+// Node records with this run's split, recording columns and mechanism
+// classes, uploaded to the device.  In FP32 the classes follow the
+// runtime-specialised kernels of the simulation's batch, or its own.
+static int sim_upload_nodes(ngpu_sim* s);
+
+// Host side of an initialisation: node records, the trace buffer (kept when
+// its size is unchanged, so the device addresses a captured graph holds stay
+// valid), the error flags.
 static int sim_prepare_init(ngpu_sim* s, float v_init, cudaStream_t st) {
     if (!s) return fail(NGPU_E_INVALID, "null sim");
     if (!s->has_params) return fail(NGPU_E_STATE, "set_params must precede init");
     if (!s->has_stim) return fail(NGPU_E_STATE, "set_stimulus must precede init");
     if (!std::isfinite(v_init)) return fail(NGPU_E_INVALID, "v_init must be finite");
-    const ngpu_model* m = s->m;
-    // node records with this run's split and recording columns
-    std::vector<int> uniq(s->n_rec_unique, -1);
-    for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
-    std::vector<int> rec(m->n, -1);
-    for (int c = 0; c < s->n_rec_unique; ++c) rec[uniq[c]] = c;
-    auto fill = [&](auto* recs) {
-        for (int i = 0; i < m->n; ++i) {
-            auto& q = recs[i];
-            using RT = std::remove_reference_t<decltype(q.a)>;
-            q.a = (RT)m->a[i];
-            q.b = (RT)m->b[i];
-            q.cm = (RT)(m->cm[i] / 1000.0);
-            q.srow = m->info[i].srow;
-            q.parent = (int16_t)m->parent[i];
-            q.jslot = (int16_t)s->part.jslot[i];
-            q.pslot = (int16_t)s->part.pslot[i];
-            q.rec = (int16_t)rec[i];
-            q.mask = (uint16_t)m->mask[i];
-            q.prow = (uint16_t)m->info[i].prow;
-            q.srows = (uint8_t)m->rows[i].x;
-            q.prows = (uint8_t)m->rows[i].y;
-            q.cls = (uint8_t)node_class(m->mechset, (uint32_t)m->mask[i]);
-            q.pad_ = 0;
-        }
-    };
-    if (s->precision == NGPU_FP64) {
-        std::vector<NodeRec<double>> recs(m->n);
-        fill(recs.data());
-        NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
-    } else {
-        std::vector<NodeRec<float>> recs(m->n);
-        fill(recs.data());
-        NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
-    }
+    const int rc = sim_upload_nodes(s);
+    if (rc != NGPU_OK) return rc;
     s->n_samples = (s->nt + s->rec_every - 1) / s->rec_every;
     const size_t tbytes = sizeof(float) * (size_t)s->n_samples * s->n_rec_unique * s->n_pad;
     if (!s->d_trace || s->trace_bytes != tbytes) {
@@ -1046,7 +1039,52 @@ struct ngpu_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<unsigned char> graph_key;
     int graph_kernels = 0;  // kernels one replay launches
+    // runtime-specialised kernels over the members' masks (nullptr: ahead of time)
+    const ngpu_jit::Module* jit = nullptr;
 };
+
+static int sim_upload_nodes(ngpu_sim* s) {
+    const ngpu_model* m = s->m;
+    s->jit = nullptr;
+    if (s->precision == NGPU_FP32) {
+        if (s->batch) s->jit = s->batch->jit;
+        else s->jit = ngpu_jit::module(m->mechset, ngpu_jit::pick_masks(model_masks(m), kMaxClasses));
+    }
+    std::vector<int> uniq(s->n_rec_unique, -1);
+    for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
+    std::vector<int> rec(m->n, -1);
+    for (int c = 0; c < s->n_rec_unique; ++c) rec[uniq[c]] = c;
+    auto fill = [&](auto* recs) {
+        for (int i = 0; i < m->n; ++i) {
+            auto& q = recs[i];
+            using RT = std::remove_reference_t<decltype(q.a)>;
+            q.a = (RT)m->a[i];
+            q.b = (RT)m->b[i];
+            q.cm = (RT)(m->cm[i] / 1000.0);
+            q.srow = m->info[i].srow;
+            q.parent = (int16_t)m->parent[i];
+            q.jslot = (int16_t)s->part.jslot[i];
+            q.pslot = (int16_t)s->part.pslot[i];
+            q.rec = (int16_t)rec[i];
+            q.mask = (uint16_t)m->mask[i];
+            q.prow = (uint16_t)m->info[i].prow;
+            q.srows = (uint8_t)m->rows[i].x;
+            q.prows = (uint8_t)m->rows[i].y;
+            q.cls = (uint8_t)ngpu_jit::class_of(s->jit, (uint32_t)m->mask[i], kGenericClass);
+            q.pad_ = 0;
+        }
+    };
+    if (s->precision == NGPU_FP64) {
+        std::vector<NodeRec<double>> recs(m->n);
+        fill(recs.data());
+        NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<NodeRec<float>> recs(m->n);
+        fill(recs.data());
+        NGPU_CUDA(cudaMemcpy(s->d_nodes, recs.data(), sizeof(recs[0]) * m->n, cudaMemcpyHostToDevice));
+    }
+    return NGPU_OK;
+}
 
 template <typename R>
 static BatchArgs<R> make_batch_args(ngpu_batch* b) {
@@ -1067,6 +1105,15 @@ template <typename R>
 static cudaError_t launch_batch(ngpu_batch* b, bool init, int t0, int n, cudaStream_t st) {
     const BatchArgs<R> B = make_batch_args<R>(b);
     cudaError_t e;
+    if (std::is_same<R, float>::value && b->jit && !init) {
+        const void* k = (const void*)b->jit->batch_advance;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+        if (e != cudaSuccess) return e;
+        void* args[] = {(void*)&B, (void*)&t0, (void*)&n};
+        e = cudaLaunchKernel(k, dim3(b->total_ctas), dim3(b->threads), args, b->smem, st);
+        g_launches++;
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     if (b->mechset == NGPU_MECHSET_TTPC) {
         if (init) {
             k_batch_init<R, 0><<<b->total_ctas, b->threads, 0, st>>>(B);
@@ -1116,6 +1163,7 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
             return fail(NGPU_E_INVALID, "a batch needs one precision");
         if (sims[k]->m->mechset != sims[0]->m->mechset)
             return fail(NGPU_E_INVALID, "a batch needs one mechanism set");
+        if (sims[k]->batch) return fail(NGPU_E_INVALID, "a simulation belongs to one batch at a time");
     }
     ngpu_batch* b = new (std::nothrow) ngpu_batch();
     if (!b) return fail(NGPU_E_NOMEM, "host allocation failed");
@@ -1130,12 +1178,36 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
                                                              : SmemPlan<float>::bytes(s->m->n));
     }
     b->threads = kLanes * W;
+    if (b->precision == NGPU_FP32) {  // one specialised kernel over every member's masks
+        std::vector<uint32_t> all;
+        for (ngpu_sim* s : b->sims) {
+            const std::vector<uint32_t> mm = model_masks(s->m);
+            all.insert(all.end(), mm.begin(), mm.end());
+        }
+        b->jit = ngpu_jit::module(b->mechset, ngpu_jit::pick_masks(all, kMaxClasses));
+    }
+    for (ngpu_sim* s : b->sims) {
+        s->batch = b;
+        if (s->initialized) {  // its records still carry its own classes
+            const int rc = sim_upload_nodes(s);
+            if (rc != NGPU_OK) {
+                for (ngpu_sim* t : b->sims) t->batch = nullptr;
+                delete b;
+                return rc;
+            }
+        }
+    }
     *out = b;
     return NGPU_OK;
 }
 
 int ngpu_batch_destroy(ngpu_batch* b) {
-    if (b) batch_drop_graph(b);
+    if (b) {
+        batch_drop_graph(b);
+        // members keep the batch's kernels until their next initialisation
+        for (ngpu_sim* s : b->sims)
+            if (s->batch == b) s->batch = nullptr;
+    }
     delete b;
     return NGPU_OK;
 }
@@ -1205,6 +1277,9 @@ int ngpu_batch_run_graph(ngpu_batch* b, float v_init, int32_t nt, int32_t chunk,
             e = b->mechset == NGPU_MECHSET_TTPC
                     ? cudaFuncSetAttribute(k_batch_advance<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem)
                     : cudaFuncSetAttribute(k_batch_advance<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+        else if (b->jit)
+            e = cudaFuncSetAttribute((const void*)b->jit->batch_advance, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)b->smem);
         else
             e = b->mechset == NGPU_MECHSET_TTPC
                     ? cudaFuncSetAttribute(k_batch_advance<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem)
@@ -1240,6 +1315,37 @@ int ngpu_batch_run_graph(ngpu_batch* b, float v_init, int32_t nt, int32_t chunk,
 }
 
 int ngpu_sim_n_samples(const ngpu_sim* s) { return s ? s->n_samples : 0; }
+
+int ngpu_sim_classes(const ngpu_sim* s, int32_t* n_classes) {
+    if (!s || !n_classes) return fail(NGPU_E_INVALID, "null argument");
+    *n_classes = s->jit ? (int32_t)s->jit->masks.size() : 0;
+    return NGPU_OK;
+}
+
+int ngpu_jit_build(int32_t mechset, const uint32_t* masks, int32_t n_masks, int32_t cc_major, int32_t cc_minor,
+                   int64_t* cubin_bytes) {
+    if (!cubin_bytes || (n_masks > 0 && !masks)) return fail(NGPU_E_INVALID, "null argument");
+    if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN) return fail(NGPU_E_INVALID, "unknown mechset");
+    if (n_masks < 1 || n_masks > kMaxClasses)
+        return fail(NGPU_E_INVALID, "1.." + std::to_string(kMaxClasses) + " masks");
+    std::vector<char> cubin;
+    std::string err;
+    const std::vector<uint32_t> mv(masks, masks + n_masks);
+    std::lock_guard<std::mutex> lock(ngpu_jit::mu());
+    if (!ngpu_jit::build_cubin(mechset, mv, std::to_string(cc_major) + std::to_string(cc_minor) + "a", &cubin, &err)) {
+        ngpu_jit::last_log() = err;
+        return fail(NGPU_E_CUDA, "runtime compilation failed: " + err);
+    }
+    *cubin_bytes = (int64_t)cubin.size();
+    return NGPU_OK;
+}
+
+const char* ngpu_jit_log(void) {
+    static thread_local std::string copy;
+    std::lock_guard<std::mutex> lock(ngpu_jit::mu());
+    copy = ngpu_jit::last_log();
+    return copy.c_str();
+}
 
 int ngpu_sim_trace_device(ngpu_sim* s, const float** trace, int32_t* n_inst_padded) {
     if (!s || !trace) return fail(NGPU_E_INVALID, "null argument");
@@ -1454,7 +1560,7 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
         q.prow = (uint16_t)m->info[i].prow;
         q.srows = (uint8_t)m->rows[i].x;
         q.prows = (uint8_t)m->rows[i].y;
-        q.cls = (uint8_t)node_class(m->mechset, (uint32_t)m->mask[i]);
+        q.cls = (uint8_t)kGenericClass;
         q.pad_ = 0;
     }
     for (int k = 0; k < n_rec_u; ++k) recs[rec_col_of_node[k]].rec = (int16_t)k;

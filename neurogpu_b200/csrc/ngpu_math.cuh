@@ -6,8 +6,19 @@
 // FP64 build of the same kernel template is the GPU-side oracle run and uses
 // the correctly rounded double-precision library functions throughout.
 #pragma once
+#ifdef __CUDACC_RTC__  // runtime compilation (NVRTC): no host headers
+typedef unsigned char uint8_t;
+typedef signed char int8_t;
+typedef unsigned short uint16_t;
+typedef short int16_t;
+typedef unsigned int uint32_t;
+typedef int int32_t;
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+#else
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 #define NGPU_HD __host__ __device__ __forceinline__
 
@@ -51,15 +62,6 @@ template <> struct Math<double> {
     static NGPU_HD double pw(double a, double b) { return pow(a, b); }
     static NGPU_HD double one_minus_exp_neg(double z) { return -expm1(-z); }
 };
-
-// Index of the lowest set bit of m (m != 0).
-NGPU_HD int low_bit(uint32_t m) {
-#ifdef __CUDA_ARCH__
-    return __ffs((int)m) - 1;
-#else
-    return __builtin_ctz(m);
-#endif
-}
 
 // cnexp update of a first-order gate: x += (1 - exp(-dt/tau)) (xinf - x).
 template <typename R>

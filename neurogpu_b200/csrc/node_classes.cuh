@@ -1,40 +1,35 @@
-// Mechanism sets compiled as straight-line channel code.
+// Mechanism-set classes: channel code compiled for fixed masks.
 //
-// A node's channel update branches on each mechanism of its mask.  For the
-// masks listed here the kernel also carries a copy of the channel code with
-// the mask fixed at compile time; there every mechanism test folds away and
-// the compiler schedules all of the node's gates together.  A node whose
-// mask is listed is given the list index as its class (node_class); any
-// other node runs the generic code.
+// A node's channel update branches on each mechanism of its mask; over a
+// runtime mask the compiler turns the short load / store blocks of absent
+// mechanisms into predicated instructions that every node issues.  A kernel
+// instantiated with a MaskList also carries a copy of the channel code per
+// listed mask, with the mask a compile-time constant (MaskC): every
+// mechanism test folds away and the compiler schedules all of the node's
+// gates together.  A node whose mask is listed gets the list index as its
+// class; any other node runs the generic code.  The ahead-of-time kernels
+// use the empty list; the host generates, compiles (NVRTC) and caches a
+// kernel per model with the model's own masks (ngpu.cu, jit_module).
 #pragma once
-#include <stdint.h>
-#include <type_traits>
+#include "ngpu_math.cuh"
 
 namespace ngpu {
+
+// a mechanism mask known at compile time; converts to its value
+template <uint32_t M>
+struct MaskC {
+    static constexpr uint32_t value = M;
+    __host__ __device__ constexpr operator uint32_t() const { return M; }
+};
 
 template <uint32_t... Ms>
 struct MaskList {
     static constexpr int size = (int)sizeof...(Ms);
 };
 
-// TTPC: basal (Ih, pas); apical (Ih, Im, NaTs2_t, pas, SKv3_1); axon; apical
-// hot zone; soma.  Mainen: soma+dendrite, axon, soma with kv.
-using TTPCClasses = MaskList<0x408u, 0x1618u, 0x1de7u, 0x1e1fu, 0x1e6fu>;
-using MainenClasses = MaskList<0x6fu, 0x70u, 0x7fu>;
+using NoClasses = MaskList<>;
 
 constexpr int kGenericClass = 255;
-
-template <uint32_t... Ms>
-inline int class_in(MaskList<Ms...>, uint32_t mask) {
-    const uint32_t v[] = {Ms...};
-    for (int k = 0; k < (int)sizeof...(Ms); ++k)
-        if (v[k] == mask) return k;
-    return kGenericClass;
-}
-
-// mechset: 0 TTPC, 1 Mainen
-inline int node_class(int mechset, uint32_t mask) {
-    return mechset == 0 ? class_in(TTPCClasses{}, mask) : class_in(MainenClasses{}, mask);
-}
+constexpr int kMaxClasses = 16;  // masks compiled per kernel; further masks stay generic
 
 }  // namespace ngpu

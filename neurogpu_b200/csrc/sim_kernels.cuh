@@ -144,7 +144,7 @@ __device__ __forceinline__ void channels(MK mk, R v, R dt, R* st, const float* p
 template <typename R, int MS, bool INIT, uint32_t M0, uint32_t... Ms>
 __device__ __forceinline__ void channels_cls(int cls, uint32_t mk, R v, R dt, R* st, const float* pr, R& I, R& G) {
     if (cls == 0) {
-        channels<R, MS, INIT>(std::integral_constant<uint32_t, M0>{}, v, dt, st, pr, I, G);
+        channels<R, MS, INIT>(MaskC<M0>{}, v, dt, st, pr, I, G);
     } else if constexpr (sizeof...(Ms) > 0) {
         channels_cls<R, MS, INIT, Ms...>(cls - 1, mk, v, dt, st, pr, I, G);
     } else {
@@ -154,7 +154,8 @@ __device__ __forceinline__ void channels_cls(int cls, uint32_t mk, R v, R dt, R*
 template <typename R, int MS, bool INIT, uint32_t... Ms>
 __device__ __forceinline__ void channels_list(MaskList<Ms...>, int cls, uint32_t mk, R v, R dt, R* st,
                                               const float* pr, R& I, R& G) {
-    channels_cls<R, MS, INIT, Ms...>(cls, mk, v, dt, st, pr, I, G);
+    if constexpr (sizeof...(Ms) > 0) channels_cls<R, MS, INIT, Ms...>(cls, mk, v, dt, st, pr, I, G);
+    else channels<R, MS, INIT>(mk, v, dt, st, pr, I, G);
 }
 
 // The per-step channel update.  (I, G) come back in registers.
@@ -162,11 +163,10 @@ template <typename R>
 struct CurrentG {
     R I, G;
 };
-template <typename R, int MS>
+template <typename R, int MS, typename Classes>
 __device__ __forceinline__ CurrentG<R> channels_step(int cls, uint32_t mk, R v, R dt, R* st, const float* pr) {
     CurrentG<R> o;
-    if constexpr (MS == 0) channels_list<R, MS, false>(TTPCClasses{}, cls, mk, v, dt, st, pr, o.I, o.G);
-    else channels_list<R, MS, false>(MainenClasses{}, cls, mk, v, dt, st, pr, o.I, o.G);
+    channels_list<R, MS, false>(Classes{}, cls, mk, v, dt, st, pr, o.I, o.G);
     return o;
 }
 
@@ -211,7 +211,7 @@ __device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A, int g) {
 // Shared memory: the node records.
 template <typename R>
 struct SmemPlan {
-    static size_t bytes(int n_nodes) { return sizeof(NodeRec<R>) * (size_t)n_nodes; }
+    static __host__ __device__ size_t bytes(int n_nodes) { return sizeof(NodeRec<R>) * (size_t)n_nodes; }
 };
 
 // Bulk prefetch of a run of rows into L2 (one instruction per contiguous block).
@@ -305,7 +305,7 @@ __device__ __forceinline__ void eliminate_range(const Group<R>& G, const NodeRec
 // then the node's row for the next step: its excess x (the grounded
 // conductance g + cm/dt), right-hand side, and e = b_i (V_p - V_i), the
 // axial term of the parent's row.
-template <typename R, int MS, bool INIT>
+template <typename R, int MS, bool INIT, typename Classes = NoClasses>
 __device__ __forceinline__ void assemble_node(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n, int i,
                                               R V, R vp, R dt, R dtn_inv, R istim_amp, R& x, R& rhs, R& e) {
     R I, Gm;
@@ -313,7 +313,7 @@ __device__ __forceinline__ void assemble_node(const SimArgs<R>& A, const Group<R
         channels<R, MS, true>((uint32_t)n.mask, V, dt, G.slab + (size_t)n.srow * kLanes, G.ptab + (size_t)n.prow * kLanes,
                               I, Gm);
     } else {
-        const CurrentG<R> ig = channels_step<R, MS>(n.cls, n.mask, V, dt, G.slab + (size_t)n.srow * kLanes,
+        const CurrentG<R> ig = channels_step<R, MS, Classes>(n.cls, n.mask, V, dt, G.slab + (size_t)n.srow * kLanes,
                                                    G.ptab + (size_t)n.prow * kLanes);
         I = ig.I;
         Gm = ig.G;
@@ -552,7 +552,7 @@ __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>
 // skeleton: its row goes to the skeleton), and, for a segment (lk >= 0),
 // the spine sep-1 .. r.  Every channel update of a step goes through this
 // one loop, so the channel code is inlined once.
-template <typename R, int MS>
+template <typename R, int MS, typename Classes>
 __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
                                               int lo, int hi, int sep, int r, int lk, R dt, R dtn_inv,
                                               R istim_amp) {
@@ -585,7 +585,7 @@ __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R
         vi = nd.parent;
         vv = vp;
         R x, rhs, e;
-        assemble_node<R, MS, false>(A, G, nd, i, V, vp, dt, dtn_inv, istim_amp, x, rhs, e);
+        assemble_node<R, MS, false, Classes>(A, G, nd, i, V, vp, dt, dtn_inv, istim_amp, x, rhs, e);
         if (p < n_light) {
             eliminate_node(G, nd, i, x, rhs, e, k.x, k.r);
         } else if (p < n_sep) {
@@ -613,7 +613,7 @@ __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R
 // operations as one launch.  n_steps timesteps of group g; the items are
 // shared by however many warps the CTA has (the split was sized for
 // A.n_warps).
-template <typename R, int MS>
+template <typename R, int MS, typename Classes>
 __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0, int n_steps, char* smem,
                                              int* ctr) {
     const Group<R> G = group_of(A, g);
@@ -698,7 +698,7 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
                 const DevSep sp = A.seps[k - A.n_comps];
                 if (sp.seg < 0) sep = sp.node;  // separators ending a segment are their segment's
             }
-            channels_item<R, MS>(A, G, nr, lo, hi, sep, r, lk, dt, dtn_inv, istim_amp);
+            channels_item<R, MS, Classes>(A, G, nr, lo, hi, sep, r, lk, dt, dtn_inv, istim_amp);
         }
         __syncthreads();
     }
@@ -709,7 +709,7 @@ template <typename R, int MS>
 __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim_advance(SimArgs<R> A, int t0, int n_steps) {
     extern __shared__ __align__(128) char smem[];
     __shared__ int ctr[2];
-    advance_body<R, MS>(A, blockIdx.x, t0, n_steps, smem, ctr);
+    advance_body<R, MS, NoClasses>(A, blockIdx.x, t0, n_steps, smem, ctr);
 }
 
 // Several simulations (morphologies of different sizes, one mechanism set)
@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS)
     extern __shared__ __align__(128) char smem[];
     __shared__ int ctr[2];
     const int k = batch_member(B.cta0, B.n);
-    advance_body<R, MS>(B.sim[k], blockIdx.x - B.cta0[k], t0, n_steps, smem, ctr);
+    advance_body<R, MS, NoClasses>(B.sim[k], blockIdx.x - B.cta0[k], t0, n_steps, smem, ctr);
 }
 
 // Parameter table: ptab[g][row][lane] = params[set][row_param[row]][row_sec[row]]

@@ -178,6 +178,13 @@ class Simulator:
         _ffi.check("ngpu_sim_get_trace", _ffi.lib().ngpu_sim_get_trace(
             self._h, C.c_void_p(dev_ptr), 1, _stream_ptr(stream)))
 
+    def classes(self) -> int:
+        """Mechanism masks compiled into the kernel that runs this simulation
+        (0: the ahead-of-time kernel, generic channel code); after init()."""
+        n = C.c_int32()
+        _ffi.check("ngpu_sim_classes", _ffi.lib().ngpu_sim_classes(self._h, C.byref(n)))
+        return n.value
+
     def n_bad(self, stream=None) -> int:
         n = C.c_int32()
         _ffi.check("ngpu_sim_check", _ffi.lib().ngpu_sim_check(self._h, C.byref(n), _stream_ptr(stream)))

@@ -1,0 +1,91 @@
+"""Runtime specialisation of the advance kernel (NVRTC, ngpu_jit.h).
+
+CPU: the generated translation unit compiles for sm_100a through the C ABI
+(ngpu_jit_build; NVRTC needs no device) for both mechanism sets, and the
+compiled image is reused from the on-disk cache.
+GPU: FP32 simulations run the specialised kernel (ngpu_sim_classes > 0) and
+agree with the ahead-of-time kernel (NGPU_JIT=0, generic channel code): the
+same arithmetic with the mechanism tests folded, so traces agree to FP32
+rounding order (bound: the FP32 parity bounds of test_gpu_parity, and the
+subthreshold difference far below them).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from helpers import spike_time_error, subthreshold_error
+
+
+def _masks(w):
+    m = w.cell.mech_mask.astype(np.int64)
+    return np.unique((m << np.arange(m.shape[0])[:, None]).sum(0)).astype(np.uint32)
+
+
+@pytest.mark.parametrize("name", ["ttpc_like", "hh_active"])
+def test_jit_builds_for_sm100a(ngpu_built, tmp_path, monkeypatch, name):
+    from neurogpu_b200 import _ffi, configs
+    w = getattr(configs, name)(n_sets=2, t_stop=1.0)
+    masks = _masks(w)
+    monkeypatch.setenv("NGPU_JIT_CACHE", str(tmp_path))
+    L = _ffi.lib()
+    n = C.c_int64(0)
+    rc = L.ngpu_jit_build(w.cell.mechset.id, masks.ctypes.data, len(masks), 10, 0, C.byref(n))
+    assert rc == 0, L.ngpu_last_error()
+    assert n.value > 0
+    cached = list(tmp_path.glob("*.cubin"))
+    assert len(cached) == 1 and cached[0].stat().st_size == n.value
+    n2 = C.c_int64(0)
+    assert L.ngpu_jit_build(w.cell.mechset.id, masks.ctypes.data, len(masks), 10, 0, C.byref(n2)) == 0
+    assert n2.value == n.value
+
+
+def test_jit_build_rejects_bad_arguments(ngpu_built):
+    from neurogpu_b200 import _ffi
+    L = _ffi.lib()
+    n = C.c_int64(0)
+    m = np.array([1], dtype=np.uint32)
+    assert L.ngpu_jit_build(7, m.ctypes.data, 1, 10, 0, C.byref(n)) != 0
+    many = np.arange(1, 18, dtype=np.uint32)
+    assert L.ngpu_jit_build(0, many.ctypes.data, len(many), 10, 0, C.byref(n)) != 0
+
+
+def _run(w, jit: bool):
+    from neurogpu_b200.sim import Simulator
+    old = os.environ.get("NGPU_JIT")
+    os.environ["NGPU_JIT"] = "1" if jit else "0"
+    try:
+        sim = Simulator(w.cell, w.n_sets, w.n_stim, "fp32")
+        sim.set_params(w.params)
+        sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+        sim.set_recording(w.rec_nodes)
+        sim.init(w.v_init)
+        sim.advance(0, w.nt)
+        out, classes, bad = sim.trace(), sim.classes(), sim.n_bad()
+        sim.close()
+    finally:
+        if old is None:
+            os.environ.pop("NGPU_JIT", None)
+        else:
+            os.environ["NGPU_JIT"] = old
+    return out, classes, bad
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["ttpc_like", "hh_active"])
+def test_specialised_kernel_matches_generic(ngpu_built, name):
+    from neurogpu_b200 import _ffi, configs
+    w = getattr(configs, name)(n_sets=16, t_stop=150.0)
+    jit, n_cls, bad_j = _run(w, True)
+    gen, n_gen, bad_g = _run(w, False)
+    assert n_cls == len(_masks(w)), _ffi.lib().ngpu_jit_log()
+    assert n_gen == 0
+    assert bad_j == 0 and bad_g == 0
+    dt = float(w.dt)
+    err, mismatched = spike_time_error(jit, gen, dt)
+    sub = subthreshold_error(jit, gen, dt)
+    print(f"{name}: specialised vs generic: spike times {err:.2e} ms, subthreshold {sub:.2e} mV")
+    assert mismatched == 0
+    assert err <= 0.05
+    assert sub <= 0.01
