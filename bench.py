@@ -40,7 +40,7 @@ METRIC = "compartment-steps/s (TTPC-like x4096)"
 UNIT = "compartment-steps/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-TRAFFIC_FILE = ROOT / "profiles" / "k_sim_advance_ttpc_like_x4096.md"
+TRAFFIC_FILE = ROOT / "profiles" / "ngpu_jit_advance_ttpc_like_x4096.md"
 
 
 def parse_args():

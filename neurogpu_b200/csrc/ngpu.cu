@@ -261,7 +261,11 @@ static Partition make_partition(const ngpu_model* m, int W) {
         }
     }
     auto heavy = [&](int i) { return (i + 1 < N && par[i + 1] == i) ? i + 1 : -1; };
-    const int64_t target = std::max<int64_t>(1, (subw[0] + W - 1) / W);
+    // items of at most ~1/(2W) of the cost: twice as many items as warps balance the
+    // dynamic queue better than one per warp (measured on B200: -10 % step time on the
+    // 500-compartment HH model, unchanged on the TTPC-like one), at a few more separators
+    const int64_t parts = W > 1 ? 2 * (int64_t)W : 1;
+    const int64_t target = std::max<int64_t>(1, (subw[0] + parts - 1) / parts);
     std::vector<char> is_sep(N, 0);
     is_sep[0] = 1;
     struct Raw { int r, l; };
