@@ -206,9 +206,10 @@ def _inputs(u: np.ndarray, n_stim: int) -> np.ndarray:
 
 def run_screened(prob: FitProblem, pop_size: int, generations: int, keep_frac: float = 0.1,
                  n_train: int = 20000, train_epochs: int = 30, tune_epochs: int = 3, err_bound: float = 0.5,
-                 seed: int = 0) -> GAResult:
+                 seed: int = 0, target: float | None = None, time_budget: float | None = None) -> GAResult:
     """The surrogate-screened GA (wall time includes building the training
-    set and training)."""
+    set and training).  Stops after `generations`, or once the best score is
+    <= target, or once time_budget wall seconds have passed."""
     from .surrogate import SurrogateMLP
     rng = np.random.default_rng(seed)
     res = GAResult()
@@ -247,5 +248,7 @@ def run_screened(prob: FitProblem, pop_size: int, generations: int, keep_frac: f
         res.best.append(float(score[0]))
         res.time.append(time.perf_counter() - t0)
         res.sims.append(prob.sim_count)
+        if (target is not None and score[0] <= target) or (time_budget is not None and res.time[-1] >= time_budget):
+            break
     res.best_u = pop[0]
     return res
