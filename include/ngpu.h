@@ -40,7 +40,7 @@ enum {
 /* Mechanism sets compiled into the library (the reference generates one
  * channel library per model: U/AllModels.cu for the TTPC cell,
  * Figures/FigureS4_mainen/CParsed/AllModels.cu for the Mainen cell). */
-enum { NGPU_MECHSET_TTPC = 0, NGPU_MECHSET_MAINEN = 1 };
+enum { NGPU_MECHSET_TTPC = 0, NGPU_MECHSET_MAINEN = 1, NGPU_MECHSET_GENERATED = 2 /* first defined set */ };
 enum { NGPU_FP32 = 0, NGPU_FP64 = 1 };
 
 typedef struct ngpu_model ngpu_model;
@@ -55,6 +55,25 @@ int ngpu_device_count(int32_t *n);
 int ngpu_set_device(int32_t device);
 /* Mechanism set description: number of mechanisms / parameters. */
 int ngpu_mechset_info(int32_t mechset, int32_t *n_mech, int32_t *n_params);
+
+/*
+ * A mechanism set defined by its channel source, generated from NMODL files
+ * by neurogpu_b200.nmodl (the counterpart of the reference's per-model
+ * AllModels.cu, which P/extractModel.py writes from NEURON's translation of
+ * the .mod files and the simulator is rebuilt with).  source defines
+ *   template <typename R, bool INIT, typename MK> NGPU_HD void
+ *   ngpu::generated_node(MK mk, R v, R dt, R* st, const float* pr, R& I, R& G)
+ * over the mechanisms in mask-bit order; state_rows[k], n_mech_params[k] and
+ * the concatenated mech_param_index give each mechanism's state rows and the
+ * parameters (indices into the n_params of an AllParams row block) it reads;
+ * cost[k] weighs it for the split over warps.  *mechset receives the new id
+ * (NGPU_MECHSET_GENERATED + k), usable with ngpu_model_create.  Models of a
+ * defined set run only through runtime compilation (FP32 and FP64; not
+ * ngpu_run_static): their first initialisation compiles the kernels.
+ */
+int ngpu_mechset_define(const char *name, const char *source, int32_t n_mech, const int32_t *state_rows,
+                        const int32_t *n_mech_params, const int32_t *mech_param_index, int32_t n_params,
+                        const int32_t *cost, int32_t *mechset);
 
 /*
  * Morphology + channel placement, shared by every instance.
@@ -194,8 +213,8 @@ int ngpu_sim_trace_device(ngpu_sim *s, const float **trace, int32_t *n_inst_padd
  *   ngpu_jit_log      the last compile failure or reason for falling back
  */
 int ngpu_sim_classes(const ngpu_sim *s, int32_t *n_classes);
-int ngpu_jit_build(int32_t mechset, const uint32_t *masks, int32_t n_masks, int32_t cc_major,
-                   int32_t cc_minor, int64_t *cubin_bytes);
+int ngpu_jit_build(int32_t mechset, int32_t precision, const uint32_t *masks, int32_t n_masks,
+                   int32_t cc_major, int32_t cc_minor, int64_t *cubin_bytes);
 const char *ngpu_jit_log(void);
 
 /*

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -59,7 +60,27 @@ struct SetDesc {
     uint32_t ca_dyn_bit;
 };
 
+// Mechanism sets generated from NMODL files (ngpu_mechset_define): their
+// layout tables and device source; ids from NGPU_MECHSET_GENERATED on.
+struct GenSet {
+    SetDesc desc;
+    std::string name, source;
+};
+std::mutex g_gen_mu;
+std::vector<std::unique_ptr<GenSet>> g_gen;  // never shrinks: references stay valid
+
+const GenSet* gen_set(int ms) {
+    std::lock_guard<std::mutex> lock(g_gen_mu);
+    const int k = ms - NGPU_MECHSET_GENERATED;
+    return (k >= 0 && k < (int)g_gen.size()) ? g_gen[k].get() : nullptr;
+}
+
+bool mechset_known(int ms) {
+    return ms == NGPU_MECHSET_TTPC || ms == NGPU_MECHSET_MAINEN || gen_set(ms) != nullptr;
+}
+
 const SetDesc& set_desc(int ms) {
+    if (ms >= NGPU_MECHSET_GENERATED) return gen_set(ms)->desc;
     // TTPC: GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/src/CudaStuff.cu:220 call list.
     static const SetDesc ttpc = {
         19,
@@ -439,6 +460,12 @@ template <typename R>
 static cudaError_t launch_init(ngpu_sim* s, cudaStream_t st) {
     SimArgs<R> A = make_args<R>(s);
     const int threads = kLanes * s->n_warps;
+    if (s->jit) {
+        void* args[] = {(void*)&A};
+        const cudaError_t e = cudaLaunchKernel((const void*)s->jit->init, dim3(s->n_groups), dim3(threads), args, 0, st);
+        g_launches++;
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     if (s->m->mechset == NGPU_MECHSET_TTPC) k_sim_init<R, 0><<<s->n_groups, threads, 0, st>>>(A);
     else k_sim_init<R, 1><<<s->n_groups, threads, 0, st>>>(A);
     g_launches++;
@@ -451,7 +478,7 @@ static cudaError_t launch_advance(ngpu_sim* s, int t0, int n, cudaStream_t st) {
     const int threads = kLanes * s->n_warps;
     const size_t smem = SmemPlan<R>::bytes(s->m->n);
     cudaError_t e;
-    if (std::is_same<R, float>::value && s->jit) {
+    if (s->jit) {
         const void* k = (const void*)s->jit->advance;
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -496,11 +523,45 @@ int ngpu_set_device(int32_t device) {
 }
 
 int ngpu_mechset_info(int32_t mechset, int32_t* n_mech, int32_t* n_params) {
-    if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN)
-        return fail(NGPU_E_INVALID, "unknown mechanism set");
+    if (!mechset_known(mechset)) return fail(NGPU_E_INVALID, "unknown mechanism set");
     const SetDesc& sd = set_desc(mechset);
     if (n_mech) *n_mech = (int32_t)sd.mechs.size();
     if (n_params) *n_params = sd.n_params;
+    return NGPU_OK;
+}
+
+int ngpu_mechset_define(const char* name, const char* source, int32_t n_mech, const int32_t* state_rows,
+                        const int32_t* n_mech_params, const int32_t* mech_param_index, int32_t n_params,
+                        const int32_t* cost, int32_t* mechset) {
+    if (!name || !source || !state_rows || !n_mech_params || !cost || !mechset)
+        return fail(NGPU_E_INVALID, "null argument");
+    if (n_mech < 1 || n_mech > 16) return fail(NGPU_E_INVALID, "a mechanism set holds 1..16 mechanisms");
+    if (n_params < 0 || n_params > 4096) return fail(NGPU_E_INVALID, "n_params out of range");
+    auto g = std::make_unique<GenSet>();
+    g->name = name;
+    g->source = source;
+    g->desc.n_params = n_params;
+    g->desc.needs_ca_dyn = 0;
+    g->desc.ca_dyn_bit = 0;
+    int off = 0;
+    for (int k = 0; k < n_mech; ++k) {
+        if (state_rows[k] < 0 || state_rows[k] > 64 || n_mech_params[k] < 0 || n_mech_params[k] > 64 || cost[k] < 0)
+            return fail(NGPU_E_INVALID, "mechanism " + std::to_string(k) + ": bad row counts or cost");
+        MechDesc md;
+        md.state_rows = state_rows[k];
+        md.cost = cost[k];
+        for (int j = 0; j < n_mech_params[k]; ++j) {
+            const int pi = mech_param_index ? mech_param_index[off + j] : -1;
+            if (pi < 0 || pi >= n_params) return fail(NGPU_E_INVALID, "parameter index out of range");
+            md.params.push_back(pi);
+        }
+        off += n_mech_params[k];
+        g->desc.mechs.push_back(md);
+    }
+    std::lock_guard<std::mutex> lock(g_gen_mu);
+    if (g_gen.size() >= 1000) return fail(NGPU_E_INVALID, "too many mechanism sets defined");
+    g_gen.push_back(std::move(g));
+    *mechset = NGPU_MECHSET_GENERATED + (int32_t)g_gen.size() - 1;
     return NGPU_OK;
 }
 
@@ -511,8 +572,7 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
     *out = nullptr;
     if (n_nodes < 1 || !parent || !a || !b || !cm || !section || !mech_mask || n_sections < 1)
         return fail(NGPU_E_INVALID, "model arrays missing or empty");
-    if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN)
-        return fail(NGPU_E_INVALID, "unknown mechanism set");
+    if (!mechset_known(mechset)) return fail(NGPU_E_INVALID, "unknown mechanism set");
     const SetDesc& sd = set_desc(mechset);
     const int NM = (int)sd.mechs.size();
     if (parent[0] != -1) return fail(NGPU_E_INVALID, "parent[0] must be -1 (node 0 is the root)");
@@ -1050,9 +1110,15 @@ struct ngpu_batch {
 static int sim_upload_nodes(ngpu_sim* s) {
     const ngpu_model* m = s->m;
     s->jit = nullptr;
-    if (s->precision == NGPU_FP32) {
+    const GenSet* gs = gen_set(m->mechset);
+    if (s->precision == NGPU_FP32 || gs) {
         if (s->batch) s->jit = s->batch->jit;
-        else s->jit = ngpu_jit::module(m->mechset, ngpu_jit::pick_masks(model_masks(m), kMaxClasses));
+        else
+            s->jit = ngpu_jit::module(m->mechset, s->precision == NGPU_FP64,
+                                      ngpu_jit::pick_masks(model_masks(m), kMaxClasses), gs ? &gs->source : nullptr);
+        if (gs && !s->jit)
+            return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
+                                         "' runs only through runtime compilation: " + ngpu_jit::last_log());
     }
     std::vector<int> uniq(s->n_rec_unique, -1);
     for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
@@ -1109,12 +1175,17 @@ template <typename R>
 static cudaError_t launch_batch(ngpu_batch* b, bool init, int t0, int n, cudaStream_t st) {
     const BatchArgs<R> B = make_batch_args<R>(b);
     cudaError_t e;
-    if (std::is_same<R, float>::value && b->jit && !init) {
-        const void* k = (const void*)b->jit->batch_advance;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
-        if (e != cudaSuccess) return e;
-        void* args[] = {(void*)&B, (void*)&t0, (void*)&n};
-        e = cudaLaunchKernel(k, dim3(b->total_ctas), dim3(b->threads), args, b->smem, st);
+    if (b->jit) {
+        if (init) {
+            void* args[] = {(void*)&B};
+            e = cudaLaunchKernel((const void*)b->jit->batch_init, dim3(b->total_ctas), dim3(b->threads), args, 0, st);
+        } else {
+            const void* k = (const void*)b->jit->batch_advance;
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+            if (e != cudaSuccess) return e;
+            void* args[] = {(void*)&B, (void*)&t0, (void*)&n};
+            e = cudaLaunchKernel(k, dim3(b->total_ctas), dim3(b->threads), args, b->smem, st);
+        }
         g_launches++;
         return e != cudaSuccess ? e : cudaGetLastError();
     }
@@ -1182,13 +1253,20 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
                                                              : SmemPlan<float>::bytes(s->m->n));
     }
     b->threads = kLanes * W;
-    if (b->precision == NGPU_FP32) {  // one specialised kernel over every member's masks
+    const GenSet* gs = gen_set(b->mechset);
+    if (b->precision == NGPU_FP32 || gs) {  // one specialised kernel over every member's masks
         std::vector<uint32_t> all;
         for (ngpu_sim* s : b->sims) {
             const std::vector<uint32_t> mm = model_masks(s->m);
             all.insert(all.end(), mm.begin(), mm.end());
         }
-        b->jit = ngpu_jit::module(b->mechset, ngpu_jit::pick_masks(all, kMaxClasses));
+        b->jit = ngpu_jit::module(b->mechset, b->precision == NGPU_FP64, ngpu_jit::pick_masks(all, kMaxClasses),
+                                  gs ? &gs->source : nullptr);
+        if (gs && !b->jit) {
+            delete b;
+            return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
+                                         "' runs only through runtime compilation: " + ngpu_jit::last_log());
+        }
     }
     for (ngpu_sim* s : b->sims) {
         s->batch = b;
@@ -1277,13 +1355,13 @@ int ngpu_batch_run_graph(ngpu_batch* b, float v_init, int32_t nt, int32_t chunk,
         batch_drop_graph(b);
         // set the shared-memory attribute outside the capture
         cudaError_t e = cudaSuccess;
-        if (b->precision == NGPU_FP64)
+        if (b->jit)
+            e = cudaFuncSetAttribute((const void*)b->jit->batch_advance, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)b->smem);
+        else if (b->precision == NGPU_FP64)
             e = b->mechset == NGPU_MECHSET_TTPC
                     ? cudaFuncSetAttribute(k_batch_advance<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem)
                     : cudaFuncSetAttribute(k_batch_advance<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
-        else if (b->jit)
-            e = cudaFuncSetAttribute((const void*)b->jit->batch_advance, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)b->smem);
         else
             e = b->mechset == NGPU_MECHSET_TTPC
                     ? cudaFuncSetAttribute(k_batch_advance<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem)
@@ -1326,17 +1404,20 @@ int ngpu_sim_classes(const ngpu_sim* s, int32_t* n_classes) {
     return NGPU_OK;
 }
 
-int ngpu_jit_build(int32_t mechset, const uint32_t* masks, int32_t n_masks, int32_t cc_major, int32_t cc_minor,
-                   int64_t* cubin_bytes) {
+int ngpu_jit_build(int32_t mechset, int32_t precision, const uint32_t* masks, int32_t n_masks, int32_t cc_major,
+                   int32_t cc_minor, int64_t* cubin_bytes) {
     if (!cubin_bytes || (n_masks > 0 && !masks)) return fail(NGPU_E_INVALID, "null argument");
-    if (mechset != NGPU_MECHSET_TTPC && mechset != NGPU_MECHSET_MAINEN) return fail(NGPU_E_INVALID, "unknown mechset");
-    if (n_masks < 1 || n_masks > kMaxClasses)
+    if (!mechset_known(mechset)) return fail(NGPU_E_INVALID, "unknown mechset");
+    if (precision != NGPU_FP32 && precision != NGPU_FP64) return fail(NGPU_E_INVALID, "precision must be FP32 or FP64");
+    const GenSet* gs = gen_set(mechset);
+    if (n_masks < (gs ? 0 : 1) || n_masks > kMaxClasses)
         return fail(NGPU_E_INVALID, "1.." + std::to_string(kMaxClasses) + " masks");
     std::vector<char> cubin;
     std::string err;
     const std::vector<uint32_t> mv(masks, masks + n_masks);
     std::lock_guard<std::mutex> lock(ngpu_jit::mu());
-    if (!ngpu_jit::build_cubin(mechset, mv, std::to_string(cc_major) + std::to_string(cc_minor) + "a", &cubin, &err)) {
+    if (!ngpu_jit::build_cubin(gs ? 2 : mechset, precision == NGPU_FP64, mv, gs ? &gs->source : nullptr,
+                               std::to_string(cc_major) + std::to_string(cc_minor) + "a", &cubin, &err)) {
         ngpu_jit::last_log() = err;
         return fail(NGPU_E_CUDA, "runtime compilation failed: " + err);
     }
@@ -1494,6 +1575,9 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
                                float* out_dev, void* cuda_stream) {
     if (!m || !params_dev || !amps_dev || !dts_dev || !rec_nodes || !out_dev)
         return fail(NGPU_E_INVALID, "ngpu_run_static: null argument");
+    if (m->mechset >= NGPU_MECHSET_GENERATED)
+        return fail(NGPU_E_INVALID, "ngpu_run_static: a mechanism set generated from NMODL files runs only "
+                                    "through runtime compilation (ngpu_run / ngpu_sim_*)");
     const int N = m->n;
     if (N > kStaticMaxNodes)
         return fail(NGPU_E_INVALID, "ngpu_run_static: at most " + std::to_string(kStaticMaxNodes) +

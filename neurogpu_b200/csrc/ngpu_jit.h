@@ -15,6 +15,8 @@
 // version, under $NGPU_JIT_CACHE or $HOME/.cache/neurogpu_b200.  When NVRTC
 // is missing or a compile fails, callers keep the ahead-of-time kernels (the
 // generic channel code); NGPU_JIT=0 in the environment selects them too.
+// Mechanism sets generated from NMODL files (ngpu_mechset_define) exist only
+// as source and always run through this path, in FP32 and FP64.
 #pragma once
 #include <cuda_runtime.h>
 #include <dlfcn.h>
@@ -36,10 +38,13 @@ namespace ngpu_jit {
 
 struct Module {
     int mechset = 0;
+    bool fp64 = false;
     std::vector<uint32_t> masks;            // class k runs the code for masks[k]
     cudaLibrary_t lib = nullptr;
-    cudaKernel_t advance = nullptr;        // (SimArgs<float>, int t0, int n_steps)
-    cudaKernel_t batch_advance = nullptr;  // (BatchArgs<float>, int t0, int n_steps)
+    cudaKernel_t init = nullptr;           // (SimArgs<R>)
+    cudaKernel_t advance = nullptr;        // (SimArgs<R>, int t0, int n_steps)
+    cudaKernel_t batch_init = nullptr;     // (BatchArgs<R>)
+    cudaKernel_t batch_advance = nullptr;  // (BatchArgs<R>, int t0, int n_steps)
 };
 
 struct Nvrtc {
@@ -96,25 +101,42 @@ inline bool enabled() {
     return !(e && e[0] == '0');
 }
 
-// The generated translation unit: both advance kernels over `masks`.
-inline std::string source(int mechset, const std::vector<uint32_t>& masks) {
+// The generated translation unit: the init and advance kernels (single and
+// batch) over `masks`.  ms: the kernel template's mechanism set (0 TTPC,
+// 1 Mainen, 2 a generated set, whose channel code comes in as the extra
+// header ngpu_generated.cuh).
+inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks) {
     std::string list;
     for (size_t k = 0; k < masks.size(); ++k) list += (k ? ", " : "") + std::to_string(masks[k]) + "u";
-    const std::string ms = std::to_string(mechset);
-    return "#include \"sim_kernels.cuh\"\n"
+    const std::string m = std::to_string(ms);
+    const std::string R = fp64 ? "double" : "float";
+    const std::string lb = "__launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)";
+    return std::string(ms == 2 ? "#define NGPU_GENERATED_NODE 1\n" : "") +
+           "#include \"sim_kernels.cuh\"\n"
            "using JitClasses = ngpu::MaskList<" + list + ">;\n"
-           "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)\n"
-           "ngpu_jit_advance(ngpu::SimArgs<float> A, int t0, int n_steps) {\n"
+           "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps)\n"
+           "ngpu_jit_init(ngpu::SimArgs<" + R + "> A) {\n"
+           "    __shared__ int ctr;\n"
+           "    ngpu::init_body<" + R + ", " + m + ">(A, blockIdx.x, &ctr);\n"
+           "}\n"
+           "extern \"C\" __global__ void " + lb + "\n"
+           "ngpu_jit_advance(ngpu::SimArgs<" + R + "> A, int t0, int n_steps) {\n"
            "    extern __shared__ __align__(128) char smem[];\n"
            "    __shared__ int ctr[2];\n"
-           "    ngpu::advance_body<float, " + ms + ", JitClasses>(A, blockIdx.x, t0, n_steps, smem, ctr);\n"
+           "    ngpu::advance_body<" + R + ", " + m + ", JitClasses>(A, blockIdx.x, t0, n_steps, smem, ctr);\n"
            "}\n"
-           "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)\n"
-           "ngpu_jit_batch_advance(const __grid_constant__ ngpu::BatchArgs<float> B, int t0, int n_steps) {\n"
+           "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps)\n"
+           "ngpu_jit_batch_init(const __grid_constant__ ngpu::BatchArgs<" + R + "> B) {\n"
+           "    __shared__ int ctr;\n"
+           "    const int k = ngpu::batch_member(B.cta0, B.n);\n"
+           "    ngpu::init_body<" + R + ", " + m + ">(B.sim[k], blockIdx.x - B.cta0[k], &ctr);\n"
+           "}\n"
+           "extern \"C\" __global__ void " + lb + "\n"
+           "ngpu_jit_batch_advance(const __grid_constant__ ngpu::BatchArgs<" + R + "> B, int t0, int n_steps) {\n"
            "    extern __shared__ __align__(128) char smem[];\n"
            "    __shared__ int ctr[2];\n"
            "    const int k = ngpu::batch_member(B.cta0, B.n);\n"
-           "    ngpu::advance_body<float, " + ms + ", JitClasses>(B.sim[k], blockIdx.x - B.cta0[k], t0, n_steps,\n"
+           "    ngpu::advance_body<" + R + ", " + m + ", JitClasses>(B.sim[k], blockIdx.x - B.cta0[k], t0, n_steps,\n"
            "                                                   smem, ctr);\n"
            "}\n";
 }
@@ -134,15 +156,16 @@ inline std::string cache_dir() {
 }
 
 // NVRTC compile of the kernels over `masks` for sm_<arch> (e.g. "100a"),
-// through the on-disk cache.  Touches no device.
-inline bool build_cubin(int mechset, const std::vector<uint32_t>& masks, const std::string& arch,
-                        std::vector<char>* out, std::string* err) {
+// through the on-disk cache.  Touches no device.  generated: the channel
+// code of a generated mechanism set (ms 2), or nullptr.
+inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, const std::string* generated,
+                        const std::string& arch, std::vector<char>* out, std::string* err) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) {
         *err = last_log();
         return false;
     }
-    const std::string src = source(mechset, masks);
+    const std::string src = source(ms, fp64, masks);
     std::vector<std::string> opt_s = {"--gpu-architecture=sm_" + arch, "-std=c++17",
                                       "-lineinfo"};
     int vmaj = 0, vmin = 0;
@@ -151,13 +174,20 @@ inline bool build_cubin(int mechset, const std::vector<uint32_t>& masks, const s
     h = fnv1a(h, src);
     for (const auto& o : opt_s) h = fnv1a(h, o);
     h = fnv1a(h, std::to_string(vmaj) + "." + std::to_string(vmin));
-    std::vector<std::string> hdr_text(kJitFileCount);
-    std::vector<const char*> hdr_src(kJitFileCount), hdr_name(kJitFileCount);
+    const int n_hdr = kJitFileCount + (generated ? 1 : 0);
+    std::vector<std::string> hdr_text(n_hdr);
+    std::vector<const char*> hdr_src(n_hdr), hdr_name(n_hdr);
     for (int f = 0; f < kJitFileCount; ++f) {
         for (int c = 0; c < kJitFiles[f].n_chunks; ++c) hdr_text[f] += kJitFiles[f].chunks[c];
         hdr_src[f] = hdr_text[f].c_str();
         hdr_name[f] = kJitFiles[f].name;
         h = fnv1a(h, hdr_text[f]);
+    }
+    if (generated) {
+        hdr_text[kJitFileCount] = *generated;
+        hdr_src[kJitFileCount] = hdr_text[kJitFileCount].c_str();
+        hdr_name[kJitFileCount] = "ngpu_generated.cuh";
+        h = fnv1a(h, *generated);
     }
     char hex[17];
     snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
@@ -175,7 +205,7 @@ inline bool build_cubin(int mechset, const std::vector<uint32_t>& masks, const s
         }
     }
     nvrtcProgram prog = nullptr;
-    if (nv.create(&prog, src.c_str(), "ngpu_jit.cu", kJitFileCount, hdr_src.data(), hdr_name.data()) !=
+    if (nv.create(&prog, src.c_str(), "ngpu_jit.cu", n_hdr, hdr_src.data(), hdr_name.data()) !=
         NVRTC_SUCCESS) {
         *err = "nvrtcCreateProgram failed";
         return false;
@@ -216,14 +246,20 @@ inline bool build_cubin(int mechset, const std::vector<uint32_t>& masks, const s
     return true;
 }
 
-// The module for (mechset, masks) on the current device, compiled and
-// loaded on first use; nullptr (reason in last_log()) when runtime
-// compilation is off or fails.  Modules live until the process exits.
-inline const Module* module(int mechset, const std::vector<uint32_t>& masks) {
-    if (!enabled() || masks.empty()) return nullptr;
+// The module for (mechset, precision, masks) on the current device, compiled
+// and loaded on first use; nullptr (reason in last_log()) when runtime
+// compilation is off or fails.  mechset >= 2 is a generated set whose channel
+// code is *generated.  Modules live until the process exits.
+inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>& masks,
+                            const std::string* generated) {
+    if (!generated && (!enabled() || masks.empty())) return nullptr;
+    if (generated && !enabled()) {
+        last_log() = "runtime compilation is off (NGPU_JIT=0)";
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lock(mu());
     static std::map<std::string, std::unique_ptr<Module>> cache;
-    std::string key = std::to_string(mechset) + ":";
+    std::string key = std::to_string(mechset) + (fp64 ? "d:" : "f:");
     for (uint32_t m : masks) key += std::to_string(m) + ",";
     auto it = cache.find(key);
     if (it != cache.end()) return it->second.get();
@@ -242,16 +278,19 @@ inline const Module* module(int mechset, const std::vector<uint32_t>& masks) {
     std::vector<char> cubin;
     std::string err;
     const std::string arch = std::to_string(maj) + std::to_string(min) + "a";
-    if (!build_cubin(mechset, masks, arch, &cubin, &err)) {
+    if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err)) {
         last_log() = err;
         cache[key] = nullptr;
         return nullptr;
     }
     auto mod = std::make_unique<Module>();
     mod->mechset = mechset;
+    mod->fp64 = fp64;
     mod->masks = masks;
     cudaError_t e = cudaLibraryLoadData(&mod->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->init, mod->lib, "ngpu_jit_init");
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->advance, mod->lib, "ngpu_jit_advance");
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->batch_init, mod->lib, "ngpu_jit_batch_init");
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->batch_advance, mod->lib, "ngpu_jit_batch_advance");
     if (e != cudaSuccess) {
         last_log() = std::string("loading the compiled kernels: ") + cudaGetErrorString(e);

@@ -35,12 +35,18 @@ template <> struct Math<float> {
     static NGPU_HD float dv(float a, float b) { return __fdividef(a, b); }
     static NGPU_HD float rc(float a) { return __fdividef(1.0f, a); }
     static NGPU_HD float pw(float a, float b) { return __powf(a, b); }
+    // exp(x) - 1: series below |x| = 1e-2 (truncation < x^5/120), where exp(x) - 1 cancels
+    static NGPU_HD float em1(float x) {
+        if (fabsf(x) < 1e-2f) return x * (1.0f + x * (0.5f + x * (0.16666667f + x * 0.041666668f)));
+        return __expf(x) - 1.0f;
+    }
 #else
     static NGPU_HD float ex(float x) { return expf(x); }
     static NGPU_HD float lg(float x) { return logf(x); }
     static NGPU_HD float dv(float a, float b) { return a / b; }
     static NGPU_HD float rc(float a) { return 1.0f / a; }
     static NGPU_HD float pw(float a, float b) { return powf(a, b); }
+    static NGPU_HD float em1(float x) { return expm1f(x); }
 #endif
     // 1 - exp(-z) for z >= 0 without the cancellation 1 - exp(-z) suffers in
     // FP32 when z = dt/tau is small (slow gates, Ca decay): below z = 1/32 the
@@ -60,6 +66,7 @@ template <> struct Math<double> {
     static NGPU_HD double dv(double a, double b) { return a / b; }
     static NGPU_HD double rc(double a) { return 1.0 / a; }
     static NGPU_HD double pw(double a, double b) { return pow(a, b); }
+    static NGPU_HD double em1(double x) { return expm1(x); }
     static NGPU_HD double one_minus_exp_neg(double z) { return -expm1(-z); }
 };
 

@@ -53,6 +53,9 @@
 #include "channels_ttpc.cuh"
 #include "ngpu_math.cuh"
 #include "node_classes.cuh"
+#ifdef NGPU_GENERATED_NODE  // a mechanism set generated from NMODL files (runtime compilation only)
+#include "ngpu_generated.cuh"
+#endif
 
 namespace ngpu {
 
@@ -131,10 +134,14 @@ struct SimArgs {
 
 // mk: the node's mechanism bits, a runtime value or a std::integral_constant
 // (then every mechanism test folds at compile time).
+// MS: 0 TTPC, 1 Mainen, 2 the generated set of this translation unit.
 template <typename R, int MS, bool INIT, typename MK>
 __device__ __forceinline__ void channels(MK mk, R v, R dt, R* st, const float* pr, R& I, R& G) {
     if constexpr (MS == 0) ttpc_node<R, INIT>(mk, v, dt, st, pr, I, G);
-    else mainen_node<R, INIT>(mk, v, dt, st, pr, I, G);
+    else if constexpr (MS == 1) mainen_node<R, INIT>(mk, v, dt, st, pr, I, G);
+#ifdef NGPU_GENERATED_NODE
+    else generated_node<R, INIT>(mk, v, dt, st, pr, I, G);
+#endif
 }
 
 // Channel update of a node of mechanism-set class cls: class k < sizeof...(Ms)

@@ -75,8 +75,9 @@ class CellModel:
         V read+write (8), Kahan term read+write (8), S_c channel state
         variables read+write (8 each, cai and the carried ica included), P_c
         FP32 parameters read (4 each)."""
-        st_rows = {"ttpc": (2, 2, 2, 1, 1, 2, 2, 2, 2, 2, 0, 1, 1),
-                   "mainen": (2, 2, 1, 1, 1, 2, 0, 0, 0)}[self.mechset.name]
+        st_rows = getattr(self.mechset, "state_rows", None) or {
+            "ttpc": (2, 2, 2, 1, 1, 2, 2, 2, 2, 2, 0, 1, 1),
+            "mainen": (2, 2, 1, 1, 1, 2, 0, 0, 0)}[self.mechset.name]
         total = 0
         for i in range(self.n_nodes):
             on = np.nonzero(self.mech_mask[:, i])[0]

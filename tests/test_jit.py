@@ -31,13 +31,13 @@ def test_jit_builds_for_sm100a(ngpu_built, tmp_path, monkeypatch, name):
     monkeypatch.setenv("NGPU_JIT_CACHE", str(tmp_path))
     L = _ffi.lib()
     n = C.c_int64(0)
-    rc = L.ngpu_jit_build(w.cell.mechset.id, masks.ctypes.data, len(masks), 10, 0, C.byref(n))
+    rc = L.ngpu_jit_build(w.cell.mechset.id, 0, masks.ctypes.data, len(masks), 10, 0, C.byref(n))
     assert rc == 0, L.ngpu_last_error()
     assert n.value > 0
     cached = list(tmp_path.glob("*.cubin"))
     assert len(cached) == 1 and cached[0].stat().st_size == n.value
     n2 = C.c_int64(0)
-    assert L.ngpu_jit_build(w.cell.mechset.id, masks.ctypes.data, len(masks), 10, 0, C.byref(n2)) == 0
+    assert L.ngpu_jit_build(w.cell.mechset.id, 0, masks.ctypes.data, len(masks), 10, 0, C.byref(n2)) == 0
     assert n2.value == n.value
 
 
@@ -46,9 +46,9 @@ def test_jit_build_rejects_bad_arguments(ngpu_built):
     L = _ffi.lib()
     n = C.c_int64(0)
     m = np.array([1], dtype=np.uint32)
-    assert L.ngpu_jit_build(7, m.ctypes.data, 1, 10, 0, C.byref(n)) != 0
+    assert L.ngpu_jit_build(7, 0, m.ctypes.data, 1, 10, 0, C.byref(n)) != 0
     many = np.arange(1, 18, dtype=np.uint32)
-    assert L.ngpu_jit_build(0, many.ctypes.data, len(many), 10, 0, C.byref(n)) != 0
+    assert L.ngpu_jit_build(0, 0, many.ctypes.data, len(many), 10, 0, C.byref(n)) != 0
 
 
 def _run(w, jit: bool):
