@@ -693,8 +693,26 @@ def simplify(e):
                 return Num(0.0)
             if isinstance(r, Num) and r.v == 1:
                 return l
+            if isinstance(r, Bin) and r.op == "/" and isinstance(r.l, Num) and r.l.v == 1:
+                return simplify(Bin("*", l, r.r))          # a / (1/x) = a x
+            if isinstance(r, Un) and r.op == "-":
+                return simplify(Un("-", Bin("/", l, r.e)))
         return Bin(e.op, l, r)
     raise TypeError(e)
+
+
+def recip(e):
+    """1/e, written without a division where e is a quotient."""
+    e = simplify(e)
+    if isinstance(e, Num):
+        return Num(1.0 / e.v)
+    if isinstance(e, Bin) and e.op == "/":
+        if isinstance(e.l, Num) and e.l.v == 1:
+            return e.r
+        return simplify(Bin("/", e.r, e.l))
+    if isinstance(e, Un) and e.op == "-":
+        return simplify(Un("-", recip(e.e)))
+    return Bin("/", Num(1.0), e)
 
 
 def diff(e, x: str, known: dict | None = None):
@@ -716,9 +734,17 @@ def diff(e, x: str, known: dict | None = None):
             return Bin("+", dl, dr)
         if e.op == "-":
             return Bin("-", dl, dr)
+        zl = isinstance(simplify(dl), Num) and simplify(dl).v == 0
+        zr = isinstance(simplify(dr), Num) and simplify(dr).v == 0
         if e.op == "*":
+            if zr:
+                return Bin("*", dl, e.r)
+            if zl:
+                return Bin("*", e.l, dr)
             return Bin("+", Bin("*", dl, e.r), Bin("*", e.l, dr))
         if e.op == "/":
+            if zr:
+                return Bin("/", dl, e.r)
             return Bin("/", Bin("-", Bin("*", dl, e.r), Bin("*", e.l, dr)), Bin("*", e.r, e.r))
         if e.op == "^":
             if isinstance(simplify(dr), Num) and simplify(dr).v == 0:
@@ -819,6 +845,8 @@ class Emitter:
                     return "(" + " * ".join([b] * int(x.r.v)) + ")"
                 return f"M::pw({self.e(x.l)}, {self.e(x.r)})"
             if x.op == "/":
+                if isinstance(x.r, Num) and x.r.v != 0:
+                    return f"({self.e(x.l)} * {_lit(1.0 / x.r.v)})"
                 return f"M::dv({self.e(x.l)}, {self.e(x.r)})"
             if x.op == "%":
                 return f"fmod({self.e(x.l)}, {self.e(x.r)})"
@@ -936,6 +964,22 @@ def generate(mods: dict, name: str = "generated", celsius: float = 34.0, reversa
                             source=src, cost=tuple(cost))
 
 
+def _rate_vars(m: Mechanism) -> set:
+    """Time constants T of equations x' = (X - x)/T that are assigned
+    variables: their reciprocal (the rate) is emitted wherever T is assigned,
+    so the integration needs no division."""
+    out = set()
+    for blk in m.derivatives.values():
+        for s in blk:
+            if isinstance(s, Deriv):
+                e = simplify(s.e)
+                if (isinstance(e, Bin) and e.op == "/" and isinstance(e.r, Var) and isinstance(e.l, Bin)
+                        and e.l.op == "-" and isinstance(e.l.r, Var) and e.l.r.name == s.name):
+                    if e.r.name in m.assigned:
+                        out.add(e.r.name)
+    return out
+
+
 def _conc_alias(m: Mechanism) -> dict:
     """Ion concentrations the mechanism sets to one of its STATEs (cai = ca)."""
     out = {}
@@ -954,6 +998,10 @@ def _emit_set(mechs, mech_params, params, celsius, ktf, reversal, cao, constants
     w('#include "ngpu_math.cuh"')
     w("namespace ngpu {")
     w("template <typename R> NGPU_HD R ngpu_sgn(R x) { return x > (R)0 ? (R)1 : (x < (R)0 ? (R)-1 : (R)0); }")
+    w("// cnexp over dt with the gate's rate 1/tau: x + (1 - exp(-dt rate)) (xinf - x)")
+    w("template <typename R> NGPU_HD R gen_cnexp_rate(R x, R xinf, R rate, R dt) {")
+    w("    return x + Math<R>::one_minus_exp_neg(dt * rate) * (xinf - x);")
+    w("}")
     w("template <typename R, bool INIT, typename MK>")
     w("NGPU_HD void generated_node(MK mk, R v, R dt, R* __restrict__ st, const float* __restrict__ pr, R& I,")
     w("                            R& G) {")
@@ -1002,6 +1050,10 @@ def _emit_set(mechs, mech_params, params, celsius, ktf, reversal, cao, constants
                     env[r] = _lit(cao) if u.ion == "ca" else _lit(_ION_DEFAULT_CONC.get(u.ion, 0.0))
                 elif r == "e" + u.ion:
                     env[r] = f"ion_e{u.ion}"
+        for t in sorted(_rate_vars(m)):
+            if t in env and env[t].startswith(pre):
+                env[t + "@rate"] = env[t] + "_rate"
+                decl.append(env[t] + "_rate")
         if decl:
             w(f"    R {', '.join(dict.fromkeys(decl))};")
         envs.append(env)
@@ -1159,8 +1211,13 @@ class _MechBody:
                 env["v"] = "v_l"
             for l in locs:
                 env[l] = f"l_{l}"
-                w(f"            R l_{l} = 0;")
+            saved = self.consts
+            self.consts = self._fold_locals(body, env, locs)
+            for l in locs:
+                if not env[l].startswith("(R)"):
+                    w(f"            R l_{l} = 0;")
             self._block(w, body, 3, env, mode="proc")
+            self.consts = saved
             w(f"            return ret;")
             w(f"        }};")
         for pname in self._proc_order():
@@ -1175,8 +1232,13 @@ class _MechBody:
                 env["v"] = "v_l"
             for l in locs:
                 env[l] = f"l_{l}"
-                w(f"            R l_{l} = 0;")
+            saved = self.consts
+            self.consts = self._fold_locals(body, env, locs)
+            for l in locs:
+                if not env[l].startswith("(R)"):
+                    w(f"            R l_{l} = 0;")
             self._block(w, body, 3, env, mode="proc")
+            self.consts = saved
             w(f"        }};")
             w(f"        (void){self.procs[pname]};")
         for fname in m.functions:
@@ -1210,6 +1272,31 @@ class _MechBody:
             visit(n)
         return order
 
+    def _fold_locals(self, body, env, locs):
+        """LOCALs assigned once, at the top level, from a constant expression:
+        mapped to the literal (and folded into later expressions)."""
+        count = {}
+
+        def walk(ss):
+            for st in ss:
+                if isinstance(st, Assign):
+                    count[st.name] = count.get(st.name, 0) + 1
+                elif isinstance(st, If):
+                    walk(st.then)
+                    walk(st.other)
+        walk(body)
+        consts = dict(self.consts)
+        for st in body:
+            if isinstance(st, Assign) and st.name in locs and count.get(st.name) == 1:
+                e = st.e
+                for n, val in consts.items():
+                    e = subst(e, n, Num(val))
+                e = simplify(e)
+                if isinstance(e, Num):
+                    consts[st.name] = e.v
+                    env[st.name] = _lit(e.v)
+        return consts
+
     def _locals(self, body, env) -> list:
         """Names assigned in a body that are not mechanism variables: block locals."""
         out = []
@@ -1230,8 +1317,13 @@ class _MechBody:
         pad = "    " * ind
         for l in locs:
             env[l] = f"l_{l}"
-            w(f"{pad}R l_{l} = 0;")
+        saved = self.consts
+        self.consts = self._fold_locals(body, env, locs)
+        for l in locs:
+            if not env[l].startswith("(R)"):
+                w(f"{pad}R l_{l} = 0;")
         self._block(w, body, ind, env, mode)
+        self.consts = saved
 
     def _block(self, w, body, ind, env, mode):
         pad = "    " * ind
@@ -1242,7 +1334,11 @@ class _MechBody:
             if isinstance(s, Assign):
                 if s.name not in env:
                     raise NmodlError(f"{self.m.suffix}: assignment to unknown {s.name!r}")
+                if env[s.name].startswith("(R)"):
+                    continue  # a LOCAL folded to a constant
                 w(f"{pad}{env[s.name]} = {em.e(s.e)};")
+                if s.name + "@rate" in env:
+                    w(f"{pad}{env[s.name + '@rate']} = {em.e(recip(s.e))};")
             elif isinstance(s, Deriv):
                 if mode != "deriv":
                     raise NmodlError(f"{self.m.suffix}: {s.name}' outside a DERIVATIVE block")
@@ -1255,14 +1351,16 @@ class _MechBody:
                         and isinstance(e.l.r, Var) and e.l.r.name == x and x not in free_vars(e.l.l)
                         and x not in free_vars(e.r)):
                     # x' = (xinf - x) / tau
-                    w(f"{pad}{xv} = cnexp({xv}, {em.e(e.l.l)}, {em.e(e.r)}, dt);")
+                    if isinstance(e.r, Var) and e.r.name + "@rate" in env:
+                        w(f"{pad}{xv} = gen_cnexp_rate({xv}, {em.e(e.l.l)}, {env[e.r.name + '@rate']}, dt);")
+                    else:
+                        w(f"{pad}{xv} = gen_cnexp_rate({xv}, {em.e(e.l.l)}, {em.e(recip(e.r))}, dt);")
                 else:
+                    # x' = a + b x: x -> xinf + (x - xinf) exp(b dt), xinf = -a/b, rate -b
                     a, b = linear_form(e, x)
-                    w(f"{pad}{{")
-                    w(f"{pad}    const R cb = {em.e(b)};")
-                    w(f"{pad}    const R ca = {em.e(a)};")
-                    w(f"{pad}    {xv} = {xv} + M::one_minus_exp_neg(-cb * dt) * (-M::dv(ca, cb) - {xv});")
-                    w(f"{pad}}}")
+                    rate = simplify(Un("-", b))
+                    w(f"{pad}{xv} = gen_cnexp_rate({xv}, {em.e(simplify(Bin('*', a, recip(rate))))}, "
+                      f"{em.e(rate)}, dt);")
             elif isinstance(s, If):
                 w(f"{pad}if ({em.e(s.cond)}) {{")
                 self._block(w, s.then, ind + 1, env, mode)
