@@ -417,7 +417,24 @@ struct ngpu_sim {
     // (nullptr: the ahead-of-time kernels, every node generic)
     const ngpu_jit::Module* jit = nullptr;
     ngpu_batch* batch = nullptr;  // the batch whose kernels this simulation's records follow
+    int s2_stage = 0;             // skeleton solved from shared memory (see sim_kernels.cuh)
 };
+
+// CTAs per SM that `smem` bytes of dynamic shared memory and W warps of 80
+// registers allow (228 KB per SM, 1 KB of it reserved per CTA).
+static int ctas_per_sm(size_t smem, int W) {
+    const int by_regs = 65536 / (kLanes * W * 80);
+    const int by_smem = (int)((228 * 1024) / (smem + 1024));
+    return std::max(1, std::min(std::min(by_regs, by_smem), 64 / W));
+}
+
+// Stage the skeleton in shared memory when that costs no occupancy.
+template <typename R>
+static int choose_s2_stage(int n_nodes, int n_seps, int W) {
+    if (W < 2 || n_seps < 2) return 0;
+    const size_t plain = SmemPlan<R>::bytes(n_nodes), staged = SmemPlan<R>::bytes(n_nodes, n_seps, 1);
+    return staged <= 227 * 1024 && ctas_per_sm(staged, W) >= ctas_per_sm(plain, W) ? 1 : 0;
+}
 
 template <typename R>
 static SimArgs<R> make_args(ngpu_sim* s) {
@@ -453,6 +470,7 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.seps = s->d_seps;
     A.n_seps = (int)s->part.seps.size();
     A.sepv = (R*)s->d_sepv;
+    A.s2_stage = s->s2_stage;
     return A;
 }
 
@@ -476,7 +494,7 @@ template <typename R>
 static cudaError_t launch_advance(ngpu_sim* s, int t0, int n, cudaStream_t st) {
     SimArgs<R> A = make_args<R>(s);
     const int threads = kLanes * s->n_warps;
-    const size_t smem = SmemPlan<R>::bytes(s->m->n);
+    const size_t smem = SmemPlan<R>::bytes(s->m->n, (int)s->part.seps.size(), s->s2_stage);
     cudaError_t e;
     if (s->jit) {
         const void* k = (const void*)s->jit->advance;
@@ -881,6 +899,8 @@ int ngpu_sim_create_ex(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t pr
     W = std::min(W, m->n);
     s->n_warps = W;
     s->part = make_partition(m, W);
+    s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W)
+                                         : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W);
     const int nj = s->part.n_jslots;
 #define ALLOC(field, type, bytes)                              \
     s->field = (type)dmalloc((bytes), &rc);                    \
@@ -1249,8 +1269,9 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
     for (ngpu_sim* s : b->sims) {
         W = std::max(W, s->n_warps);
         b->total_ctas += s->n_groups;
-        b->smem = std::max(b->smem, b->precision == NGPU_FP64 ? SmemPlan<double>::bytes(s->m->n)
-                                                             : SmemPlan<float>::bytes(s->m->n));
+        const int ns = (int)s->part.seps.size();
+        b->smem = std::max(b->smem, b->precision == NGPU_FP64 ? SmemPlan<double>::bytes(s->m->n, ns, s->s2_stage)
+                                                             : SmemPlan<float>::bytes(s->m->n, ns, s->s2_stage));
     }
     b->threads = kLanes * W;
     const GenSet* gs = gen_set(b->mechset);
@@ -1731,6 +1752,7 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     A.seps = (const DevSep*)(base + o_seps);
     A.n_seps = 1;
     A.sepv = (float*)(base + o_sepv);
+    A.s2_stage = 0;
 
     const size_t total = G * m->ptab_rows * L;
     const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);

@@ -130,6 +130,7 @@ struct SimArgs {
     const DevSep* seps;    // skeleton, ascending node index
     int n_seps;
     R* sepv;               // [n_seps][4] rows per group: A, B, excess, rhs terms of segment links
+    int s2_stage;          // skeleton solve from shared memory (SmemPlan)
 };
 
 // mk: the node's mechanism bits, a runtime value or a std::integral_constant
@@ -215,10 +216,18 @@ __device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A, int g) {
     return p;
 }
 
-// Shared memory: the node records.
+// Shared memory: the node records, then (s2_stage) the skeleton's staging
+// rows, [n_seps][32] each: two FP64 accumulators (excess, right-hand side)
+// and five R rows (coupling A / later c, coupling B / later r, axial term
+// e / later dV, V, Kahan term).
 template <typename R>
 struct SmemPlan {
-    static __host__ __device__ size_t bytes(int n_nodes) { return sizeof(NodeRec<R>) * (size_t)n_nodes; }
+    static __host__ __device__ size_t nodes(int n_nodes) {
+        return (sizeof(NodeRec<R>) * (size_t)n_nodes + 15) / 16 * 16;
+    }
+    static __host__ __device__ size_t bytes(int n_nodes, int n_seps = 0, int stage = 0) {
+        return nodes(n_nodes) + (stage ? (size_t)n_seps * 32 * (2 * sizeof(double) + 5 * sizeof(R)) : 0);
+    }
 };
 
 // Bulk prefetch of a run of rows into L2 (one instruction per contiguous block).
@@ -605,10 +614,91 @@ __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R
     }
 }
 
-// Per timestep (two barriers):
+// S2 through shared memory.  Every warp stages a share of the separators
+// at once (their accumulated rows, couplings and voltages: one memory round
+// trip for all of them), then warp 0 runs the skeleton's elimination and
+// back-substitution on the staged rows, where each separator's dependence
+// on its children goes through shared memory instead of a global
+// read-modify-write, and writes back dV and V.
+template <typename R>
+__device__ __forceinline__ void skeleton_staged(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
+                                                char* smem, bool rec_now, float* trace, int& bad) {
+    using M = Math<R>;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int S = A.n_seps;
+    double* acx = (double*)(smem + SmemPlan<R>::nodes(A.n_nodes));
+    double* acr = acx + (size_t)S * kLanes;
+    R* sA = (R*)(acr + (size_t)S * kLanes);
+    R* sB = sA + (size_t)S * kLanes;
+    R* sE = sB + (size_t)S * kLanes;
+    R* sV = sE + (size_t)S * kLanes;
+    R* sC = sV + (size_t)S * kLanes;
+    for (int k = w; k < S; k += nw) {
+        const DevSep sp = A.seps[k];
+        const NodeRec<R> s = nr[sp.node];
+        const R* row = G.scr + (size_t)sp.node * 3 * kLanes;
+        double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
+        const R* vo = G.vbuf + (size_t)sp.node * 2 * kLanes;
+        double x = (double)row[0] + ja[0], rh = (double)row[kLanes] + ja[kLanes];
+        R a = s.a, b = s.b, e = row[2 * kLanes];
+        if (sp.seg >= 0) {
+            const R* sv = G.sepv + (size_t)k * 4 * kLanes;
+            a = sv[0];
+            b = sv[kLanes];
+            x += (double)sv[2 * kLanes];
+            rh += (double)sv[3 * kLanes];
+            e = 0;  // the segment already folded this node's axial term in
+        }
+        ja[0] = 0.0;
+        ja[kLanes] = 0.0;
+        const size_t o = (size_t)k * kLanes + lane;
+        acx[o] = x;
+        acr[o] = rh;
+        sA[o] = a;
+        sB[o] = b;
+        sE[o] = e;
+        sV[o] = vo[0];
+        sC[o] = vo[kLanes];
+    }
+    __syncthreads();
+    if (w != 0) return;
+    for (int k = S - 1; k >= 0; --k) {
+        const size_t o = (size_t)k * kLanes + lane;
+        const R x = (R)acx[o], rh = (R)acr[o];
+        if (k == 0) {
+            sB[o] = M::dv(rh, x);
+            break;
+        }
+        const R Acp = sA[o], Bcp = sB[o], e_up = sE[o];
+        const R inv = M::rc(x - Acp);
+        const R rr = rh * inv, cc = Acp * inv;
+        sA[o] = cc;
+        sB[o] = rr;
+        const size_t op = (size_t)A.seps[k].par * kLanes + lane;
+        acx[op] += (double)(-Bcp * (x * inv));
+        acr[op] += (double)(e_up - Bcp * rr);
+    }
+    for (int k = 0; k < S; ++k) {
+        const DevSep sp = A.seps[k];
+        const NodeRec<R> s = nr[sp.node];
+        const size_t o = (size_t)k * kLanes + lane;
+        const R x = k == 0 ? sB[o] : sB[o] - sA[o] * sE[(size_t)sp.par * kLanes + lane];
+        sE[o] = x;
+        G.jx[(size_t)s.jslot * kLanes] = x;
+        R* vo = G.vbuf + (size_t)sp.node * 2 * kLanes;
+        R V = sV[o], vc = sC[o];
+        kahan_add(V, vc, x);
+        vo[0] = V;
+        vo[kLanes] = vc;
+        record(A, s, V, rec_now, trace);
+        if (k == 0 && !(fabs(V) < (R)1e6)) bad = 1;  // NaN / Inf / blow-up
+    }
+}
+
+// Per timestep (two barriers, three with a staged skeleton):
 //   S2  warp 0 solves the skeleton (the separators, a few dozen nodes) with
 //       the reduced couplings of the segments, and updates (and records)
-//       their V
+//       their V; staged (skeleton_staged), all warps first load its rows
 //   S3  all warps take items from a queue, largest first: an item's
 //       back-substitution pass, then its channel pass (channel update,
 //       next-step assembly and elimination node by node, above); each
@@ -640,7 +730,9 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
         float* trace;
         step_inputs(A, G, t, false, dt, dtn_inv, istim_amp, rec_now, trace);
         // S2: skeleton
-        if (w == 0) {
+        if (A.s2_stage) {
+            skeleton_staged<R>(A, G, nr, smem, rec_now, trace, bad);
+        } else if (w == 0) {
             using M = Math<R>;
             for (int k = A.n_seps - 1; k >= 0; --k) {
                 const DevSep sp = A.seps[k];
