@@ -198,6 +198,24 @@ int ngpu_sim_check(ngpu_sim *s, int32_t *n_bad, void *cuda_stream);
 int ngpu_sim_trace_device(ngpu_sim *s, const float **trace, int32_t *n_inst_padded);
 
 /*
+ * 20 spike / ISI / amplitude / AHP / voltage features per trace on the GPU,
+ * the vector of neurogpu_b200.features.FEATURES (spikes: upward crossings
+ * of `threshold` inside [stim_on, stim_off) ms; every feature defined
+ * without spikes).  Replaces the reference's per-trace extraction on a CPU
+ * pool (P/efel_ext.py:23-96 with eFEL, GUI/score_functions.py).
+ *   ngpu_trace_features  traces at v_dev[t * stride_trace + s * stride_sample]
+ *                        (device memory), out_dev [n_traces][20]
+ *   ngpu_sim_features    from a simulation's own trace buffer, recording site
+ *                        `site`, without copying it: out_dev [n_sets][n_stim][20];
+ *                        dt is the sample spacing (step dt x rec_every)
+ */
+int ngpu_trace_features(const float *v_dev, int64_t stride_trace, int64_t stride_sample, int32_t n_traces,
+                        int32_t n_samples, double dt, double stim_on, double stim_off, float threshold,
+                        float *out_dev, void *cuda_stream);
+int ngpu_sim_features(ngpu_sim *s, int32_t site, double dt, double stim_on, double stim_off, float threshold,
+                      float *out_dev, void *cuda_stream);
+
+/*
  * Runtime specialisation of the advance kernel.  At initialisation an FP32
  * simulation (or, at creation, an FP32 batch) gets a kernel compiled with
  * NVRTC for its model's mechanism masks (up to 16): nodes with those masks

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/ngpu.h"
+#include "features.cuh"
 #include "gemm_tc.cuh"
 #include "ngpu_jit.h"
 #include "sim_kernels.cuh"
@@ -1418,6 +1419,72 @@ int ngpu_batch_run_graph(ngpu_batch* b, float v_init, int32_t nt, int32_t chunk,
 }
 
 int ngpu_sim_n_samples(const ngpu_sim* s) { return s ? s->n_samples : 0; }
+
+// Window bounds as features.py computes them (Python's round: half to even).
+static int feature_args(int32_t n_samples, double dt, double stim_on, double stim_off, FeatureArgs* a) {
+    if (n_samples < 2 || !(dt > 0) || !std::isfinite(dt) || !std::isfinite(stim_on) || !std::isfinite(stim_off))
+        return fail(NGPU_E_INVALID, "features: need >= 2 samples, dt > 0 and finite window bounds");
+    const int T = n_samples;
+    auto rnd = [](double x) { return (int)std::nearbyint(x); };
+    a->i_on = std::max(0, rnd(stim_on / dt));
+    a->i_off = std::min(T, rnd(stim_off / dt));
+    if (a->i_off - a->i_on < 2) return fail(NGPU_E_INVALID, "features: the stimulus window holds < 2 samples");
+    a->dur = (float)((a->i_off - a->i_on) * dt);
+    auto win = [&](double lo, double hi, int* ia, int* ib) {
+        const int r = rnd(lo / dt);
+        *ia = std::max(0, r);
+        *ib = std::min(T, std::max(r + 1, rnd(hi / dt)));
+    };
+    win(std::max(0.0, stim_on - 10.0), stim_on, &a->vb_lo, &a->vb_hi);
+    win(std::max(stim_on, stim_off - 50.0), stim_off, &a->ss_lo, &a->ss_hi);
+    if (stim_off + 10.0 < T * dt) win(stim_off + 10.0, T * dt, &a->af_lo, &a->af_hi);
+    else a->af_lo = a->af_hi = -1;
+    a->dt = (float)dt;
+    a->n_samples = T;
+    return NGPU_OK;
+}
+
+static int launch_features(FeatureArgs a, cudaStream_t st) {
+    if (a.n_traces < 1) return NGPU_OK;
+    k_trace_features<<<(a.n_traces + 127) / 128, 128, 0, st>>>(a);
+    g_launches++;
+    NGPU_CUDA(cudaGetLastError());
+    return NGPU_OK;
+}
+
+int ngpu_trace_features(const float* v_dev, int64_t stride_trace, int64_t stride_sample, int32_t n_traces,
+                        int32_t n_samples, double dt, double stim_on, double stim_off, float threshold, float* out_dev,
+                        void* cuda_stream) {
+    if (!v_dev || !out_dev) return fail(NGPU_E_INVALID, "features: null pointer");
+    if (n_traces < 0 || stride_trace < 0 || stride_sample < 1) return fail(NGPU_E_INVALID, "features: bad strides");
+    FeatureArgs a;
+    const int rc = feature_args(n_samples, dt, stim_on, stim_off, &a);
+    if (rc != NGPU_OK) return rc;
+    a.v = v_dev;
+    a.stride_trace = stride_trace;
+    a.stride_sample = stride_sample;
+    a.n_traces = n_traces;
+    a.threshold = threshold;
+    a.out = out_dev;
+    return launch_features(a, (cudaStream_t)cuda_stream);
+}
+
+int ngpu_sim_features(ngpu_sim* s, int32_t site, double dt, double stim_on, double stim_off, float threshold,
+                      float* out_dev, void* cuda_stream) {
+    if (!s || !out_dev) return fail(NGPU_E_INVALID, "null argument");
+    if (!s->initialized || !s->d_trace) return fail(NGPU_E_STATE, "run the simulation first");
+    if (site < 0 || site >= (int)s->rec_cols.size()) return fail(NGPU_E_INVALID, "recording site out of range");
+    FeatureArgs a;
+    const int rc = feature_args(s->n_samples, dt, stim_on, stim_off, &a);
+    if (rc != NGPU_OK) return rc;
+    a.v = s->d_trace + (size_t)s->rec_cols[site] * s->n_pad;   // [sample][column][instance]
+    a.stride_trace = 1;
+    a.stride_sample = (int64_t)s->n_rec_unique * s->n_pad;
+    a.n_traces = s->n_inst;
+    a.threshold = threshold;
+    a.out = out_dev;
+    return launch_features(a, (cudaStream_t)cuda_stream);
+}
 
 int ngpu_sim_classes(const ngpu_sim* s, int32_t* n_classes) {
     if (!s || !n_classes) return fail(NGPU_E_INVALID, "null argument");

@@ -87,3 +87,22 @@ def extract(v: torch.Tensor, dt: float, stim_on: float, stim_off: float) -> torc
     return torch.stack([n, first_lat, mean_isi, isi_cv, first_isi, last_isi, adaptation, pk_mean, pk_std, ahp_mean,
                         amp, t_half, vb, ss, after, v.max(1).values, w.min(1).values, w.mean(1), w.std(1),
                         last_t], 1)
+
+
+def extract_device(v: torch.Tensor, dt: float, stim_on: float, stim_off: float,
+                   threshold: float = THRESHOLD) -> torch.Tensor:
+    """extract() by the library's CUDA kernel (ngpu_trace_features): v [B, T]
+    float32 on the GPU, any strides; one thread per trace, both passes over
+    the trace in one launch."""
+    import ctypes as C
+
+    from . import _ffi
+    if not v.is_cuda or v.dtype != torch.float32 or v.dim() != 2:
+        raise ValueError("v must be a float32 CUDA tensor [B, T]")
+    B, T = v.shape
+    out = torch.empty((B, N_FEATURES), dtype=torch.float32, device=v.device)
+    stream = torch.cuda.current_stream(v.device).cuda_stream
+    _ffi.check("ngpu_trace_features", _ffi.lib().ngpu_trace_features(
+        C.c_void_p(v.data_ptr()), v.stride(0), v.stride(1), B, T, float(dt), float(stim_on), float(stim_off),
+        float(threshold), C.c_void_p(out.data_ptr()), C.c_void_p(stream)))
+    return out

@@ -178,6 +178,19 @@ class Simulator:
         _ffi.check("ngpu_sim_get_trace", _ffi.lib().ngpu_sim_get_trace(
             self._h, C.c_void_p(dev_ptr), 1, _stream_ptr(stream)))
 
+    def features(self, dt: float, stim_on: float, stim_off: float, site: int = 0, threshold: float = -20.0,
+                 stream=None):
+        """The 20 features of neurogpu_b200.features of every instance's trace
+        at recording site `site`, computed where the trace lies
+        (ngpu_sim_features): a float32 CUDA tensor [n_sets, n_stim, 20].
+        dt: the sample spacing (step dt x rec_every)."""
+        import torch
+        out = torch.empty((self.n_sets, self.n_stim, 20), dtype=torch.float32, device="cuda")
+        _ffi.check("ngpu_sim_features", _ffi.lib().ngpu_sim_features(
+            self._h, int(site), float(dt), float(stim_on), float(stim_off), float(threshold),
+            C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
     def classes(self) -> int:
         """Mechanism masks compiled into the kernel that runs this simulation
         (0: the ahead-of-time kernel, generic channel code); after init()."""
