@@ -146,6 +146,140 @@ def ancestor_table(ks: np.ndarray) -> np.ndarray:
     return tab[:, :n]
 
 
+def _starts_ends(groups: list) -> tuple[np.ndarray, np.ndarray]:
+    """0-based start / end position of each group in their concatenation."""
+    lens = np.array([len(g) for g in groups], dtype=np.int64)
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]]) if lens.size else lens
+    return starts, starts + lens - 1
+
+
+def level_schedule(ks: np.ndarray) -> dict:
+    """The reference's level schedule of its branched solve over the reversed
+    1-based parent field Ks (P/make_tree_from_parent_vec.py:17-59): the
+    junction fathers and, per father, the positions that call it; the chain
+    segments between calls (SegStartI / SegEndI, 1-based); each segment's
+    elimination level and each father's level.  Index arithmetic as there,
+    including where it mixes 1-based values and 0-based positions."""
+    ks = np.asarray(ks, dtype=np.int64)
+    n = ks.size
+    pos = np.arange(1, n + 1)
+    fathers = np.unique(ks[(ks != pos) & (ks > 0)])
+    related = [np.nonzero(ks == fa)[0] for fa in fathers]
+    call = np.nonzero(np.isin(ks, fathers))[0] + 1
+    r_fathers = np.zeros(int(fathers.max()) if fathers.size else 0)
+    r_fathers[fathers - 1] = np.arange(1, fathers.size + 1)
+    seg_start = np.concatenate([[2], call + 1])
+    seg_end = np.concatenate([call - 1, [n - 1]])
+    level = np.zeros(seg_start.size, dtype=np.int64)
+    level[np.isin(seg_start - 1, fathers)] = 1
+    for lv in range(1, 51):
+        calls_to = ks[seg_end[level == lv]]
+        level[np.isin(seg_start - 1, calls_to)] = lv + 1
+    flevel = np.ones(fathers.size, dtype=np.int64)
+    for lv in range(1, int(level.max()) + 1):
+        calls_to = ks[seg_end[level == lv]]
+        # a (1, m) index array of positions minus one, as the reference forms it
+        sel = np.subtract(np.where(calls_to <= fathers.max()), 1)
+        which = r_fathers[np.subtract(calls_to[sel], 1)][0]
+        flevel[which.astype(np.int64) - 1] = lv + 1
+    seg_end[-1] = n
+    rel_starts, rel_ends = _starts_ends(related)
+    return {"fathers": fathers, "related": related, "rel_starts": rel_starts, "rel_ends": rel_ends,
+            "rel_vec": np.concatenate(related) if related else np.zeros(0, np.int64), "call": call,
+            "seg_start": seg_start, "seg_end": seg_end, "level": level, "flevel": flevel,
+            "depth": int(level.max())}
+
+
+def _by_level32(levels: np.ndarray, targets) -> tuple[np.ndarray, list]:
+    """Rows of 32 (1-based) indices per level, the last index repeated to fill
+    a row; the 1-based row numbers of each level."""
+    rows, related = [], []
+    for lv in targets:
+        comps = np.nonzero(levels == lv)[0] + 1
+        k = int(np.ceil(comps.size / 32.0))
+        padded = np.full(k * 32, comps[-1])
+        padded[:comps.size] = comps
+        first = len(rows) + 1
+        rows += list(padded.reshape(k, 32))
+        related.append(list(range(first, len(rows) + 1)))
+    return (np.array(rows) if rows else np.zeros((0, 32))), related
+
+
+def basic_const_fields(ks: np.ndarray, e: np.ndarray, f: np.ndarray, seg_to_comp: np.ndarray, cms: np.ndarray,
+                       bool_model: np.ndarray, n_comps: int) -> dict[str, np.ndarray]:
+    """All 32 fields of BasicConstSegP.csv from the model's reversed parent
+    field Ks, coefficients e / f (reversed B / A columns of NEURON's matrix),
+    node-to-compartment map, capacitances and mechanism flags [n_models][N]:
+    the auxiliary data the reference's solver reads
+    (P/create_auxilliary_data_3.py:22-271, with
+    P/make_tree_from_parent_vec.py); uint16 fields wrap as there."""
+    ks = np.asarray(ks, dtype=np.int64)
+    n = ks.size
+    parent = parent_from_ks(ks)
+    sons = son_no_vec(parent)
+    if sons.max() > 2:  # the reference's solver allows two children per node (create_auxilliary_data_3.py:83)
+        raise ValueError("a node has more than two children: the reference's format cannot hold the tree")
+    fidx = ancestor_table(ks)
+    sch = level_schedule(ks)
+    depth = sch["depth"]
+    level, flevel = sch["level"], sch["flevel"]
+    last_level_i = int(np.nonzero(level == level.max())[0][0]) + 1
+    ksb = np.concatenate([ks, [sch["seg_end"][last_level_i - 1]]])
+    comp32, lrel = _by_level32(level, range(depth + 1))
+    fcomp32, flrel = _by_level32(flevel, range(1, depth + 1)) if depth > 0 else (np.zeros((0, 32)), [])
+    ls, le = _starts_ends(lrel)
+    fs, fe = _starts_ends(flrel) if depth > 0 else (np.zeros(0), np.zeros(0))
+    u16 = lambda x: np.asarray(x, dtype=np.int64).astype(np.uint16).astype(np.float64)
+    bm = np.asarray(bool_model, dtype=np.float64)
+    return {
+        "N": np.array([n], dtype=np.float64), "NComps": np.array([n_comps], dtype=np.float64),
+        "e": np.asarray(e, dtype=np.float64), "f": np.asarray(f, dtype=np.float64), "Ks": u16(ks),
+        "SegToComp": u16(seg_to_comp), "Cms": np.asarray(cms, dtype=np.float64),
+        "NModels": np.array([bm.shape[0]], dtype=np.float64), "boolModel": bm.reshape(-1),
+        "SonNoVec": u16(sons), "Depth": np.array([depth], dtype=np.float64),
+        "LognDepth": np.array([fidx.shape[0]], dtype=np.float64),
+        "nFathers": np.array([sch["fathers"].size], dtype=np.float64),
+        "nCallForFather": np.array([sch["call"].size], dtype=np.float64),
+        "RelStarts": u16(sch["rel_starts"] + 1), "RelEnds": u16(sch["rel_ends"] + 1),
+        "RelVec": u16(sch["rel_vec"] + 1), "SegStartI": u16(sch["seg_start"]), "SegEndI": u16(sch["seg_end"]),
+        "Fathers": u16(sch["fathers"]), "FIdxs": u16(fidx.reshape(-1)),
+        "CompDepth": np.array([comp32.shape[0]], dtype=np.float64),
+        "CompFDepth": np.array([fcomp32.shape[0]], dtype=np.float64),
+        "CompByLevel32": u16(comp32.reshape(-1)), "CompByFLevel32": u16(fcomp32.reshape(-1)),
+        "nLRel": np.array([len(lrel)], dtype=np.float64), "LRelStarts": u16(ls), "LRelEnds": u16(le),
+        "nFLRel": np.array([len(flrel)], dtype=np.float64), "FLRelStarts": u16(fs), "FLRelEnds": u16(fe),
+        "KsB": u16(ksb - 1),
+    }
+
+
+def format_basic_const_segp(fields: dict[str, np.ndarray]) -> str:
+    """The file text: one line per field, every value as %.9f followed by a
+    comma (P/create_auxilliary_data_3.py:262-271)."""
+    return "".join("".join(f"{x:.9f}," for x in np.asarray(fields[k]).reshape(-1)) + "\n" for k in BCS_FIELDS)
+
+
+def ks_from_parent(parent: np.ndarray) -> np.ndarray:
+    """Inverse of parent_from_ks: the reversed 1-based parent field."""
+    n = parent.size
+    ks = np.zeros(n, dtype=np.int64)
+    for j in range(1, n):
+        ks[j] = n - int(parent[n - j])
+    return ks
+
+
+def write_basic_const_segp(path: str | os.PathLike, cell: CellModel, bool_model: np.ndarray | None = None) -> None:
+    """BasicConstSegP.csv of a CellModel (node order: Hines, root 0), for the
+    reference's simulator or this library's command line.  bool_model: the
+    file's mechanism rows [n_models][N] (default: the cell's mechanism mask)."""
+    n = cell.n_nodes
+    ks = ks_from_parent(np.asarray(cell.parent))
+    f = np.asarray(cell.a, dtype=np.float64)[::-1].copy()
+    e = np.asarray(cell.b, dtype=np.float64)[::-1].copy()
+    bm = np.asarray(cell.mech_mask if bool_model is None else bool_model, dtype=np.float64)
+    fields = basic_const_fields(ks, e, f, np.asarray(cell.section), np.asarray(cell.cm), bm, cell.n_sections)
+    Path(path).write_text(format_basic_const_segp(fields))
+
+
 @dataclass
 class ReferenceModel:
     """A reference Data/ directory turned into the library's inputs."""
@@ -294,6 +428,36 @@ def read_data_dir(data: str | os.PathLike, stim_index: int | None = None,
         raise ValueError(f"stimulus location {loc + 1} outside the {n_nodes}-node tree")
     return ReferenceModel(cell, params, amps, dts, loc, area, rec, v_init,
                           raw={"basic_const": bc, "file_params": fparams})
+
+
+def write_data_dir(data: str | os.PathLike, cell: CellModel, params: np.ndarray, amps: np.ndarray,
+                   dts: np.ndarray, stim_node: int, stim_area: float, rec_nodes, v_init: float, dt: float,
+                   bool_model: np.ndarray | None = None, stim_index: int | None = None,
+                   param_index=None) -> None:
+    """A reference Data/ directory for a model: BasicConstSegP.csv,
+    AllParams.csv, Sim.csv, Stim_meta.csv, Stim_raw[<stim_index>].csv and
+    times.csv, in the formats read_data_dir (and the reference's reader,
+    src/MainC.cu:335-551, src/Util.cu) reads.  params [n_sets, n_params,
+    n_sections] in the library mechanism set's order; param_index: the
+    library parameter index of each parameter the reference build lists
+    (default: all, in order; the inverse of map_params); amps [n_stim, nt]
+    nA; dts [nt] ms.  AllParams.csv holds 6 significant digits, as the
+    reference's writer prints them."""
+    d = Path(data)
+    d.mkdir(parents=True, exist_ok=True)
+    write_basic_const_segp(d / "BasicConstSegP.csv", cell, bool_model)
+    params = np.asarray(params, dtype=np.float32)
+    if param_index is not None:
+        params = params[:, np.asarray(param_index, dtype=np.int64), :]
+    write_allparams_csv(d / "AllParams.csv", params)
+    rec = [int(r) for r in np.asarray(rec_nodes).reshape(-1)]
+    (d / "Sim.csv").write_text(f"{v_init:.5f},\n{dt:.5f},\n{len(rec):.5f},\n" +
+                              "".join(f"{r:.5f}," for r in rec) + "\n")
+    amps = np.asarray(amps, dtype=np.float32)
+    (d / "Stim_meta.csv").write_text(f"{amps.shape[0]}\n{amps.shape[1]}\n0\n{stim_node + 1}\n{stim_area!r}\n")
+    raw = "Stim_raw.csv" if stim_index is None else f"Stim_raw{stim_index}.csv"
+    (d / raw).write_text("".join("".join(f"{x:.6f}," for x in row) + "\n" for row in amps))
+    (d / "times.csv").write_text("".join(f"{x:.5f}," for x in np.asarray(dts, dtype=np.float64)) + "\n")
 
 
 def write_vhot(path: str | os.PathLike, traces: np.ndarray) -> None:
