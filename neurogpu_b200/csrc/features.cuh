@@ -38,9 +38,26 @@ struct FeatureArgs {
     float* out;              // [n_traces][20]
 };
 
+// Samples are read kChunk at a time into registers, all loads of a chunk
+// issued before any is used: kChunk rows in flight per thread.
+constexpr int kChunk = 16;
+
+template <typename F>
+__device__ __forceinline__ void for_samples(const float* v, int64_t st, int lo, int hi, F&& f) {
+    for (int j0 = lo; j0 < hi; j0 += kChunk) {
+        float x[kChunk];
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u)
+            if (j0 + u < hi) x[u] = v[(int64_t)(j0 + u) * st];
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u)
+            if (j0 + u < hi) f(j0 + u, x[u]);
+    }
+}
+
 __device__ __forceinline__ double win_mean(const float* v, int64_t st, int lo, int hi) {
     double s = 0;
-    for (int i = lo; i < hi; ++i) s += (double)v[(int64_t)i * st];
+    for_samples(v, st, lo, hi, [&](int, float x) { s += (double)x; });
     return hi > lo ? s / (double)(hi - lo) : 0.0;
 }
 
@@ -54,8 +71,8 @@ __global__ void __launch_bounds__(128) k_trace_features(const FeatureArgs a) {
     const float dur = a.dur;
     // pass 1
     float vmax = -INFINITY;
-    for (int s = 0; s < a.i_on; ++s) vmax = fmaxf(vmax, v[(int64_t)s * st]);
-    for (int s = a.i_off; s < a.n_samples; ++s) vmax = fmaxf(vmax, v[(int64_t)s * st]);
+    for_samples(v, st, 0, a.i_on, [&](int, float x) { vmax = fmaxf(vmax, x); });
+    for_samples(v, st, a.i_off, a.n_samples, [&](int, float x) { vmax = fmaxf(vmax, x); });
     float wmin = INFINITY, wmax = -INFINITY;
     double wsum = 0, wsq = 0;
     int n = 0, first_idx = -1;
@@ -64,8 +81,7 @@ __global__ void __launch_bounds__(128) k_trace_features(const FeatureArgs a) {
     float seg_max = -INFINITY, seg_min = INFINITY;
     double pk_sum = 0, pk_sq = 0, tr_sum = 0;
     float prev = 0;
-    for (int j = 0; j < W; ++j) {
-        const float x = v[(int64_t)(a.i_on + j) * st];
+    for_samples(v + (int64_t)a.i_on * st, st, 0, W, [&](int j, float x) {
         vmax = fmaxf(vmax, x);
         wmin = fminf(wmin, x);
         wmax = fmaxf(wmax, x);
@@ -96,7 +112,7 @@ __global__ void __launch_bounds__(128) k_trace_features(const FeatureArgs a) {
             seg_min = fminf(seg_min, x);
         }
         prev = x;
-    }
+    });
     if (n > 0) {
         pk_sum += seg_max;
         pk_sq += (double)seg_max * seg_max;
@@ -117,8 +133,7 @@ __global__ void __launch_bounds__(128) k_trace_features(const FeatureArgs a) {
     const float half = (float)(0.5 * (pk_mean + ahp));
     // pass 2: samples at or above half amplitude after the first crossing
     int above = 0;
-    if (has1)
-        for (int j = first_idx; j < W; ++j) above += v[(int64_t)(a.i_on + j) * st] >= half ? 1 : 0;
+    if (has1) for_samples(v + (int64_t)a.i_on * st, st, first_idx, W, [&](int, float x) { above += x >= half ? 1 : 0; });
     const double wmean = W > 0 ? wsum / W : 0.0;
     const double wstd = W > 1 ? sqrt(fmax(0.0, (wsq - (double)W * wmean * wmean) / (double)(W - 1))) : 0.0;
     float* o = a.out + (int64_t)t * kNFeatures;
