@@ -15,9 +15,12 @@ which the library compiles at run time into the advance kernel
 
 Supported NMODL: NEURON (SUFFIX, USEION ... READ/WRITE, NONSPECIFIC_CURRENT,
 RANGE / GLOBAL), PARAMETER, CONSTANT, ASSIGNED, STATE, UNITS (FARADAY, R,
-PI), INITIAL, BREAKPOINT with SOLVE ... METHOD cnexp, DERIVATIVE, PROCEDURE,
-FUNCTION, LOCAL, if / else, UNITSON / UNITSOFF, TABLE (ignored: rates are
-computed directly), comments.  KINETIC, VERBATIM, NET_RECEIVE and other
+PI), INITIAL, BREAKPOINT with SOLVE ... METHOD cnexp (DERIVATIVE) or METHOD
+sparse (KINETIC), DERIVATIVE, KINETIC with first-order reactions
+(~ a <-> b (kf, kb)), sources (~ a << (f)) and CONSERVE, SOLVE ...
+STEADYSTATE sparse in INITIAL, PROCEDURE, FUNCTION, LOCAL, if / else,
+UNITSON / UNITSOFF, TABLE (ignored: rates are computed directly), comments.
+VERBATIM, NET_RECEIVE, point processes, higher-order reactions and other
 integration methods raise NmodlError.
 
 Semantics, as NEURON's fixed-step method and the reference's simulator
@@ -38,7 +41,12 @@ Semantics, as NEURON's fixed-step method and the reference's simulator
   * an ion current a mechanism READs (CaDynamics' ica) is the node's total
     of that current from the previous step's current phase, kept in an
     extra state row after the mechanism's STATE rows;
-  * PROCEDURE / FUNCTION arguments, and v inside them, are local copies.
+  * PROCEDURE / FUNCTION arguments, and v inside them, are local copies;
+  * KINETIC: one backward-Euler step of the scheme's linear system (what
+    NEURON's sparse method computes for first-order reactions), solved
+    exactly by straight-line elimination; the reference's code generator
+    instead runs three relaxation sweeps (P/kinetic_template.txt,
+    Cubackwards_euler).
 Numerics: 1 - exp(E) and exp(E) - 1 are emitted as expm1 with a series
 below |E| = 1e-2, so the removable singularities of alpha/beta rates keep
 FP32 precision next to the singular voltage; divisions and exponentials
@@ -173,7 +181,30 @@ class CallStmt:
 @dataclass
 class Solve:
     block: str
-    method: str
+    method: str | None
+    steady: bool = False      # SOLVE ... STEADYSTATE (in INITIAL)
+
+
+@dataclass
+class Reaction:
+    """~ a <-> b (kf, kb): first order both ways."""
+    a: str
+    b: str
+    kf: object
+    kb: object
+
+
+@dataclass
+class Flux:
+    """~ a << (f): a source term of a's equation."""
+    a: str
+    f: object
+
+
+@dataclass
+class Conserve:
+    lhs: object
+    rhs: object
 
 
 _BUILTIN_FUNCS = {"exp", "log", "log10", "fabs", "sqrt", "pow", "sin", "cos", "tanh", "fmin", "fmax"}
@@ -356,11 +387,17 @@ class Parser:
             return None
         if v == "SOLVE":
             block = self.ident()
-            method = "cnexp"
-            if self.peek().val == "METHOD":
-                self.next()
+            method, steady = None, False
+            if self.peek().val in ("METHOD", "STEADYSTATE"):
+                steady = self.next().val == "STEADYSTATE"
                 method = self.ident()
-            return Solve(block, method)
+            return Solve(block, method, steady)
+        if v == "~":
+            return self.reaction(tok.line)
+        if v == "CONSERVE":
+            lhs = self.expr()
+            self.expect("=")
+            return Conserve(lhs, self.expr())
         if v == "if":
             self.expect("(")
             cond = self.expr()
@@ -379,7 +416,7 @@ class Parser:
             else:
                 self.i = save
             return If(cond, then, other)
-        if v in ("VERBATIM", "KINETIC", "NET_RECEIVE", "LINEAR", "NONLINEAR", "CONSERVE", "COMPARTMENT",
+        if v in ("VERBATIM", "KINETIC", "NET_RECEIVE", "LINEAR", "NONLINEAR", "COMPARTMENT",
                  "FROM", "WHILE", "FOR_NETCONS"):
             raise NmodlError(f"line {tok.line}: {v} is not supported")
         if tok.kind == "id":
@@ -402,6 +439,44 @@ class Parser:
                 return CallStmt(v, tuple(args))
         raise NmodlError(f"line {tok.line}: cannot read statement at {v!r}")
 
+    def species(self, line: int) -> str:
+        """One side of a reaction: a single STATE with stoichiometry 1."""
+        names = []
+        while True:
+            if self.peek().kind == "num":
+                raise NmodlError(f"line {line}: stoichiometric coefficients are not supported (first-order "
+                                 "reactions only)")
+            names.append(self.ident())
+            if self.peek().val == "[":
+                raise NmodlError(f"line {line}: array states are not supported")
+            if self.peek().val != "+":
+                break
+            self.next()
+        if len(names) != 1:
+            raise NmodlError(f"line {line}: {' + '.join(names)}: first-order reactions only")
+        return names[0]
+
+    def reaction(self, line: int):
+        a = self.species(line)
+        t = self.next()
+        if t.val == "<" and self.peek().val == "-" and self.peek(1).val == ">":
+            self.next()
+            self.next()
+            b = self.species(line)
+            self.expect("(")
+            kf = self.expr()
+            self.expect(",")
+            kb = self.expr()
+            self.expect(")")
+            return Reaction(a, b, kf, kb)
+        if t.val == "<" and self.peek().val == "<":
+            self.next()
+            self.expect("(")
+            f = self.expr()
+            self.expect(")")
+            return Flux(a, f)
+        raise NmodlError(f"line {line}: expected <-> or << after ~ {a}")
+
 
 # ---------------------------------------------------------------- mechanism
 @dataclass
@@ -422,6 +497,7 @@ class Mechanism:
     unit_consts: dict = field(default_factory=dict)
     breakpoint: list = field(default_factory=list)
     derivatives: dict = field(default_factory=dict)
+    kinetics: dict = field(default_factory=dict)      # KINETIC blocks: name -> stmts
     initial: list = field(default_factory=list)
     procedures: dict = field(default_factory=dict)    # name -> (args, stmts)
     functions: dict = field(default_factory=dict)
@@ -582,6 +658,9 @@ def parse_mod(text: str, name_hint: str = "") -> Mechanism:
         elif v == "DERIVATIVE":
             dname = p.ident()
             mech.derivatives[dname] = p.stmts()
+        elif v == "KINETIC":
+            kname = p.ident()
+            mech.kinetics[kname] = p.stmts()
         elif v in ("PROCEDURE", "FUNCTION"):
             name = p.ident()
             p.expect("(")
@@ -595,7 +674,7 @@ def parse_mod(text: str, name_hint: str = "") -> Mechanism:
             p.skip_units()
             body = p.stmts()
             (mech.procedures if v == "PROCEDURE" else mech.functions)[name] = (args, body)
-        elif v in ("KINETIC", "NET_RECEIVE", "VERBATIM", "LINEAR", "NONLINEAR", "DISCRETE", "PARTIAL"):
+        elif v in ("NET_RECEIVE", "VERBATIM", "LINEAR", "NONLINEAR", "DISCRETE", "PARTIAL"):
             raise NmodlError(f"line {tok.line}: {v} blocks are not supported")
         else:
             raise NmodlError(f"line {tok.line}: unexpected {v!r} at top level")
@@ -614,6 +693,26 @@ BREAKPOINT { i = g*(v - e) }
 
 
 # ------------------------------------------------------- symbolic algebra
+def _var_order(e) -> list:
+    """Names in an expression, left to right, first appearance."""
+    out = []
+
+    def walk(x):
+        if isinstance(x, Var):
+            if x.name not in out:
+                out.append(x.name)
+        elif isinstance(x, Un):
+            walk(x.e)
+        elif isinstance(x, Bin):
+            walk(x.l)
+            walk(x.r)
+        elif isinstance(x, Call):
+            for a in x.args:
+                walk(a)
+    walk(e)
+    return out
+
+
 def free_vars(e) -> set:
     if isinstance(e, Var):
         return {e.name}
@@ -1112,7 +1211,13 @@ def _emit_set(mechs, mech_params, params, celsius, ktf, reversal, cao, constants
         w("        } else {")
         solve = [s for s in m.breakpoint if isinstance(s, Solve)]
         for sv in solve:
-            if sv.method != "cnexp":
+            if sv.block in m.kinetics:
+                if sv.method not in (None, "sparse"):
+                    raise NmodlError(f"{m.suffix}: METHOD {sv.method} is not supported for KINETIC {sv.block} "
+                                     "(sparse only)")
+                body.kinetic(w, sv.block, 3, dict(body.env), steady=False)
+                continue
+            if sv.method not in (None, "cnexp"):
                 raise NmodlError(f"{m.suffix}: METHOD {sv.method} is not supported (cnexp only)")
             if sv.block not in m.derivatives:
                 raise NmodlError(f"{m.suffix}: no DERIVATIVE {sv.block}")
@@ -1376,9 +1481,158 @@ class _MechBody:
                 else:
                     raise NmodlError(f"{self.m.suffix}: call of unknown {s.name}()")
             elif isinstance(s, Solve):
+                if s.steady:
+                    if s.block not in self.m.kinetics or s.method not in (None, "sparse"):
+                        raise NmodlError(f"{self.m.suffix}: SOLVE {s.block} STEADYSTATE {s.method}: only KINETIC "
+                                         "blocks with sparse")
+                    self.kinetic(w, s.block, ind, env, steady=True)
                 continue
             else:
                 raise NmodlError(f"{self.m.suffix}: unsupported statement {s!r}")
+
+    # a steady state is backward Euler over this step (ms): every rate times
+    # the step dwarfs 1, so the solution is the scheme's fixed point
+    STEADY_DT = 1e9
+
+    def kinetic(self, w, name, ind, env, steady):
+        """A first-order KINETIC scheme advanced by one backward-Euler step,
+        (I - dt Q) x' = x + dt s (Q: the rate matrix, s: the << sources), the
+        solve NEURON's sparse method performs for a linear scheme.  CONSERVE
+        replaces the equation of the last state it names by the conservation
+        law.  The system is eliminated without pivoting, in state order with
+        the conserved state last: I - dt Q is diagonally dominant by columns
+        (each state's outflow appears on its diagonal and as inflow in the
+        other rows of its column), so every pivot before the last is at least
+        1, and only structural non-zeros and their fill-in are emitted.
+        steady (SOLVE ... STEADYSTATE in INITIAL): the same step with
+        dt = STEADY_DT in FP64."""
+        m = self.m
+        body = m.kinetics[name]
+        pad = "    " * ind
+        T = "double" if steady else "R"
+        dts = "(double)" + repr(self.STEADY_DT) if steady else "dt"
+        env = dict(env)
+        plain = [st for st in body if not isinstance(st, (Reaction, Flux, Conserve))]
+        locs = self._locals(plain, env)
+        w(f"{pad}{{  // KINETIC {name}{' (steady state)' if steady else ''}")
+        ind += 1
+        pad = "    " * ind
+        for l in locs:
+            env[l] = f"l_{l}"
+            w(f"{pad}R l_{l} = 0;")
+        states = []
+        out_rates, in_rates, sources = {}, {}, {}
+        conserve = None
+        em = self._em(env)
+        nr = 0
+
+        def use(x):
+            if x not in m.states:
+                raise NmodlError(f"{m.suffix}: {x} in KINETIC {name} is not a STATE")
+            if x not in states:
+                states.append(x)
+        for st in body:
+            if isinstance(st, Reaction):
+                use(st.a)
+                use(st.b)
+                kf, kb = f"kn{self.k}_f{nr}", f"kn{self.k}_b{nr}"
+                nr += 1
+                w(f"{pad}const R {kf} = {em.e(st.kf)};")
+                w(f"{pad}const R {kb} = {em.e(st.kb)};")
+                out_rates.setdefault(st.a, []).append(kf)
+                in_rates.setdefault((st.b, st.a), []).append(kf)
+                out_rates.setdefault(st.b, []).append(kb)
+                in_rates.setdefault((st.a, st.b), []).append(kb)
+            elif isinstance(st, Flux):
+                use(st.a)
+                fl = f"kn{self.k}_s{nr}"
+                nr += 1
+                w(f"{pad}const R {fl} = {em.e(st.f)};")
+                sources.setdefault(st.a, []).append(fl)
+            elif isinstance(st, Conserve):
+                if conserve is not None:
+                    raise NmodlError(f"{m.suffix}: more than one CONSERVE in KINETIC {name}")
+                conserve = st
+            else:
+                self._block(w, [st], ind, env, mode="proc")
+        if not states:
+            raise NmodlError(f"{m.suffix}: KINETIC {name} has no reactions")
+        order = [x for x in m.states if x in states]
+        cons_row = {}
+        if conserve is not None:
+            named = [x for x in _var_order(conserve.lhs) if x in m.states]
+            if not named:
+                raise NmodlError(f"{m.suffix}: CONSERVE names no STATE")
+            for x in named:
+                use(x)
+            order = [x for x in m.states if x in states]
+            for x in order:
+                c = simplify(diff(conserve.lhs, x))
+                if not isinstance(c, Num):
+                    raise NmodlError(f"{m.suffix}: CONSERVE must be linear in the states with constant coefficients")
+                if c.v != 0:
+                    cons_row[x] = c.v
+            rest = simplify(conserve.lhs)
+            for x in order:
+                rest = subst(rest, x, Num(0.0))
+            if free_vars(simplify(rest)):
+                raise NmodlError(f"{m.suffix}: CONSERVE's left side may hold only states")
+            last = named[-1]
+            order = [x for x in order if x != last] + [last]
+        n = len(order)
+        ix = {x: i for i, x in enumerate(order)}
+        mat = {}                        # (row, col) -> C++ variable
+
+        def var(i, j):
+            return f"kn{self.k}_m{i}_{j}"
+        for x in order:
+            i = ix[x]
+            if conserve is not None and x == order[-1]:
+                for y, c in cons_row.items():
+                    mat[(i, ix[y])] = var(i, ix[y])
+                    w(f"{pad}{T} {var(i, ix[y])} = ({T}){c!r};")
+                w(f"{pad}{T} kn{self.k}_r{i} = ({T})({em.e(conserve.rhs)});")
+                continue
+            rates = out_rates.get(x, [])
+            diag = f"({T})1 + {dts} * ({T})({' + '.join(rates)})" if rates else f"({T})1"
+            mat[(i, i)] = var(i, i)
+            w(f"{pad}{T} {var(i, i)} = {diag};")
+            for y in order:
+                r = in_rates.get((x, y))
+                if r and y != x:
+                    mat[(i, ix[y])] = var(i, ix[y])
+                    w(f"{pad}{T} {var(i, ix[y])} = -{dts} * ({T})({' + '.join(r)});")
+            src = sources.get(x)
+            rhs = f"({T}){env[x]}" + (f" + {dts} * ({T})({' + '.join(src)})" if src else "")
+            w(f"{pad}{T} kn{self.k}_r{i} = {rhs};")
+        if (n - 1, n - 1) not in mat:
+            raise NmodlError(f"{m.suffix}: CONSERVE of KINETIC {name} leaves its last state out")
+        div = (lambda a, b: f"{a} / {b}") if steady else (lambda a, b: f"M::dv({a}, {b})")
+        for p_ in range(n):
+            w(f"{pad}const {T} kn{self.k}_i{p_} = {div(f'({T})1', var(p_, p_))};")
+            for r in range(p_ + 1, n):
+                if (r, p_) not in mat:
+                    continue
+                f = f"kn{self.k}_l{r}_{p_}"
+                w(f"{pad}const {T} {f} = {var(r, p_)} * kn{self.k}_i{p_};")
+                for c in range(p_ + 1, n):
+                    if (p_, c) not in mat:
+                        continue
+                    if (r, c) in mat:
+                        w(f"{pad}{var(r, c)} -= {f} * {var(p_, c)};")
+                    else:
+                        mat[(r, c)] = var(r, c)
+                        w(f"{pad}{T} {var(r, c)} = -{f} * {var(p_, c)};")
+                w(f"{pad}kn{self.k}_r{r} -= {f} * kn{self.k}_r{p_};")
+        for p_ in reversed(range(n)):
+            acc = f"kn{self.k}_r{p_}"
+            for c in range(p_ + 1, n):
+                if (p_, c) in mat:
+                    w(f"{pad}{acc} -= {var(p_, c)} * kn{self.k}_r{c};")
+            w(f"{pad}{acc} *= kn{self.k}_i{p_};")
+        for x in order:
+            w(f"{pad}{env[x]} = (R)kn{self.k}_r{ix[x]};")
+        w("    " * (ind - 1) + "}")
 
     def current_stmts(self, w, body, ind) -> dict:
         """BREAKPOINT assignments with their d/dv: returns name -> C++ derivative."""

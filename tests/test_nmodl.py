@@ -241,7 +241,7 @@ def _py(x):
 
 
 @pytest.mark.parametrize("text,msg", [
-    ("NEURON { SUFFIX k1 }\nSTATE { a b }\nKINETIC kin { ~ a <-> b (1, 2) }\n", "KINETIC"),
+    ("NEURON { SUFFIX k1 }\nSTATE { a }\nNET_RECEIVE (w) { a = a + w }\n", "NET_RECEIVE"),
     ("NEURON { SUFFIX q }\nSTATE { x }\nBREAKPOINT { SOLVE d METHOD cnexp }\nDERIVATIVE d { x' = -x*x }\n",
      "not linear"),
     ("NEURON { SUFFIX q }\nSTATE { x }\nBREAKPOINT { SOLVE d METHOD euler }\nDERIVATIVE d { x' = -x }\n",
