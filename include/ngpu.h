@@ -286,6 +286,40 @@ int ngpu_gemm_bf16_tn(const void *A, const void *B, int32_t M, int32_t N, int32_
                       int32_t ldt, const float *bias, const float *zin, void *cuda_stream);
 int ngpu_gemm_error(int32_t *flag);
 
+/*
+ * Genetic-algorithm steps on the device (all pointers device memory, all
+ * objectives minimised), so that a generation needs no host round trip.
+ * They replace the host-side DEAP operators between simulator calls
+ * (GUI/DEAP_helper.py:126-182 varOr; bluepyopt's selector set up at
+ * Figures/Figure4_DEAP/optimize_parameters_genetic_alg.py:49).
+ *
+ *   ngpu_ga_offspring       n_kids children of the population pop[mu][n_genes]:
+ *                           binary tournaments on (rank asc, crowd desc), with
+ *                           probability cx_prob bounded SBX (eta_c, per-gene
+ *                           probability 1/2) of the two winners, then bounded
+ *                           polynomial mutation (eta_m, per-gene probability
+ *                           p_mut), genes in [low, up].  Random draws are
+ *                           SplitMix64 of (seed, generation, child, draw): the
+ *                           same arguments give the same children.
+ *   ngpu_ga_select_truncation  the mu smallest scores (ties: lower index
+ *                           first; NaN last) -> out_idx[mu], in score order.
+ *   ngpu_ga_select_nsga2    NSGA-II survivors of obj[n][m]: front ranks by
+ *                           non-dominated sorting (rank[n]), crowding distance
+ *                           within fronts (crowd[n]; +inf at a front's ends),
+ *                           out_idx[mu] in (rank asc, crowd desc, index asc)
+ *                           order; n_fronts[0] = number of fronts.  NaN counts
+ *                           as +inf.  n <= 32768, m <= 192.
+ * Scratch memory is taken from and returned to the stream's pool
+ * (cudaMallocAsync).
+ */
+int ngpu_ga_offspring(const double *pop_dev, const int32_t *rank_dev, const double *crowd_dev, int32_t mu,
+                      int32_t n_genes, int32_t n_kids, double low, double up, double eta_c, double eta_m, double cx_prob,
+                      double p_mut, uint64_t seed, uint64_t generation, double *kids_dev, void *cuda_stream);
+int ngpu_ga_select_truncation(const double *score_dev, int32_t n, int32_t mu, int32_t *out_idx_dev,
+                              void *cuda_stream);
+int ngpu_ga_select_nsga2(const double *obj_dev, int32_t n, int32_t m, int32_t mu, int32_t *out_idx_dev,
+                         int32_t *rank_dev, double *crowd_dev, int32_t *n_fronts_dev, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,7 +38,7 @@ def lib() -> C.CDLL:
                 f"{LIB_PATH} is missing: build it with `python -m neurogpu_b200._build` "
                 "(the CUDA extension is required; there is no CPU path)")
         L = C.CDLL(str(LIB_PATH))
-        P, I32, I64, F32 = C.c_void_p, C.c_int32, C.c_int64, C.c_float
+        P, I32, I64, F32, D = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_double
         sig = {
             "ngpu_last_error": (C.c_char_p, []),
             "ngpu_abi_version": (C.c_int, []),
@@ -80,6 +80,10 @@ def lib() -> C.CDLL:
             "ngpu_jit_log": (C.c_char_p, []),
             "ngpu_launch_count": (I64, [I32]),
             "ngpu_run_static": (C.c_int, [P, I32, P, I32, I32, P, P, I32, F32, I32, P, F32, P, P]),
+            "ngpu_ga_offspring": (C.c_int, [P, P, P, I32, I32, I32, D, D, D, D, D, D, C.c_uint64, C.c_uint64,
+                                            P, P]),
+            "ngpu_ga_select_truncation": (C.c_int, [P, I32, I32, P, P]),
+            "ngpu_ga_select_nsga2": (C.c_int, [P, I32, I32, I32, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

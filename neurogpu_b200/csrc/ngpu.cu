@@ -23,6 +23,7 @@
 
 #include "../../include/ngpu.h"
 #include "features.cuh"
+#include "ga.cuh"
 #include "gemm_tc.cuh"
 #include "ngpu_jit.h"
 #include "sim_kernels.cuh"
@@ -1911,5 +1912,106 @@ extern "C" int ngpu_gemm_error(int32_t* flag) {
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_gemm_err, &zero, sizeof(int));
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("gemm error flag: ") + cudaGetErrorString(e));
     if (flag) *flag = v;
+    return NGPU_OK;
+}
+
+// ------------------------------------------------------------------ GA
+namespace {
+
+uint32_t pow2_at_least(int n) {
+    uint32_t p = 2;
+    while (p < (uint32_t)n) p <<= 1;
+    return p;
+}
+
+// stream-ordered scratch, freed on the same stream
+struct StreamScratch {
+    cudaStream_t st;
+    std::vector<void*> ptrs;
+    explicit StreamScratch(cudaStream_t s) : st(s) {}
+    ~StreamScratch() {
+        for (void* p : ptrs) cudaFreeAsync(p, st);
+    }
+    template <typename T>
+    T* get(size_t count, int* rc) {
+        void* p = nullptr;
+        const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), st);
+        if (e != cudaSuccess) {
+            *rc = fail(NGPU_E_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+            return nullptr;
+        }
+        ptrs.push_back(p);
+        return (T*)p;
+    }
+};
+
+int grid_for(size_t n, int threads) { return (int)std::min<size_t>((n + threads - 1) / threads, 148 * 32); }
+
+}  // namespace
+
+int ngpu_ga_offspring(const double* pop_dev, const int32_t* rank_dev, const double* crowd_dev, int32_t mu,
+                      int32_t n_genes, int32_t n_kids, double low, double up, double eta_c, double eta_m, double cx_prob,
+                      double p_mut, uint64_t seed, uint64_t generation, double* kids_dev, void* cuda_stream) {
+    if (!pop_dev || !rank_dev || !crowd_dev || !kids_dev) return fail(NGPU_E_INVALID, "ga_offspring: null pointer");
+    if (mu < 1 || n_genes < 1 || n_kids < 0) return fail(NGPU_E_INVALID, "ga_offspring: mu, n_genes >= 1");
+    if ((uint64_t)n_kids >= (1ull << 44) || kGaDrawsFixed + kGaDrawsPerGene * (uint64_t)n_genes >= (1u << 20))
+        return fail(NGPU_E_INVALID, "ga_offspring: too many children or genes for the draw counter");
+    if (!(up > low) || !(eta_c >= 0) || !(eta_m >= 0)) return fail(NGPU_E_INVALID, "ga_offspring: bad bounds or eta");
+    if (n_kids == 0) return NGPU_OK;
+    GaVariation a{pop_dev, rank_dev, crowd_dev, mu, n_genes, n_kids, low, up, eta_c, eta_m, cx_prob, p_mut,
+                  ga_key(seed, generation), kids_dev};
+    k_ga_offspring<<<(n_kids + 127) / 128, 128, 0, (cudaStream_t)cuda_stream>>>(a);
+    g_launches++;
+    NGPU_CUDA(cudaGetLastError());
+    return NGPU_OK;
+}
+
+int ngpu_ga_select_truncation(const double* score_dev, int32_t n, int32_t mu, int32_t* out_idx_dev,
+                              void* cuda_stream) {
+    if (!score_dev || !out_idx_dev) return fail(NGPU_E_INVALID, "ga_select_truncation: null pointer");
+    if (n < 1 || n > (1 << 24) || mu < 1 || mu > n) return fail(NGPU_E_INVALID, "ga_select_truncation: 1 <= mu <= n <= 2^24");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    int rc = NGPU_OK;
+    StreamScratch ws(st);
+    const uint32_t n2 = pow2_at_least(n);
+    GaSortSlice s{ws.get<uint64_t>(n2, &rc), ws.get<uint64_t>(n2, &rc), ws.get<uint32_t>(n2, &rc)};
+    if (rc != NGPU_OK) return rc;
+    k_ga_truncation_keys<<<grid_for(n2, 256), 256, 0, st>>>(score_dev, n, n2, s);
+    k_ga_sort<<<1, 1024, 0, st>>>(s, n2);
+    k_ga_take<<<grid_for(mu, 256), 256, 0, st>>>(s.idx, mu, out_idx_dev);
+    g_launches += 3;
+    NGPU_CUDA(cudaGetLastError());
+    return NGPU_OK;
+}
+
+int ngpu_ga_select_nsga2(const double* obj_dev, int32_t n, int32_t m, int32_t mu, int32_t* out_idx_dev,
+                         int32_t* rank_dev, double* crowd_dev, int32_t* n_fronts_dev, void* cuda_stream) {
+    if (!obj_dev || !out_idx_dev || !rank_dev || !crowd_dev || !n_fronts_dev)
+        return fail(NGPU_E_INVALID, "ga_select_nsga2: null pointer");
+    if (n < 1 || n > 32 * kGaMaxWords || mu < 1 || mu > n)
+        return fail(NGPU_E_INVALID, "ga_select_nsga2: 1 <= mu <= n <= " + std::to_string(32 * kGaMaxWords));
+    if (m < 1 || m > 192) return fail(NGPU_E_INVALID, "ga_select_nsga2: 1..192 objectives");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    int rc = NGPU_OK;
+    StreamScratch ws(st);
+    const int W = (n + 31) / 32;
+    const uint32_t n2 = pow2_at_least(n);
+    double* fT = ws.get<double>((size_t)n * m, &rc);
+    uint32_t* dom = ws.get<uint32_t>((size_t)n * W, &rc);
+    GaCrowdArgs c{fT, rank_dev, n, m, n2, ws.get<uint64_t>((size_t)m * n2, &rc), ws.get<uint64_t>((size_t)m * n2, &rc),
+                  ws.get<uint32_t>((size_t)m * n2, &rc), ws.get<int32_t>((size_t)m * n, &rc),
+                  ws.get<int32_t>((size_t)m * n, &rc), ws.get<double>((size_t)m * n, &rc)};
+    GaSortSlice s{ws.get<uint64_t>(n2, &rc), ws.get<uint64_t>(n2, &rc), ws.get<uint32_t>(n2, &rc)};
+    if (rc != NGPU_OK) return rc;
+    k_ga_transpose<<<grid_for((size_t)n * m, 256), 256, 0, st>>>(obj_dev, n, m, fT);
+    k_ga_dominance<<<dim3((n + kGaDomThreads - 1) / kGaDomThreads, W), kGaDomThreads, (size_t)m * 32 * sizeof(double),
+                     st>>>(fT, n, m, W, dom);
+    k_ga_fronts<<<1, 1024, 0, st>>>(dom, n, W, rank_dev, n_fronts_dev);
+    k_ga_crowding<<<m, 1024, 0, st>>>(c);
+    k_ga_crowd_sum<<<grid_for(n2, 256), 256, 0, st>>>(c.contrib, rank_dev, n, m, n2, crowd_dev, s);
+    k_ga_sort<<<1, 1024, 0, st>>>(s, n2);
+    k_ga_take<<<grid_for(mu, 256), 256, 0, st>>>(s.idx, mu, out_idx_dev);
+    g_launches += 7;
+    NGPU_CUDA(cudaGetLastError());
     return NGPU_OK;
 }

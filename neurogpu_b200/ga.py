@@ -51,6 +51,7 @@ class FitProblem:
     scale: np.ndarray = None
     sim_count: int = 0
     sim_seconds: float = 0.0
+    _dev: tuple | None = None
 
     def __post_init__(self):
         rng = np.random.default_rng(self.seed)
@@ -107,6 +108,61 @@ class FitProblem:
         feature's spread, over protocols and features: [n]."""
         d = (np.asarray(f) - self.target_f[None]) / self.scale[None, None, :]
         return np.mean(d * d, axis=(1, 2))
+
+    # ---- the same on CUDA tensors: parameters, features and scores stay on the device
+    def _tables(self):
+        """(base parameters [P][S], free-parameter map [K][P][S], target
+        features, feature spreads) as float64 CUDA tensors."""
+        if self._dev is None:
+            import torch
+            w = np.zeros((self.n_params,) + self.base.shape)
+            sec_region = np.array([self.cell.region_names[r] for r in self.cell.region])
+            for j, (pname, regions) in enumerate(FREE12):
+                w[j, MAINEN.param_index(pname), np.nonzero(np.isin(sec_region, regions))[0]] = 1.0
+            t = [torch.tensor(np.asarray(x, dtype=np.float64), device="cuda")
+                 for x in (self.base, w, self.target_f, self.scale)]
+            self._dev = tuple(t)
+        return self._dev
+
+    def params_device(self, u):
+        """params_of on the device: base x 2^u on each free parameter's
+        sections, [n][P][S] float32."""
+        import torch
+        base, w, _, _ = self._tables()
+        return (base[None] * torch.exp2(torch.einsum("nk,kps->nps", u.to(torch.float64), w))).float()
+
+    def simulate_device(self, u, chunk_sets: int = 16384):
+        """Features [n, n_stim, 20] (float32, on the device) of parameter
+        vectors u [n, 12] (a CUDA tensor)."""
+        import torch
+        from .sim import Simulator
+        t0 = time.perf_counter()
+        out = []
+        for i in range(0, u.shape[0], chunk_sets):
+            uu = u[i:i + chunk_sets]
+            sim = Simulator(self.cell, uu.shape[0], self.n_stim, "fp32")
+            sim.set_params(self.params_device(uu))
+            sim.set_stimulus(self.amps, np.full(self.amps.shape[1], self.dt, np.float32), 0, float(self.cell.area[0]))
+            sim.set_recording(np.array([0], dtype=np.int32), self.rec_every)
+            sim.init(-70.0)
+            sim.advance(0, self.amps.shape[1])
+            out.append(sim.features(self.dt * self.rec_every, self.stim_on, self.stim_off))
+            sim.close()
+        self.sim_count += u.shape[0]
+        self.sim_seconds += time.perf_counter() - t0
+        return torch.cat(out)
+
+    def score_device(self, f):
+        _, _, target, scale = self._tables()
+        d = (f.to(target.dtype) - target[None]) / scale[None, None, :]
+        return (d * d).mean(dim=(1, 2))
+
+    def objectives_device(self, f):
+        """One objective per (protocol, feature): |difference| in units of the
+        feature's spread, [n][n_stim * 20]."""
+        _, _, target, scale = self._tables()
+        d = (f.to(target.dtype) - target[None]) / scale[None, None, :]
+        return d.abs().reshape(d.shape[0], -1)
 
 
 # ------------------------------------------------------------------ operators
@@ -190,6 +246,51 @@ def run_plain(prob: FitProblem, pop_size: int, generations: int, seed: int = 0) 
         res.time.append(time.perf_counter() - t0)
         res.sims.append(prob.sim_count)
     res.best_u = pop[0]
+    return res
+
+
+def run_device(prob: FitProblem, pop_size: int, generations: int, seed: int = 0,
+               selector: str = "truncation") -> GAResult:
+    """The GA with every step on the device (csrc/ga.cuh): offspring by the
+    variation kernel, parameters expanded, simulated and reduced to features
+    and scores without a host copy, survivors by (mu + lambda) truncation on
+    the scalar score or by NSGA-II on the per-(protocol, feature)
+    objectives.  The host reads one number per generation (the best score,
+    for the result)."""
+    import torch
+
+    from .ga_device import DeviceGA, select_nsga2, select_truncation
+    if selector not in ("truncation", "nsga2"):
+        raise ValueError("selector: 'truncation' or 'nsga2'")
+    ga = DeviceGA(prob.n_params, seed=seed)
+    res = GAResult()
+    t0 = time.perf_counter()
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    pop = torch.rand((pop_size, prob.n_params), generator=gen, device="cuda", dtype=torch.float64) * 2.0 - 1.0
+    f = prob.simulate_device(pop)
+    score = prob.score_device(f)
+    if selector == "nsga2":
+        obj = prob.objectives_device(f)
+        _, rank, crowd, _ = select_nsga2(obj, pop_size)
+    else:
+        rank = torch.zeros(pop_size, dtype=torch.int32, device="cuda")
+        crowd = -score
+    for g in range(generations):
+        kids = ga.offspring(pop, rank, crowd, pop_size, g)
+        fk = prob.simulate_device(kids)
+        allp, alls = torch.cat([pop, kids]), torch.cat([score, prob.score_device(fk)])
+        if selector == "nsga2":
+            allo = torch.cat([obj, prob.objectives_device(fk)])
+            idx, rk, cr, _ = select_nsga2(allo, pop_size)
+            pop, score, obj, rank, crowd = allp[idx], alls[idx], allo[idx], rk[idx], cr[idx]
+        else:
+            idx = select_truncation(alls, pop_size)
+            pop, score = allp[idx], alls[idx]
+            crowd = -score
+        res.best.append(float(score.min()))
+        res.time.append(time.perf_counter() - t0)
+        res.sims.append(prob.sim_count)
+    res.best_u = pop[int(torch.argmin(score))].cpu().numpy()
     return res
 
 
