@@ -20,12 +20,17 @@
 // d, so any child is reproducible on its own and the host restatement
 // replays the same stream bit for bit.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
+
 namespace ngpu {
+
+namespace cg = cooperative_groups;
 
 __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ull;
@@ -149,37 +154,87 @@ struct GaSortSlice {
     uint32_t* idx;
 };
 
-__device__ __forceinline__ bool ga_less(const GaSortSlice& s, uint32_t a, uint32_t b) {
-    if (s.k1[a] != s.k1[b]) return s.k1[a] < s.k1[b];
-    if (s.k2[a] != s.k2[b]) return s.k2[a] < s.k2[b];
-    return s.idx[a] < s.idx[b];
+// Segmented bitonic sort: `count` independent segments of n2 entries (a
+// power of two) each, ascending by (k1, k2, idx).  Strides below the tile
+// (kGaSortTile entries, one CTA) run in shared memory -- the whole network
+// up to the tile size at first, then the tail of every later merge; strides
+// of a tile or more run as grid-wide stages, one launch each, every thread
+// one compare-exchange.  The direction of a pair follows its position in its
+// segment, so segments never mix.
+constexpr uint32_t kGaSortTile = 2048;
+constexpr int kGaSortThreads = 1024;
+
+__device__ __forceinline__ void ga_cmpswap(uint64_t* k1, uint64_t* k2, uint32_t* ix, size_t i, size_t l, bool asc) {
+    const bool less_li = k1[l] != k1[i] ? k1[l] < k1[i] : (k2[l] != k2[i] ? k2[l] < k2[i] : ix[l] < ix[i]);
+    if (less_li == asc) {
+        const uint64_t a1 = k1[i], a2 = k2[i];
+        const uint32_t ai = ix[i];
+        k1[i] = k1[l];
+        k2[i] = k2[l];
+        ix[i] = ix[l];
+        k1[l] = a1;
+        k2[l] = a2;
+        ix[l] = ai;
+    }
 }
 
-// Bitonic sort of n2 (a power of two) entries by (k1, k2, idx), ascending,
-// by one CTA over global memory; the barrier after each stage orders the
-// block's global writes.
-__device__ void ga_bitonic(const GaSortSlice& s, uint32_t n2) {
-    for (uint32_t k = 2; k <= n2; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const bool asc = (i & k) == 0;
-                    if (ga_less(s, l, i) == asc) {
-                        const uint64_t a1 = s.k1[i], a2 = s.k2[i];
-                        const uint32_t ai = s.idx[i];
-                        s.k1[i] = s.k1[l];
-                        s.k2[i] = s.k2[l];
-                        s.idx[i] = s.idx[l];
-                        s.k1[l] = a1;
-                        s.k2[l] = a2;
-                        s.idx[l] = ai;
-                    }
-                }
+// one tile per CTA: k_merge == 0 sorts the tile (every k up to the tile
+// size); otherwise the strides below the tile of merge step k_merge
+__global__ void __launch_bounds__(kGaSortThreads) k_ga_sort_tile(GaSortSlice s, uint32_t n2, uint32_t tile,
+                                                                 uint32_t k_merge) {
+    __shared__ uint64_t k1[kGaSortTile], k2[kGaSortTile];
+    __shared__ uint32_t ix[kGaSortTile];
+    const size_t base = (size_t)blockIdx.x * tile;
+    for (uint32_t t = threadIdx.x; t < tile; t += blockDim.x) {
+        k1[t] = s.k1[base + t];
+        k2[t] = s.k2[base + t];
+        ix[t] = s.idx[base + t];
+    }
+    __syncthreads();
+    const uint32_t pos0 = (uint32_t)(base & (n2 - 1));   // position of the tile in its segment
+    const uint32_t k_lo = k_merge ? k_merge : 2, k_hi = k_merge ? k_merge : tile;
+    for (uint32_t k = k_lo; k <= k_hi; k <<= 1) {
+        for (uint32_t j = (k_merge ? tile : k) >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < tile; t += blockDim.x) {
+                const uint32_t l = t ^ j;
+                if (l > t) ga_cmpswap(k1, k2, ix, t, l, ((pos0 + t) & k) == 0);
             }
             __syncthreads();
         }
     }
+    for (uint32_t t = threadIdx.x; t < tile; t += blockDim.x) {
+        s.k1[base + t] = k1[t];
+        s.k2[base + t] = k2[t];
+        s.idx[base + t] = ix[t];
+    }
+}
+
+// one grid-wide stage (k, j) with j >= the tile: pair p -> (i, i + j), bit j of i clear
+__global__ void k_ga_sort_stage(GaSortSlice s, size_t total, uint32_t n2, uint32_t k, uint32_t j) {
+    const size_t pairs = total >> 1;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < pairs; p += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = (p / j) * (2 * (size_t)j) + (p % j);
+        ga_cmpswap(s.k1, s.k2, s.idx, i, i + j, ((uint32_t)(i & (n2 - 1)) & k) == 0);
+    }
+}
+
+// host side: sort `count` segments of n2 entries on a stream; returns the launches issued
+inline int ga_sort(const GaSortSlice& s, uint32_t n2, int count, cudaStream_t st) {
+    const uint32_t tile = n2 < kGaSortTile ? n2 : kGaSortTile;
+    const size_t total = (size_t)n2 * count;
+    const unsigned tiles = (unsigned)(total / tile);
+    const unsigned grid = (unsigned)std::min<size_t>((total / 2 + 255) / 256, 148 * 16);
+    int launches = 1;
+    k_ga_sort_tile<<<tiles, kGaSortThreads, 0, st>>>(s, n2, tile, 0);
+    for (uint32_t k = 2 * tile; k <= n2; k <<= 1) {
+        for (uint32_t j = k >> 1; j >= tile; j >>= 1) {
+            k_ga_sort_stage<<<grid, 256, 0, st>>>(s, total, n2, k, j);
+            ++launches;
+        }
+        k_ga_sort_tile<<<tiles, kGaSortThreads, 0, st>>>(s, n2, tile, k);
+        ++launches;
+    }
+    return launches;
 }
 
 // keys of (mu + lambda) truncation: the score, then the index
@@ -191,8 +246,6 @@ __global__ void k_ga_truncation_keys(const double* score, int n, uint32_t n2, Ga
         s.idx[i] = i;
     }
 }
-
-__global__ void __launch_bounds__(1024) k_ga_sort(GaSortSlice s, uint32_t n2) { ga_bitonic(s, n2); }
 
 __global__ void k_ga_take(const uint32_t* sorted_idx, int mu, int32_t* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < mu; i += gridDim.x * blockDim.x) out[i] = (int32_t)sorted_idx[i];
@@ -242,101 +295,131 @@ __global__ void __launch_bounds__(kGaDomThreads) k_ga_dominance(const double* fT
 }
 
 // Front ranks by peeling: front r holds the individuals no remaining one
-// dominates.  One CTA; every front is non-empty (dominance is a strict
-// partial order), so at most n rounds.
+// dominates.  A cooperative grid: each round, every CTA stages the remaining
+// set R in shared memory and tests its share of individuals against it
+// (dominance rows are read until a remaining dominator turns up, so a
+// round's traffic is spread over the grid); new front members are or-ed
+// into NF; after a grid barrier R loses NF.  Every front is non-empty
+// (dominance is a strict partial order), so at most n rounds.  R, NF and
+// the count are written by other CTAs: they are read through L2 (__ldcg).
 constexpr int kGaMaxWords = 1024;   // n <= 32768
+constexpr int kGaFrontThreads = 256;
 
-__global__ void __launch_bounds__(1024) k_ga_fronts(const uint32_t* dom, int n, int W, int32_t* rank, int32_t* n_fronts) {
-    __shared__ uint32_t R[kGaMaxWords], NF[kGaMaxWords];
-    __shared__ int remaining;
-    for (int w = threadIdx.x; w < W; w += blockDim.x) {
-        const int valid = n - 32 * w;
-        R[w] = valid >= 32 ? 0xFFFFFFFFu : ((1u << valid) - 1u);
+struct GaFrontArgs {
+    const uint32_t* dom;     // [n][W]
+    int n, W;
+    int32_t* rank;           // [n]
+    uint32_t* R;             // [W] remaining
+    uint32_t* NF;            // [W] this round's front
+    int* remaining;
+    int32_t* n_fronts;
+};
+
+__global__ void __launch_bounds__(kGaFrontThreads) k_ga_fronts(const GaFrontArgs a) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ uint32_t Rs[kGaMaxWords];
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    for (int w = gtid; w < a.W; w += gstride) {
+        const int valid = a.n - 32 * w;
+        a.R[w] = valid >= 32 ? 0xFFFFFFFFu : ((1u << valid) - 1u);
+        a.NF[w] = 0;
     }
-    if (threadIdx.x == 0) remaining = n;
-    __syncthreads();
+    if (gtid == 0) *a.remaining = a.n;
+    grid.sync();
     int front = 0;
-    for (; front < n && remaining > 0; ++front) {
-        for (int w = threadIdx.x; w < W; w += blockDim.x) NF[w] = 0;
+    for (; front < a.n; ++front) {
+        if (__ldcg(a.remaining) == 0) break;    // the same value in every thread: read after the barrier
+        for (int w = threadIdx.x; w < a.W; w += blockDim.x) Rs[w] = __ldcg(a.R + w);
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            if (!((R[i >> 5] >> (i & 31)) & 1u)) continue;
-            const uint32_t* row = dom + (size_t)i * W;
+        for (int i = gtid; i < a.n; i += gstride) {
+            if (!((Rs[i >> 5] >> (i & 31)) & 1u)) continue;
+            const uint32_t* row = a.dom + (size_t)i * a.W;
             bool dominated = false;
-            for (int w = 0; w < W; ++w) {
-                if (row[w] & R[w]) {
+            for (int w = 0; w < a.W; ++w) {
+                if (row[w] & Rs[w]) {
                     dominated = true;
                     break;
                 }
             }
             if (!dominated) {
-                atomicOr(&NF[i >> 5], 1u << (i & 31));
-                rank[i] = front;
+                atomicOr(a.NF + (i >> 5), 1u << (i & 31));
+                a.rank[i] = front;
             }
         }
-        __syncthreads();
-        int removed = 0;
-        for (int w = threadIdx.x; w < W; w += blockDim.x) {
-            R[w] &= ~NF[w];
-            removed += __popc(NF[w]);
+        grid.sync();
+        for (int w = gtid; w < a.W; w += gstride) {
+            const uint32_t nf = __ldcg(a.NF + w);
+            if (nf) {
+                a.R[w] = __ldcg(a.R + w) & ~nf;
+                a.NF[w] = 0;
+                atomicSub(a.remaining, __popc(nf));
+            }
         }
-        if (removed) atomicSub(&remaining, removed);
-        __syncthreads();
+        grid.sync();
     }
     // unreachable with every front non-empty; kept so that a rank is always a valid index
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        if ((R[i >> 5] >> (i & 31)) & 1u) rank[i] = min(front, n - 1);
-    if (threadIdx.x == 0) *n_fronts = remaining == 0 ? front : -1;
+    for (int i = gtid; i < a.n; i += gstride)
+        if ((__ldcg(a.R + (i >> 5)) >> (i & 31)) & 1u) a.rank[i] = min(front, a.n - 1);
+    if (gtid == 0) *a.n_fronts = __ldcg(a.remaining) == 0 ? front : -1;
 }
 
-// Crowding distance, one CTA per objective k: sort by (rank, f_k, index);
-// the first and last of each front get +inf, the others (f_next - f_prev) /
-// (f_last - f_first) of their front (0 where the front is flat in f_k).
+// Crowding distance per objective k (one sorted segment each): sort by
+// (rank, f_k, index); the first and last of each front get +inf, the others
+// (f_next - f_prev) / (f_last - f_first) of their front (0 where the front is
+// flat in f_k).
 struct GaCrowdArgs {
     const double* fT;        // [m][n]
     const int32_t* rank;     // [n]
     int n, m;
     uint32_t n2;
-    uint64_t* k1;            // [m][n2] workspace
-    uint64_t* k2;
-    uint32_t* idx;
+    GaSortSlice s;           // [m][n2]
     int32_t* start;          // [m][n] first sorted position of each rank
     int32_t* end;
     double* contrib;         // [m][n]
 };
 
-__global__ void __launch_bounds__(1024) k_ga_crowding(const GaCrowdArgs a) {
-    const int k = blockIdx.x;
-    const double* f = a.fT + (size_t)k * a.n;
-    GaSortSlice s{a.k1 + (size_t)k * a.n2, a.k2 + (size_t)k * a.n2, a.idx + (size_t)k * a.n2};
-    int32_t* st = a.start + (size_t)k * a.n;
-    int32_t* en = a.end + (size_t)k * a.n;
-    for (uint32_t i = threadIdx.x; i < a.n2; i += blockDim.x) {
+__global__ void k_ga_crowd_keys(const GaCrowdArgs a) {
+    const size_t total = (size_t)a.m * a.n2;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = t / a.n2;
+        const uint32_t i = (uint32_t)(t % a.n2);
         const bool in = i < (uint32_t)a.n;
-        s.k1[i] = in ? (uint64_t)a.rank[i] : ~0ull;
-        s.k2[i] = in ? ga_order_key(f[i]) : ~0ull;
-        s.idx[i] = i;
+        a.s.k1[t] = in ? (uint64_t)a.rank[i] : ~0ull;
+        a.s.k2[t] = in ? ga_order_key(a.fT[k * a.n + i]) : ~0ull;
+        a.s.idx[t] = i;
     }
-    __syncthreads();
-    ga_bitonic(s, a.n2);
-    for (int p = threadIdx.x; p < a.n; p += blockDim.x) {
-        const uint64_t r = s.k1[p];
-        if (p == 0 || s.k1[p - 1] != r) st[r] = p;
-        if (p == a.n - 1 || s.k1[p + 1] != r) en[r] = p;
+}
+
+__global__ void k_ga_crowd_bounds(const GaCrowdArgs a) {
+    const size_t total = (size_t)a.m * a.n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = t / a.n;
+        const int p = (int)(t % a.n);
+        const uint64_t* k1 = a.s.k1 + k * a.n2;
+        const uint64_t r = k1[p];
+        if (p == 0 || k1[p - 1] != r) a.start[k * a.n + r] = p;
+        if (p == a.n - 1 || k1[p + 1] != r) a.end[k * a.n + r] = p;
     }
-    __syncthreads();
-    double* out = a.contrib + (size_t)k * a.n;
-    for (int p = threadIdx.x; p < a.n; p += blockDim.x) {
-        const uint64_t r = s.k1[p];
-        const int p0 = st[r], p1 = en[r];
+}
+
+__global__ void k_ga_crowd_contrib(const GaCrowdArgs a) {
+    const size_t total = (size_t)a.m * a.n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = t / a.n;
+        const int p = (int)(t % a.n);
+        const uint64_t* k1 = a.s.k1 + k * a.n2;
+        const uint32_t* ix = a.s.idx + k * a.n2;
+        const double* f = a.fT + k * a.n;
+        const uint64_t r = k1[p];
+        const int p0 = a.start[k * a.n + r], p1 = a.end[k * a.n + r];
         double c;
         if (p == p0 || p == p1) {
             c = INFINITY;
         } else {
-            const double lo = f[s.idx[p0]], hi = f[s.idx[p1]];
-            c = hi == lo ? 0.0 : (f[s.idx[p + 1]] - f[s.idx[p - 1]]) / (hi - lo);
+            const double lo = f[ix[p0]], hi = f[ix[p1]];
+            c = hi == lo ? 0.0 : (f[ix[p + 1]] - f[ix[p - 1]]) / (hi - lo);
         }
-        out[s.idx[p]] = c;
+        a.contrib[k * a.n + ix[p]] = c;
     }
 }
 

@@ -1977,9 +1977,9 @@ int ngpu_ga_select_truncation(const double* score_dev, int32_t n, int32_t mu, in
     GaSortSlice s{ws.get<uint64_t>(n2, &rc), ws.get<uint64_t>(n2, &rc), ws.get<uint32_t>(n2, &rc)};
     if (rc != NGPU_OK) return rc;
     k_ga_truncation_keys<<<grid_for(n2, 256), 256, 0, st>>>(score_dev, n, n2, s);
-    k_ga_sort<<<1, 1024, 0, st>>>(s, n2);
+    g_launches += ga_sort(s, n2, 1, st);
     k_ga_take<<<grid_for(mu, 256), 256, 0, st>>>(s.idx, mu, out_idx_dev);
-    g_launches += 3;
+    g_launches += 2;
     NGPU_CUDA(cudaGetLastError());
     return NGPU_OK;
 }
@@ -1998,20 +1998,39 @@ int ngpu_ga_select_nsga2(const double* obj_dev, int32_t n, int32_t m, int32_t mu
     const uint32_t n2 = pow2_at_least(n);
     double* fT = ws.get<double>((size_t)n * m, &rc);
     uint32_t* dom = ws.get<uint32_t>((size_t)n * W, &rc);
-    GaCrowdArgs c{fT, rank_dev, n, m, n2, ws.get<uint64_t>((size_t)m * n2, &rc), ws.get<uint64_t>((size_t)m * n2, &rc),
-                  ws.get<uint32_t>((size_t)m * n2, &rc), ws.get<int32_t>((size_t)m * n, &rc),
-                  ws.get<int32_t>((size_t)m * n, &rc), ws.get<double>((size_t)m * n, &rc)};
+    GaCrowdArgs c{fT, rank_dev, n, m, n2,
+                  GaSortSlice{ws.get<uint64_t>((size_t)m * n2, &rc), ws.get<uint64_t>((size_t)m * n2, &rc),
+                              ws.get<uint32_t>((size_t)m * n2, &rc)},
+                  ws.get<int32_t>((size_t)m * n, &rc), ws.get<int32_t>((size_t)m * n, &rc),
+                  ws.get<double>((size_t)m * n, &rc)};
     GaSortSlice s{ws.get<uint64_t>(n2, &rc), ws.get<uint64_t>(n2, &rc), ws.get<uint32_t>(n2, &rc)};
     if (rc != NGPU_OK) return rc;
     k_ga_transpose<<<grid_for((size_t)n * m, 256), 256, 0, st>>>(obj_dev, n, m, fT);
     k_ga_dominance<<<dim3((n + kGaDomThreads - 1) / kGaDomThreads, W), kGaDomThreads, (size_t)m * 32 * sizeof(double),
                      st>>>(fT, n, m, W, dom);
-    k_ga_fronts<<<1, 1024, 0, st>>>(dom, n, W, rank_dev, n_fronts_dev);
-    k_ga_crowding<<<m, 1024, 0, st>>>(c);
+    {
+        // cooperative: every CTA resident at once (the grid barrier needs it)
+        int dev = 0, sms = 0, per_sm = 0;
+        NGPU_CUDA(cudaGetDevice(&dev));
+        NGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        NGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ga_fronts, kGaFrontThreads, 0));
+        if (per_sm < 1) return fail(NGPU_E_CUDA, "ga_select_nsga2: the front kernel cannot be resident");
+        const int blocks = std::max(1, std::min(sms * per_sm, (n + kGaFrontThreads - 1) / kGaFrontThreads));
+        GaFrontArgs fa{dom, n, W, rank_dev, ws.get<uint32_t>(W, &rc), ws.get<uint32_t>(W, &rc), ws.get<int>(1, &rc),
+                       n_fronts_dev};
+        if (rc != NGPU_OK) return rc;
+        void* args[] = {&fa};
+        NGPU_CUDA(cudaLaunchCooperativeKernel((const void*)k_ga_fronts, dim3(blocks), dim3(kGaFrontThreads), args, 0,
+                                              st));
+    }
+    k_ga_crowd_keys<<<grid_for((size_t)m * n2, 256), 256, 0, st>>>(c);
+    g_launches += ga_sort(c.s, n2, m, st);
+    k_ga_crowd_bounds<<<grid_for((size_t)m * n, 256), 256, 0, st>>>(c);
+    k_ga_crowd_contrib<<<grid_for((size_t)m * n, 256), 256, 0, st>>>(c);
     k_ga_crowd_sum<<<grid_for(n2, 256), 256, 0, st>>>(c.contrib, rank_dev, n, m, n2, crowd_dev, s);
-    k_ga_sort<<<1, 1024, 0, st>>>(s, n2);
+    g_launches += ga_sort(s, n2, 1, st);
     k_ga_take<<<grid_for(mu, 256), 256, 0, st>>>(s.idx, mu, out_idx_dev);
-    g_launches += 7;
+    g_launches += 8;
     NGPU_CUDA(cudaGetLastError());
     return NGPU_OK;
 }
