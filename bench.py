@@ -58,7 +58,7 @@ def parse_args():
     ap.add_argument("--cpu-sample-steps", type=int, default=400)
     ap.add_argument("--ga-pop", type=int, default=8192)
     ap.add_argument("--ga-gens", type=int, default=20)
-    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga"],
+    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga", "ga_ops"],
                     help="uneven_batch: 8192 sets over 200/800/1500/3000-compartment trees x 5 protocols, "
                          "one launch per chunk, the run captured as a CUDA graph (auxiliary line)")
     return ap.parse_args()
@@ -322,12 +322,74 @@ def run_ga(args):
         "time_ratio": None if t_scr is None else t_scr / plain.time[-1]}))
 
 
+def run_ga_ops(args):
+    """One JSON line of the device GA steps (csrc/ga.cuh) at the reference's
+    GA size: bluepyopt's offspring_size 5000 (mu + lambda = 10,000), 12
+    genes, 60 objectives (3 protocols x 20 features); NSGA-II also at 2,048
+    and 32,768, and with 2 objectives (many fronts).  Device time with CUDA
+    events on the current stream over `--steps` calls after `--warmup`; the
+    numpy restatement (oracle/ga_numpy.py) on the host beside it where it
+    finishes in seconds.  value = the NSGA-II selection at 10,000 x 60 (ms)."""
+    import torch
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ga_numpy
+    from neurogpu_b200.ga_device import DeviceGA, select_nsga2, select_truncation
+
+    def dev_ms(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    def host_ms(fn, n=3):
+        t = time.perf_counter()
+        for _ in range(n):
+            fn()
+        return (time.perf_counter() - t) / n * 1e3
+
+    rng = np.random.default_rng(0)
+    mu, lam, genes = 5000, 5000, 12
+    pop = rng.uniform(-1, 1, (mu, genes))
+    rank = np.zeros(mu, np.int32)
+    crowd = rng.normal(size=mu)
+    ga = DeviceGA(genes, eta_c=20.0, eta_m=20.0, cx_prob=0.7, p_mut=0.3, seed=1)
+    tp, tr, tc = (torch.tensor(x, device="cuda") for x in (pop, rank, crowd))
+    out = {"offspring_5000x12": {"gpu_ms": dev_ms(lambda: ga.offspring(tp, tr, tc, lam, 3)),
+                                 "numpy_ms": host_ms(lambda: ga_numpy.offspring(pop, rank, crowd, lam, -1.0, 1.0,
+                                                                                20.0, 20.0, 0.7, 0.3, 1, 3))}}
+    sc = rng.normal(size=mu + lam)
+    ts = torch.tensor(sc, device="cuda")
+    out["truncation_10000"] = {"gpu_ms": dev_ms(lambda: select_truncation(ts, mu)),
+                               "numpy_ms": host_ms(lambda: ga_numpy.select_truncation(sc, mu))}
+    for n, m in ((2048, 60), (10000, 60), (32768, 60), (10000, 2)):
+        obj = rng.uniform(0, 1, (n, m))
+        to = torch.tensor(obj, device="cuda")
+        row = {"gpu_ms": dev_ms(lambda: select_nsga2(to, n // 2)), "fronts": int(select_nsga2(to, n // 2)[3])}
+        if n * n * m <= 2048 * 2048 * 60:
+            row["numpy_ms"] = host_ms(lambda: ga_numpy.select_nsga2(obj, n // 2), 1)
+        out[f"nsga2_{n}x{m}"] = row
+    print(json.dumps({
+        "metric": "NSGA-II selection time (10,000 x 60 objectives)", "value": out["nsga2_10000x60"]["gpu_ms"],
+        "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "dtype": "f64", "data": "synthetic (seeded uniform objectives)", "vs_baseline": None,
+        "config": {"workload": "ga_ops", "mu": mu, "lambda": lam, "genes": genes, "objectives": 60},
+        "steps_ms": out}))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "ga":
         return run_ga(args)
+    if args.workload == "ga_ops":
+        return run_ga_ops(args)
     if args.workload == "uneven_batch":
         return run_uneven(args)
     import torch
