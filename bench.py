@@ -228,7 +228,7 @@ def run_reference(args):
 
 
 def run_uneven(args):
-    """Config-4 line: the uneven batch, autotuned warps per morphology, init +
+    """Config-4 line: the uneven batch, autotuned warps and items per warp per morphology, init +
     `chunk` timesteps of every member captured once as a CUDA graph; each
     timed step replays it.  Inputs are resident; the state exceeds L2."""
     import torch
@@ -241,8 +241,8 @@ def run_uneven(args):
         m = Model(w.cell)
         res = autotune.tune_warps(m, w.params, w.amps, w.dts, w.stim_node, w.stim_area, w.rec_nodes, w.v_init,
                                   candidates=(2, 4, 6, 8), steps=min(100, w.nt - 20), warmup=20)
-        tuned[w.cell.n_nodes] = res["n_warps"]
-        s = Simulator(m, w.n_sets, w.n_stim, "fp32", n_warps=res["n_warps"])
+        tuned[w.cell.n_nodes] = [res["n_warps"], res["items_per_warp"]]
+        s = Simulator(m, w.n_sets, w.n_stim, "fp32", n_warps=res["n_warps"], items_per_warp=res["items_per_warp"])
         s.set_params(w.params)
         s.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
         s.set_recording(w.rec_nodes, 1)
@@ -278,7 +278,7 @@ def run_uneven(args):
             "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": "uneven_batch", "trees": [w.cell.n_nodes for w in ws],
                        "sets_per_tree": ws[0].n_sets, "protocols": ws[0].n_stim, "timesteps_per_step": nt,
-                       "warps_per_cta": tuned, "graph": "init + one batch launch per step, replayed",
+                       "warps_and_items_per_warp": tuned, "graph": "init + one batch launch per step, replayed",
                        "l2": "state larger than L2 (no flush)"},
             "gpu_launches": launches, "clocks": clk, "non_finite_instances": bad}))
     batch.close()

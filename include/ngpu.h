@@ -168,6 +168,14 @@ int ngpu_sim_advance(ngpu_sim *s, int32_t t0, int32_t n_steps, void *cuda_stream
  * morphology by timing. */
 int ngpu_sim_create_ex(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
                        ngpu_sim **out);
+/* As ngpu_sim_create_ex, also choosing how many work items per warp the tree
+ * is split into (1..8; 0 = the library's choice: 2 where the channel pass
+ * prefetches rows, 3 where it does not).  More items balance the warps'
+ * dynamic queue better at the price of more skeleton nodes; the best count
+ * depends on the morphology, so the autotuner times it.  No counterpart in
+ * the reference (one thread per compartment group, no split). */
+int ngpu_sim_create_shaped(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
+                           int32_t items_per_warp, ngpu_sim **out);
 
 /*
  * Several simulations in one launch (morphologies of different sizes, one

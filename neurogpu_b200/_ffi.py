@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
             "ngpu_run": (C.c_int, [P, I32, P, I32, I32, P, P, I32, F32, I32, P, F32, I32, P]),
             "ngpu_sim_create": (C.c_int, [P, I32, I32, I32, P]),
             "ngpu_sim_create_ex": (C.c_int, [P, I32, I32, I32, I32, P]),
+            "ngpu_sim_create_shaped": (C.c_int, [P, I32, I32, I32, I32, I32, P]),
             "ngpu_batch_create": (C.c_int, [P, I32, P]),
             "ngpu_batch_destroy": (C.c_int, [P]),
             "ngpu_batch_init": (C.c_int, [P, F32, P]),

@@ -1,8 +1,9 @@
 """Launch-shape autotuner for the simulation kernels.
 
-Per morphology and batch shape it picks the CTA's warp count, i.e. how finely
-the tree is split into work items for the CTA's warps (more warps: more
-parallel items and more skeleton nodes; fewer: longer items).  The candidates
+Per morphology and batch shape it picks the CTA's warp count and the number
+of work items per warp, i.e. how finely the tree is split for the CTA's warps
+(more warps or items: more parallel items, better balance and more skeleton
+nodes; fewer: longer items).  The candidates
 are timed on the device with CUDA events over a short advance of the real
 batch (all instances resident, so occupancy matches the production run), and
 the fastest is cached per (morphology, n_sets, n_stim, precision).
@@ -35,15 +36,16 @@ def _key(cell: CellModel, n_sets: int, n_stim: int, precision: str) -> str:
 
 def tune_warps(model: Model | CellModel, params, amps, dts, stim_node: int, stim_area: float, rec_nodes,
                v_init: float, candidates=(2, 4, 6, 8), steps: int = 100, warmup: int = 20,
-               precision: str = "fp32", cache_file: str | Path | None = None) -> dict:
-    """Times each candidate warp count on this batch and returns
-    {"n_warps": best, "ms_per_step": {W: ms}}.  params [n_sets, ...] and
-    amps [n_stim, nt >= warmup + steps] are the batch's own inputs."""
+               precision: str = "fp32", cache_file: str | Path | None = None, items=(2, 3, 4)) -> dict:
+    """Times each candidate (warp count, items per warp) on this batch and
+    returns {"n_warps": W, "items_per_warp": k, "ms_per_step": {"W:k": ms}}.
+    params [n_sets, ...] and amps [n_stim, nt >= warmup + steps] are the
+    batch's own inputs."""
     import torch
     model = model if isinstance(model, Model) else Model(model)
     cell = model.cell
     n_sets, n_stim = int(np.asarray(params).shape[0]), int(np.asarray(amps).shape[0])
-    key = _key(cell, n_sets, n_stim, precision)
+    key = _key(cell, n_sets, n_stim, precision) + ":" + ",".join(map(str, sorted(items)))
     if cache_file and Path(cache_file).exists() and not _CACHE:
         _CACHE.update(json.loads(Path(cache_file).read_text()))
     if key in _CACHE:
@@ -53,8 +55,10 @@ def tune_warps(model: Model | CellModel, params, amps, dts, stim_node: int, stim
         raise ValueError(f"need at least {warmup + steps} stimulus steps to time")
     stream = torch.cuda.current_stream()
     timings = {}
-    for W in sorted({int(w) for w in candidates if 1 <= int(w) <= 8}):
-        sim = Simulator(model, n_sets, n_stim, precision, n_warps=W)
+    shapes = [(W, k) for W in sorted({int(w) for w in candidates if 1 <= int(w) <= 8})
+              for k in (sorted({int(i) for i in items if 1 <= int(i) <= 8}) if W > 1 else [1])]
+    for W, k in shapes:
+        sim = Simulator(model, n_sets, n_stim, precision, n_warps=W, items_per_warp=k)
         sim.set_params(params)
         sim.set_stimulus(amps, dts, stim_node, stim_area)
         sim.set_recording(rec_nodes)
@@ -65,10 +69,11 @@ def tune_warps(model: Model | CellModel, params, amps, dts, stim_node: int, stim
         sim.advance(warmup, steps, stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        timings[W] = e0.elapsed_time(e1) / steps
+        timings[(W, k)] = e0.elapsed_time(e1) / steps
         sim.close()
     best = min(timings, key=timings.get)
-    res = {"n_warps": best, "ms_per_step": {str(k): v for k, v in timings.items()}}
+    res = {"n_warps": best[0], "items_per_warp": best[1],
+           "ms_per_step": {f"{w}:{k}": v for (w, k), v in timings.items()}}
     _CACHE[key] = res
     if cache_file:
         Path(cache_file).write_text(json.dumps(_CACHE, indent=1))

@@ -268,7 +268,7 @@ struct Partition {
     int n_jslots = 0;
 };
 
-static Partition make_partition(const ngpu_model* m, int W) {
+static Partition make_partition(const ngpu_model* m, int W, int items_per_warp = 2) {
     const int N = m->n;
     const std::vector<int>& par = m->parent;
     Partition P;
@@ -284,10 +284,9 @@ static Partition make_partition(const ngpu_model* m, int W) {
         }
     }
     auto heavy = [&](int i) { return (i + 1 < N && par[i + 1] == i) ? i + 1 : -1; };
-    // items of at most ~1/(2W) of the cost: twice as many items as warps balance the
-    // dynamic queue better than one per warp (measured on B200: -10 % step time on the
-    // 500-compartment HH model, unchanged on the TTPC-like one), at a few more separators
-    const int64_t parts = W > 1 ? 2 * (int64_t)W : 1;
+    // items of at most ~1/(k W) of the cost: k items per warp balance the dynamic queue
+    // better than one, at a few more separators (the simulation chooses k per model)
+    const int64_t parts = W > 1 ? (int64_t)std::max(1, items_per_warp) * W : 1;
     const int64_t target = std::max<int64_t>(1, (subw[0] + parts - 1) / parts);
     std::vector<char> is_sep(N, 0);
     is_sep[0] = 1;
@@ -420,7 +419,19 @@ struct ngpu_sim {
     const ngpu_jit::Module* jit = nullptr;
     ngpu_batch* batch = nullptr;  // the batch whose kernels this simulation's records follow
     int s2_stage = 0;             // skeleton solved from shared memory (see sim_kernels.cuh)
+    int items_per_warp = 2;       // work items per warp in the tree split
+    bool ch_prefetch = true;      // the runtime-specialised kernel compiles the channel-pass L2 prefetch in
 };
+
+// Rows (state and parameter) a node's channel update reads, on average; the
+// channel-pass prefetch is compiled in from kPrefetchRowsPerNode on.  Measured
+// on B200: the HH-type cells (~30 rows per node) run 7-13 % faster with it,
+// the TTPC-like cell (~12) 7 % faster without it.
+constexpr double kPrefetchRowsPerNode = 20.0;
+
+static double rows_per_node(const ngpu_model* m) {
+    return m->n > 0 ? (double)(m->state_vars + m->param_reads) / m->n : 0.0;
+}
 
 // CTAs per SM that `smem` bytes of dynamic shared memory and W warps of 80
 // registers allow (228 KB per SM, 1 KB of it reserved per CTA).
@@ -867,7 +878,14 @@ int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t preci
 
 int ngpu_sim_create_ex(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
                        ngpu_sim** out) {
+    return ngpu_sim_create_shaped(m, n_sets, n_stim, precision, n_warps, 0, out);
+}
+
+int ngpu_sim_create_shaped(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
+                           int32_t items_per_warp, ngpu_sim** out) {
     if (!out) return fail(NGPU_E_INVALID, "out is null");
+    if (items_per_warp < 0 || items_per_warp > 8)
+        return fail(NGPU_E_INVALID, "items_per_warp must be 0 (automatic) or 1..8");
     if (n_warps < 0 || n_warps > kMaxWarps)
         return fail(NGPU_E_INVALID, "n_warps must be 0 (automatic) or 1.." + std::to_string(kMaxWarps));
     *out = nullptr;
@@ -900,7 +918,14 @@ int ngpu_sim_create_ex(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t pr
     if (n_warps > 0) W = n_warps;
     W = std::min(W, m->n);
     s->n_warps = W;
-    s->part = make_partition(m, W);
+    s->ch_prefetch = rows_per_node(m) >= kPrefetchRowsPerNode;
+    if (const char* ev = getenv("NGPU_CH_PREFETCH")) s->ch_prefetch = atoi(ev) != 0;
+    // without the prefetch, finer items balance better (TTPC-like: +4 % from 2 to 3 per warp);
+    // the autotuner searches this per morphology
+    s->items_per_warp = s->ch_prefetch ? 2 : 3;
+    if (const char* ev = getenv("NGPU_ITEMS_PER_WARP")) s->items_per_warp = std::max(1, std::min(8, atoi(ev)));
+    if (items_per_warp > 0) s->items_per_warp = items_per_warp;
+    s->part = make_partition(m, W, s->items_per_warp);
     s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W)
                                          : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W);
     const int nj = s->part.n_jslots;
@@ -1137,7 +1162,8 @@ static int sim_upload_nodes(ngpu_sim* s) {
         if (s->batch) s->jit = s->batch->jit;
         else
             s->jit = ngpu_jit::module(m->mechset, s->precision == NGPU_FP64,
-                                      ngpu_jit::pick_masks(model_masks(m), kMaxClasses), gs ? &gs->source : nullptr);
+                                      ngpu_jit::pick_masks(model_masks(m), kMaxClasses), gs ? &gs->source : nullptr,
+                                      s->ch_prefetch);
         if (gs && !s->jit)
             return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
                                          "' runs only through runtime compilation: " + ngpu_jit::last_log());
@@ -1279,12 +1305,14 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
     const GenSet* gs = gen_set(b->mechset);
     if (b->precision == NGPU_FP32 || gs) {  // one specialised kernel over every member's masks
         std::vector<uint32_t> all;
+        int64_t pf_ctas = 0;   // the prefetch follows the members that hold most of the CTAs
         for (ngpu_sim* s : b->sims) {
             const std::vector<uint32_t> mm = model_masks(s->m);
             all.insert(all.end(), mm.begin(), mm.end());
+            pf_ctas += s->ch_prefetch ? s->n_groups : -s->n_groups;
         }
         b->jit = ngpu_jit::module(b->mechset, b->precision == NGPU_FP64, ngpu_jit::pick_masks(all, kMaxClasses),
-                                  gs ? &gs->source : nullptr);
+                                  gs ? &gs->source : nullptr, pf_ctas >= 0);
         if (gs && !b->jit) {
             delete b;
             return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +

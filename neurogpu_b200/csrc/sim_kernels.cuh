@@ -64,6 +64,14 @@ constexpr int kMaxWarps = 8;   // 256 threads; with 3 CTAs per SM the 85-registe
 #ifndef NGPU_ADV_MIN_BLOCKS
 #define NGPU_ADV_MIN_BLOCKS 3
 #endif
+// L2 prefetch of each node's state and parameter rows two nodes ahead in the
+// channel pass.  A compile-time choice: it pays on models whose nodes read
+// many rows (every node of the HH-type cells carries 7 mechanisms, ~30 rows)
+// and costs where most nodes read few (the TTPC-like cell, ~12), even when a
+// runtime flag turns it off; the runtime-specialised kernels set it per model.
+#ifndef NGPU_CH_PREFETCH
+#define NGPU_CH_PREFETCH 1
+#endif
 
 // Per-node record, identical for every instance; staged in shared memory
 // once per launch (32 bytes in FP32).
@@ -588,12 +596,13 @@ __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R
     R e_l = 0;
     int vi = -1;  // node whose V was read last as a parent voltage
     R vv = 0;
-    if (n > 0) prefetch_channels(G, nr[node_at(0)]);
-    if (n > 1) prefetch_channels(G, nr[node_at(1)]);
+    constexpr bool pf = NGPU_CH_PREFETCH != 0;
+    if (pf && n > 0) prefetch_channels(G, nr[node_at(0)]);
+    if (pf && n > 1) prefetch_channels(G, nr[node_at(1)]);
     for (int p = 0; p < n; ++p) {
         const int i = node_at(p);
         const NodeRec<R> nd = nr[i];
-        if (p + 2 < n) prefetch_channels(G, nr[node_at(p + 2)]);
+        if (pf && p + 2 < n) prefetch_channels(G, nr[node_at(p + 2)]);
         R V;
         if (vi == i) V = vv;
         else V = G.vbuf[(size_t)i * 2 * kLanes];

@@ -112,15 +112,17 @@ class Simulator:
     """Resident simulation of n_sets x n_stim instances of one model."""
 
     def __init__(self, model: Model | CellModel, n_sets: int, n_stim: int, precision: str = "fp32",
-                 n_warps: int = 0):
-        """n_warps: warps per CTA (1..8), 0 = the library's choice; see
+                 n_warps: int = 0, items_per_warp: int = 0):
+        """n_warps: warps per CTA (1..8), items_per_warp: work items per warp
+        in the tree split (1..8); 0 = the library's choice for either; see
         neurogpu_b200.autotune for timing-based selection."""
         self.model = model if isinstance(model, Model) else Model(model)
         self.n_sets, self.n_stim = int(n_sets), int(n_stim)
         self.precision = precision
         h = C.c_void_p()
-        _ffi.check("ngpu_sim_create_ex", _ffi.lib().ngpu_sim_create_ex(
-            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], int(n_warps), C.byref(h)))
+        _ffi.check("ngpu_sim_create_shaped", _ffi.lib().ngpu_sim_create_shaped(
+            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], int(n_warps), int(items_per_warp),
+            C.byref(h)))
         self._h = h
         self.nt = 0
         self.n_rec = 1

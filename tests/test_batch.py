@@ -76,10 +76,10 @@ def test_autotuner_picks_a_candidate(ngpu_built, workloads):
     from neurogpu_b200 import autotune
     w = workloads[2]
     res = autotune.tune_warps(w.cell, w.params, w.amps, w.dts, w.stim_node, w.stim_area, w.rec_nodes, w.v_init,
-                              candidates=(2, 4, 8), steps=100, warmup=20)
-    assert res["n_warps"] in (2, 4, 8) and len(res["ms_per_step"]) == 3
+                              candidates=(2, 4, 8), steps=100, warmup=20, items=(2, 3))
+    assert res["n_warps"] in (2, 4, 8) and res["items_per_warp"] in (2, 3) and len(res["ms_per_step"]) == 6
     assert autotune.tune_warps(w.cell, w.params, w.amps, w.dts, w.stim_node, w.stim_area, w.rec_nodes,
-                               w.v_init, candidates=(2, 4, 8)) is res      # cached
+                               w.v_init, candidates=(2, 4, 8), items=(2, 3)) is res      # cached
 
 
 def test_uneven_batch_fp32_vs_oracle_sample(ngpu_built, oracle, workloads):
