@@ -371,7 +371,7 @@ def run_ga_ops(args):
         obj = rng.uniform(0, 1, (n, m))
         to = torch.tensor(obj, device="cuda")
         row = {"gpu_ms": dev_ms(lambda: select_nsga2(to, n // 2)), "fronts": int(select_nsga2(to, n // 2)[3])}
-        if n * n * m <= 2048 * 2048 * 60:
+        if n <= 2048:
             row["numpy_ms"] = host_ms(lambda: ga_numpy.select_nsga2(obj, n // 2), 1)
         out[f"nsga2_{n}x{m}"] = row
     print(json.dumps({

@@ -317,8 +317,10 @@ int ngpu_gemm_error(int32_t *flag);
  *                           out_idx[mu] in (rank asc, crowd desc, index asc)
  *                           order; n_fronts[0] = number of fronts.  NaN counts
  *                           as +inf.  n <= 32768, m <= 192.
- * Scratch memory is taken from and returned to the stream's pool
- * (cudaMallocAsync).
+ * Scratch memory is taken from and returned to the device's default
+ * stream-ordered pool (cudaMallocAsync); the first call raises that pool's
+ * release threshold so that freed scratch stays in the pool for the next
+ * call (for the life of the process).
  */
 int ngpu_ga_offspring(const double *pop_dev, const int32_t *rank_dev, const double *crowd_dev, int32_t mu,
                       int32_t n_genes, int32_t n_kids, double low, double up, double eta_c, double eta_m, double cx_prob,

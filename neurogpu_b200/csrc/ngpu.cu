@@ -1952,11 +1952,30 @@ uint32_t pow2_at_least(int n) {
     return p;
 }
 
+// Keep freed scratch in the current device's stream-ordered pool instead of
+// returning it to the system at every synchronisation (the pool's default),
+// so that repeated GA steps reuse it; set once per device, for this process.
+void keep_pool_memory() {
+    static std::mutex mu;
+    static std::vector<int> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done.push_back(dev);
+}
+
 // stream-ordered scratch, freed on the same stream
 struct StreamScratch {
     cudaStream_t st;
     std::vector<void*> ptrs;
-    explicit StreamScratch(cudaStream_t s) : st(s) {}
+    explicit StreamScratch(cudaStream_t s) : st(s) { keep_pool_memory(); }
     ~StreamScratch() {
         for (void* p : ptrs) cudaFreeAsync(p, st);
     }

@@ -23,9 +23,9 @@ TOL_FP32_MV = 0.1
 TOL_SPIKE_MS = 0.05
 
 
-def _gpu_run(w, precision, chunks=None):
+def _gpu_run(w, precision, chunks=None, **shape):
     from neurogpu_b200.sim import Simulator
-    sim = Simulator(w.cell, w.n_sets, w.n_stim, precision)
+    sim = Simulator(w.cell, w.n_sets, w.n_stim, precision, **shape)
     sim.set_params(w.params)
     sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
     sim.set_recording(w.rec_nodes)
@@ -82,6 +82,17 @@ def test_fp32_matches_oracle(ngpu_built, refs, cfg, name):
     assert mism == 0
     assert st <= TOL_SPIKE_MS
     assert sub <= TOL_FP32_MV, f"{name}: FP32 max|dV| away from spikes = {sub:.3e} mV"
+
+
+@pytest.mark.parametrize("name,items", [("hh", 1), ("hh", 4), ("ttpc", 1), ("ttpc", 4)])
+def test_items_per_warp_split_matches_oracle(ngpu_built, refs, cfg, name, items):
+    """Another split of the tree (1 or 4 work items per warp instead of the
+    default) changes only the elimination's grouping: FP64 against the
+    oracle within the same bound."""
+    w = cfg[name]
+    got = _gpu_run(w, "fp64", items_per_warp=items)
+    err = np.max(np.abs(got.astype(np.float64) - refs[name]))
+    assert err <= TOL_FP64_MV, f"{name}, {items} items per warp: FP64 max|dV| = {err:.3e} mV"
 
 
 def test_chunked_advance_is_bitwise_identical(ngpu_built, cfg):

@@ -359,3 +359,20 @@ def test_stiff_edge_merging(ngpu_built):
     assert np.max(np.abs(x - xg[ni])) <= 1e-8 * np.max(np.abs(x))
     for c in CELLS.values():
         assert Model(c).nodes()["n_internal"] == c.n_nodes
+
+
+def test_shaped_simulation_rejects_bad_shapes(ngpu_built):
+    """ngpu_sim_create_shaped checks its warp and item counts before any
+    device work."""
+    import ctypes as C
+
+    from neurogpu_b200 import _ffi, configs
+    from neurogpu_b200.sim import Model
+    w = configs.passive_cable(n_sets=2, t_stop=1.0)
+    m = Model(w.cell)
+    L = _ffi.lib()
+    h = C.c_void_p()
+    assert L.ngpu_sim_create_shaped(m.handle, 2, 1, 0, 4, 9, C.byref(h)) == -1
+    assert b"items_per_warp" in L.ngpu_last_error()
+    assert L.ngpu_sim_create_shaped(m.handle, 2, 1, 0, 4, -1, C.byref(h)) == -1
+    assert L.ngpu_sim_create_shaped(m.handle, 2, 1, 0, 9, 2, C.byref(h)) == -1
