@@ -239,6 +239,13 @@ int ngpu_sim_features(ngpu_sim *s, int32_t site, double dt, double stim_on, doub
  *   ngpu_jit_log      the last compile failure or reason for falling back
  */
 int ngpu_sim_classes(const ngpu_sim *s, int32_t *n_classes);
+/* Parameters the simulation's runtime-specialised kernel compiles in as
+ * constants (after init): those with one value in every parameter set and
+ * every section that uses them, found by set_params; 0 where folding does
+ * not apply (FP64, generated sets, batches, NGPU_JIT=0 or NGPU_PARAM_FOLD=0).
+ * The reference compiles its model's GLOBAL parameters into its generated
+ * channel code in the same way (AllModels.cu). */
+int ngpu_sim_param_folds(const ngpu_sim *s, int32_t *n_folds);
 int ngpu_jit_build(int32_t mechset, int32_t precision, const uint32_t *masks, int32_t n_masks,
                    int32_t cc_major, int32_t cc_minor, int64_t *cubin_bytes);
 const char *ngpu_jit_log(void);

@@ -17,7 +17,7 @@ INCLUDE = HERE.parent / "include"
 
 # kernel headers the runtime specialisation (ngpu_jit.h) compiles with NVRTC,
 # embedded in the library as text
-JIT_HEADERS = ["ngpu_math.cuh", "node_classes.cuh", "channels_ttpc.cuh", "channels_mainen.cuh", "sim_kernels.cuh"]
+JIT_HEADERS = ["ngpu_math.cuh", "param_fold.cuh", "node_classes.cuh", "channels_ttpc.cuh", "channels_mainen.cuh", "sim_kernels.cuh"]
 JIT_INC = CSRC / "jit_sources.inc"
 
 NVCC_FLAGS = [

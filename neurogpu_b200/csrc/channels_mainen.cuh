@@ -46,38 +46,37 @@ NGPU_HD void mainen_node(MK mk, R v, R dt, R* __restrict__ st, const float* __re
     R pas[6] = {0, 0, 0, 0, 0, 0};
     {
         int s = 0, q = 0;
-        if (mk & Mainen::kCa) { if (!INIT) { ca_m = st[s * S]; ca_h = st[(s + 1) * S]; } s += 2; g_ca = (R)pr[q * S]; q += 1; }
+        // parameter rows hold the set's parameters 0, 2-33 (ca's cao, 1, is not read)
+        if (mk & Mainen::kCa) { if (!INIT) { ca_m = st[s * S]; ca_h = st[(s + 1) * S]; } s += 2; g_ca = pload<R, 0>(pr, q); q += 1; }
         if (mk & Mainen::kCad) { if (!INIT) { cai = st[s * S]; ica = st[(s + 1) * S]; } s += 2; }
         if (mk & Mainen::kKca) {
             if (!INIT) kca_n = st[s * S];
             s += 1;
-            g_kca = (R)pr[q * S]; caix = (R)pr[(q + 1) * S]; ra_kca = (R)pr[(q + 2) * S]; rb_kca = (R)pr[(q + 3) * S];
+            g_kca = pload<R, 2>(pr, q); caix = pload<R, 3>(pr, q + 1); ra_kca = pload<R, 4>(pr, q + 2);
+            rb_kca = pload<R, 5>(pr, q + 3);
             q += 4;
         }
         if (mk & Mainen::kKm) {
             if (!INIT) km_n = st[s * S];
             s += 1;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) km[k] = (R)pr[(q + k) * S];
+            pload_n<R, 6, 5>(pr, q, km);
             q += 5;
         }
         if (mk & Mainen::kKv) {
             if (!INIT) kv_n = st[s * S];
             s += 1;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) kv[k] = (R)pr[(q + k) * S];
+            pload_n<R, 11, 5>(pr, q, kv);
             q += 5;
         }
         if (mk & Mainen::kNa) {
             if (!INIT) { na_m = st[s * S]; na_h = st[(s + 1) * S]; }
             s += 2;
-#pragma unroll
-            for (int k = 0; k < 12; ++k) na[k] = (R)pr[(q + k) * S];
+            pload_n<R, 16, 12>(pr, q, na);
             q += 12;
         }
-        if (mk & Mainen::kPas) { pas[0] = (R)pr[q * S]; pas[1] = (R)pr[(q + 1) * S]; q += 2; }
-        if (mk & Mainen::kPas2) { pas[2] = (R)pr[q * S]; pas[3] = (R)pr[(q + 1) * S]; q += 2; }
-        if (mk & Mainen::kPasx) { pas[4] = (R)pr[q * S]; pas[5] = (R)pr[(q + 1) * S]; q += 2; }
+        if (mk & Mainen::kPas) { pas[0] = pload<R, 28>(pr, q); pas[1] = pload<R, 29>(pr, q + 1); q += 2; }
+        if (mk & Mainen::kPas2) { pas[2] = pload<R, 30>(pr, q); pas[3] = pload<R, 31>(pr, q + 1); q += 2; }
+        if (mk & Mainen::kPasx) { pas[4] = pload<R, 32>(pr, q); pas[5] = pload<R, 33>(pr, q + 1); q += 2; }
     }
     // ------------------------------------------------------------- compute
     R Itot = 0, Gtot = 0;

@@ -24,6 +24,7 @@
 // Parameter rows: the reference parameter indices each mechanism reads.
 #pragma once
 #include "ngpu_math.cuh"
+#include "param_fold.cuh"
 
 namespace ngpu {
 
@@ -207,20 +208,21 @@ NGPU_HD void ttpc_node(MK mk, R v, R dt, R* __restrict__ st, const float* __rest
         int s = 0, q = 0;
 #define LD2(A, B) { if (!INIT) { A = st[s * S]; B = st[(s + 1) * S]; } s += 2; }
 #define LD1(A) { if (!INIT) A = st[s * S]; s += 1; }
-#define P1(A) { A = (R)pr[q * S]; q += 1; }
-        if (mk & TTPC::kCaHVA) { LD2(hva_m, hva_h) P1(g_hva) }
-        if (mk & TTPC::kCaLVA) { LD2(lva_m, lva_h) P1(g_lva) }
-        if (mk & TTPC::kCaDyn) { LD2(cai, ica) P1(gamma) P1(decay) P1(depth) P1(mincai) }
-        if (mk & TTPC::kIh) { LD1(ih_m) P1(g_ih) P1(e_ih) }
-        if (mk & TTPC::kIm) { LD1(im_m) P1(g_im) }
-        if (mk & TTPC::kKP) { LD2(kp_m, kp_h) P1(g_kp) }
-        if (mk & TTPC::kKT) { LD2(kt_m, kt_h) P1(g_kt) }
-        if (mk & TTPC::kNap) { LD2(nap_m, nap_h) P1(g_nap) }
-        if (mk & TTPC::kNaTa) { LD2(nta_m, nta_h) P1(g_nta) }
-        if (mk & TTPC::kNaTs2) { LD2(nts_m, nts_h) P1(g_nts) }
-        if (mk & TTPC::kPas) { P1(g_pas) P1(e_pas) }
-        if (mk & TTPC::kSK) { LD1(sk_z) P1(g_sk) P1(ztau) }
-        if (mk & TTPC::kSKv3) { LD1(skv_m) P1(g_skv) }
+// P1(A, I): A = parameter I of the set (a compile-time constant where folded)
+#define P1(A, I) { A = pload<R, I>(pr, q); q += 1; }
+        if (mk & TTPC::kCaHVA) { LD2(hva_m, hva_h) P1(g_hva, 0) }
+        if (mk & TTPC::kCaLVA) { LD2(lva_m, lva_h) P1(g_lva, 1) }
+        if (mk & TTPC::kCaDyn) { LD2(cai, ica) P1(gamma, 2) P1(decay, 3) P1(depth, 4) P1(mincai, 5) }
+        if (mk & TTPC::kIh) { LD1(ih_m) P1(g_ih, 6) P1(e_ih, 7) }
+        if (mk & TTPC::kIm) { LD1(im_m) P1(g_im, 8) }
+        if (mk & TTPC::kKP) { LD2(kp_m, kp_h) P1(g_kp, 9) }
+        if (mk & TTPC::kKT) { LD2(kt_m, kt_h) P1(g_kt, 10) }
+        if (mk & TTPC::kNap) { LD2(nap_m, nap_h) P1(g_nap, 11) }
+        if (mk & TTPC::kNaTa) { LD2(nta_m, nta_h) P1(g_nta, 12) }
+        if (mk & TTPC::kNaTs2) { LD2(nts_m, nts_h) P1(g_nts, 13) }
+        if (mk & TTPC::kPas) { P1(g_pas, 14) P1(e_pas, 15) }
+        if (mk & TTPC::kSK) { LD1(sk_z) P1(g_sk, 16) P1(ztau, 17) }
+        if (mk & TTPC::kSKv3) { LD1(skv_m) P1(g_skv, 18) }
 #undef LD2
 #undef LD1
 #undef P1

@@ -420,6 +420,8 @@ struct ngpu_sim {
     ngpu_batch* batch = nullptr;  // the batch whose kernels this simulation's records follow
     int s2_stage = 0;             // skeleton solved from shared memory (see sim_kernels.cuh)
     int items_per_warp = 2;       // work items per warp in the tree split
+    ngpu_jit::Folds folds;        // parameters the runtime-specialised kernel compiles in
+    uint2* d_prange = nullptr;    // [ptab_rows] bit-pattern range of each parameter row
     bool ch_prefetch = true;      // the runtime-specialised kernel compiles the channel-pass L2 prefetch in
 };
 
@@ -865,7 +867,7 @@ static void sim_free(ngpu_sim* s) {
     if (!s) return;
     void* ptrs[] = {s->d_nodes, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc, s->d_jx,
                     s->d_inst_stim, s->d_bad, s->d_err, s->d_row_param, s->d_row_sec, s->d_amps,
-                    s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv};
+                    s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv, s->d_prange};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete s;
@@ -986,6 +988,54 @@ int ngpu_sim_destroy(ngpu_sim* s) {
     return NGPU_OK;
 }
 
+static int sim_upload_nodes(ngpu_sim* s);
+
+// Parameters with one value (the same bits) in every parameter set and every
+// section whose nodes use them: the runtime-specialised kernel compiles them
+// in (param_fold.cuh).  Only where that kernel runs (FP32, built-in sets, not
+// in a batch, runtime compilation on, NGPU_PARAM_FOLD not 0).  New values
+// after initialisation re-select the kernel before the next launch.
+static int sim_find_folds(ngpu_sim* s) {
+    const ngpu_model* m = s->m;
+    ngpu_jit::Folds folds;
+    const char* ev = getenv("NGPU_PARAM_FOLD");
+    const bool on = s->precision == NGPU_FP32 && !gen_set(m->mechset) && !s->batch && ngpu_jit::enabled() &&
+                    !(ev && ev[0] == '0') && m->ptab_rows > 0;
+    if (on) {
+        if (!s->d_prange) {
+            int rc = NGPU_OK;
+            s->d_prange = (uint2*)dmalloc(sizeof(uint2) * m->ptab_rows, &rc);
+            if (!s->d_prange) return rc;
+        }
+        k_ptab_range<<<m->ptab_rows, 256>>>(s->d_ptab, m->ptab_rows, s->n_groups, s->d_prange);
+        g_launches++;
+        std::vector<uint2> rng(m->ptab_rows);
+        NGPU_CUDA(cudaMemcpy(rng.data(), s->d_prange, sizeof(uint2) * m->ptab_rows, cudaMemcpyDeviceToHost));
+        std::vector<int> state(m->n_params, 0);        // 0 unseen, 1 one value so far, 2 varies
+        std::vector<unsigned> bits(m->n_params, 0);
+        for (int r = 0; r < m->ptab_rows; ++r) {
+            const int p = m->row_param[r];
+            const uint2 b = rng[r];
+            const bool finite = (b.x & 0x7F800000u) != 0x7F800000u;
+            if (b.x != b.y || !finite || (state[p] == 1 && bits[p] != b.x)) state[p] = 2;
+            else if (state[p] == 0) {
+                state[p] = 1;
+                bits[p] = b.x;
+            }
+        }
+        for (int p = 0; p < m->n_params; ++p)
+            if (state[p] == 1) {
+                float v;
+                std::memcpy(&v, &bits[p], 4);
+                folds.emplace_back(p, v);
+            }
+    }
+    const bool changed = folds != s->folds;
+    s->folds = std::move(folds);
+    if (changed && s->initialized) return sim_upload_nodes(s);
+    return NGPU_OK;
+}
+
 int ngpu_sim_set_params(ngpu_sim* s, const float* params, int32_t on_device) {
     if (!s || !params) return fail(NGPU_E_INVALID, "null sim or params");
     const ngpu_model* m = s->m;
@@ -1016,7 +1066,7 @@ int ngpu_sim_set_params(ngpu_sim* s, const float* params, int32_t on_device) {
     }
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("param gather: ") + cudaGetErrorString(e));
     s->has_params = true;
-    return NGPU_OK;
+    return sim_find_folds(s);
 }
 
 int ngpu_sim_set_stimulus(ngpu_sim* s, int32_t nt, const float* amps, const float* dts,
@@ -1088,7 +1138,6 @@ static std::vector<uint32_t> model_masks(const ngpu_model* m) {
 // Node records with this run's split, recording columns and mechanism
 // classes, uploaded to the device.  In FP32 the classes follow the
 // runtime-specialised kernels of the simulation's batch, or its own.
-static int sim_upload_nodes(ngpu_sim* s);
 
 // Host side of an initialisation: node records, the trace buffer (kept when
 // its size is unchanged, so the device addresses a captured graph holds stay
@@ -1163,7 +1212,7 @@ static int sim_upload_nodes(ngpu_sim* s) {
         else
             s->jit = ngpu_jit::module(m->mechset, s->precision == NGPU_FP64,
                                       ngpu_jit::pick_masks(model_masks(m), kMaxClasses), gs ? &gs->source : nullptr,
-                                      s->ch_prefetch);
+                                      s->ch_prefetch, s->folds);
         if (gs && !s->jit)
             return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
                                          "' runs only through runtime compilation: " + ngpu_jit::last_log());
@@ -1513,6 +1562,12 @@ int ngpu_sim_features(ngpu_sim* s, int32_t site, double dt, double stim_on, doub
     a.threshold = threshold;
     a.out = out_dev;
     return launch_features(a, (cudaStream_t)cuda_stream);
+}
+
+int ngpu_sim_param_folds(const ngpu_sim* s, int32_t* n_folds) {
+    if (!s || !n_folds) return fail(NGPU_E_INVALID, "null argument");
+    *n_folds = (s->jit && !s->batch) ? (int32_t)s->folds.size() : 0;
+    return NGPU_OK;
 }
 
 int ngpu_sim_classes(const ngpu_sim* s, int32_t* n_classes) {

@@ -36,6 +36,16 @@
 
 namespace ngpu_jit {
 
+// Parameters compiled in as constants: (index in the mechanism set, value).
+using Folds = std::vector<std::pair<int, float>>;
+
+// The literal of a float, exact (hexadecimal).
+inline std::string float_literal(float v) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%af", (double)v);
+    return buf;
+}
+
 struct Module {
     int mechset = 0;
     bool fp64 = false;
@@ -106,14 +116,24 @@ inline bool enabled() {
 // batch) over `masks`.  ms: the kernel template's mechanism set (0 TTPC,
 // 1 Mainen, 2 a generated set, whose channel code comes in as the extra
 // header ngpu_generated.cuh).  prefetch: the channel pass's L2 prefetch.
-inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks, bool prefetch = true) {
+inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks, bool prefetch = true,
+                          const Folds& folds = {}) {
     std::string list;
     for (size_t k = 0; k < masks.size(); ++k) list += (k ? ", " : "") + std::to_string(masks[k]) + "u";
     const std::string m = std::to_string(ms);
     const std::string R = fp64 ? "double" : "float";
     const std::string lb = "__launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)";
+    std::string fold;
+    if (!folds.empty()) {
+        fold = "#include \"param_fold.cuh\"\nnamespace ngpu {\n";
+        for (const auto& f : folds)
+            fold += "template <> struct ParamFold<" + std::to_string(f.first) +
+                    "> { static constexpr bool on = true; static constexpr float v = " + float_literal(f.second) +
+                    "; };\n";
+        fold += "}\n";
+    }
     return std::string(ms == 2 ? "#define NGPU_GENERATED_NODE 1\n" : "") +
-           std::string(prefetch ? "" : "#define NGPU_CH_PREFETCH 0\n") +
+           std::string(prefetch ? "" : "#define NGPU_CH_PREFETCH 0\n") + fold +
            "#include \"sim_kernels.cuh\"\n"
            "using JitClasses = ngpu::MaskList<" + list + ">;\n"
            "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps)\n"
@@ -161,13 +181,14 @@ inline std::string cache_dir() {
 // through the on-disk cache.  Touches no device.  generated: the channel
 // code of a generated mechanism set (ms 2), or nullptr.
 inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, const std::string* generated,
-                        const std::string& arch, std::vector<char>* out, std::string* err, bool prefetch = true) {
+                        const std::string& arch, std::vector<char>* out, std::string* err, bool prefetch = true,
+                        const Folds& folds = {}) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) {
         *err = last_log();
         return false;
     }
-    const std::string src = source(ms, fp64, masks, prefetch);
+    const std::string src = source(ms, fp64, masks, prefetch, folds);
     std::vector<std::string> opt_s = {"--gpu-architecture=sm_" + arch, "-std=c++17",
                                       "-lineinfo"};
     int vmaj = 0, vmin = 0;
@@ -253,7 +274,7 @@ inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, c
 // compilation is off or fails.  mechset >= 2 is a generated set whose channel
 // code is *generated.  Modules live until the process exits.
 inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>& masks,
-                            const std::string* generated, bool prefetch = true) {
+                            const std::string* generated, bool prefetch = true, const Folds& folds = {}) {
     if (!generated && (!enabled() || masks.empty())) return nullptr;
     if (generated && !enabled()) {
         last_log() = "runtime compilation is off (NGPU_JIT=0)";
@@ -263,6 +284,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     static std::map<std::string, std::unique_ptr<Module>> cache;
     std::string key = std::to_string(mechset) + (fp64 ? "d" : "f") + (prefetch ? "p:" : "n:");
     for (uint32_t m : masks) key += std::to_string(m) + ",";
+    for (const auto& f : folds) key += ";" + std::to_string(f.first) + "=" + float_literal(f.second);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second.get();
     int dev = 0, maj = 0, min = 0;
@@ -280,7 +302,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     std::vector<char> cubin;
     std::string err;
     const std::string arch = std::to_string(maj) + std::to_string(min) + "a";
-    if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err, prefetch)) {
+    if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err, prefetch, folds)) {
         last_log() = err;
         cache[key] = nullptr;
         return nullptr;

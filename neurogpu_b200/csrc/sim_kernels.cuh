@@ -874,6 +874,34 @@ __global__ void k_gather_params(const float* __restrict__ params, const int* __r
     }
 }
 
+// Per parameter-table row: the smallest and largest bit pattern over every
+// instance (equal: one value, the same bits, in every parameter set).
+__global__ void __launch_bounds__(256) k_ptab_range(const float* __restrict__ ptab, int ptab_rows, int n_groups,
+                                                    uint2* __restrict__ out) {
+    __shared__ unsigned lo_s[8], hi_s[8];
+    const int row = blockIdx.x;
+    unsigned lo = 0xFFFFFFFFu, hi = 0u;
+    for (int t = threadIdx.x; t < n_groups * kLanes; t += blockDim.x) {
+        const unsigned b = __float_as_uint(ptab[((size_t)(t >> 5) * ptab_rows + row) * kLanes + (t & 31)]);
+        lo = min(lo, b);
+        hi = max(hi, b);
+    }
+    lo = __reduce_min_sync(0xFFFFFFFFu, lo);
+    hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        lo_s[threadIdx.x >> 5] = lo;
+        hi_s[threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            lo = min(lo, lo_s[w]);
+            hi = max(hi, hi_s[w]);
+        }
+        out[row] = make_uint2(lo, hi);
+    }
+}
+
 // out[inst][rec][sample] <- trace[sample][rec][inst], tiled through shared memory.
 __global__ void k_trace_transpose(const float* __restrict__ trace, int n_samples, int n_rec,
                                   int n_inst_pad, int n_inst, float* __restrict__ out) {

@@ -193,6 +193,13 @@ class Simulator:
             C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
         return out
 
+    def param_folds(self) -> int:
+        """Parameters compiled into this simulation's kernel as constants
+        (after init; see ngpu_sim_param_folds)."""
+        n = C.c_int32()
+        _ffi.check("ngpu_sim_param_folds", _ffi.lib().ngpu_sim_param_folds(self._h, C.byref(n)))
+        return n.value
+
     def classes(self) -> int:
         """Mechanism masks compiled into the kernel that runs this simulation
         (0: the ahead-of-time kernel, generic channel code); after init()."""

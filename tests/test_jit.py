@@ -89,3 +89,73 @@ def test_specialised_kernel_matches_generic(ngpu_built, name):
     assert mismatched == 0
     assert err <= 0.05
     assert sub <= 0.01
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,min_folds", [("ttpc_like", 4), ("hh_active", 15)])
+def test_folded_parameters_match_loaded(ngpu_built, monkeypatch, name, min_folds):
+    """Parameters that hold one value in every set and section (the models'
+    kinetic constants) are compiled in as constants; the traces match those
+    of the kernel that loads them, within the FP32 parity bounds (a constant
+    lets the compiler evaluate an expression once, in its own rounding)."""
+    from neurogpu_b200 import configs
+    from neurogpu_b200.sim import Simulator
+    w = getattr(configs, name)(n_sets=16, t_stop=150.0)
+
+    def run(fold):
+        monkeypatch.setenv("NGPU_PARAM_FOLD", "1" if fold else "0")
+        sim = Simulator(w.cell, w.n_sets, w.n_stim, "fp32")
+        sim.set_params(w.params)
+        sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+        sim.set_recording(w.rec_nodes)
+        sim.init(w.v_init)
+        sim.advance(0, w.nt)
+        out, n, bad = sim.trace(), sim.param_folds(), sim.n_bad()
+        sim.close()
+        return out, n, bad
+    folded, n_f, bad_f = run(True)
+    loaded, n_l, bad_l = run(False)
+    assert n_f >= min_folds and n_l == 0
+    assert bad_f == 0 and bad_l == 0
+    err, mismatched = spike_time_error(folded, loaded, float(w.dt))
+    sub = subthreshold_error(folded, loaded, float(w.dt))
+    print(f"{name}: {n_f} parameters folded; spike times {err:.2e} ms, subthreshold {sub:.2e} mV")
+    assert mismatched == 0 and err <= 0.05 and sub <= 0.01
+
+
+@pytest.mark.gpu
+def test_new_parameters_mid_run_reselect_the_kernel(ngpu_built, monkeypatch):
+    """set_params in the middle of a run with values that change which
+    parameters are uniform: e_pas, compiled in as one constant at first, is
+    then given a different value per set.  The rest of the run uses the new
+    values (a kernel that kept the old constant would miss by millivolts):
+    it matches the same run with folding off within the FP32 parity bounds."""
+    from neurogpu_b200 import configs
+    from neurogpu_b200.sim import Simulator
+    w = configs.hh_active(n_sets=8, t_stop=100.0)
+    p2 = w.params.copy()
+    p2[:, w.cell.mechset.param_index("e_pas"), :] += np.linspace(-3.0, 3.0, w.n_sets, dtype=np.float32)[:, None]
+    k = w.nt // 2
+
+    def run(fold):
+        monkeypatch.setenv("NGPU_PARAM_FOLD", "1" if fold else "0")
+        sim = Simulator(w.cell, w.n_sets, w.n_stim, "fp32")
+        sim.set_params(w.params)
+        sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+        sim.set_recording(w.rec_nodes)
+        sim.init(w.v_init)
+        n0 = sim.param_folds()
+        sim.advance(0, k)
+        sim.set_params(p2)
+        n1 = sim.param_folds()
+        sim.advance(k, w.nt - k)
+        out = sim.trace()
+        assert sim.n_bad() == 0
+        sim.close()
+        return out, n0, n1
+    a, n0, n1 = run(True)
+    c, m0, m1 = run(False)
+    assert n1 == n0 - 1 and n0 > 0 and m0 == m1 == 0
+    err, mismatched = spike_time_error(a, c, float(w.dt))
+    sub = subthreshold_error(a, c, float(w.dt))
+    assert mismatched == 0 and err <= 0.05 and sub <= 0.01, (err, sub)
