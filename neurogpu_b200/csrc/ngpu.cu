@@ -992,8 +992,11 @@ static int sim_upload_nodes(ngpu_sim* s);
 
 // Parameters with one value (the same bits) in every parameter set and every
 // section whose nodes use them: the runtime-specialised kernel compiles them
-// in (param_fold.cuh).  Only where that kernel runs (FP32, built-in sets, not
-// in a batch, runtime compilation on, NGPU_PARAM_FOLD not 0).  New values
+// in (param_fold.cuh).  Only for the built-in sets in FP32, not in a batch,
+// with runtime compilation on and NGPU_PARAM_FOLD not 0: generated sets read
+// every parameter (their kernels spill at the register cap, and folding moved
+// the spills: the TTPC set generated from its .mod files ran 8 % slower
+// folded).  New values
 // after initialisation re-select the kernel before the next launch.
 static int sim_find_folds(ngpu_sim* s) {
     const ngpu_model* m = s->m;

@@ -1095,6 +1095,7 @@ def _emit_set(mechs, mech_params, params, celsius, ktf, reversal, cao, constants
     w("// Generated by neurogpu_b200/nmodl.py from NMODL mechanism files; do not edit.")
     w("#pragma once")
     w('#include "ngpu_math.cuh"')
+    w('#include "param_fold.cuh"')
     w("namespace ngpu {")
     w("template <typename R> NGPU_HD R ngpu_sgn(R x) { return x > (R)0 ? (R)1 : (x < (R)0 ? (R)-1 : (R)0); }")
     w("// cnexp over dt with the gate's rate 1/tau: x + (1 - exp(-dt rate)) (xinf - x)")
@@ -1188,7 +1189,7 @@ def _emit_set(mechs, mech_params, params, celsius, ktf, reversal, cao, constants
         w(f"            s += {n};")
         for j, pi in enumerate(mech_params[k]):
             pn = params[pi][: -(len(m.suffix) + 1)]
-            w(f"            {env[pn]} = (R)pr[(q + {j}) * S];")
+            w(f"            {env[pn]} = pload<R, {pi}>(pr, q + {j});  // a constant where folded")
         w(f"            q += {len(mech_params[k])};")
         w("        }")
     w("    }")
