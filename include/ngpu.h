@@ -246,6 +246,13 @@ int ngpu_sim_classes(const ngpu_sim *s, int32_t *n_classes);
  * The reference compiles its model's GLOBAL parameters into its generated
  * channel code in the same way (AllModels.cu). */
 int ngpu_sim_param_folds(const ngpu_sim *s, int32_t *n_folds);
+/* Parameter rows per group of 32 instances that the kernels read, and the
+ * rows the table holds: set_params lets the nodes of a section whose
+ * parameter values (every row, every instance) repeat another section's of
+ * the same mechanism combination read that section's rows, so only distinct
+ * rows are touched (NGPU_PARAM_DEDUP=0 keeps every section's own).  No
+ * counterpart in the reference, which stores parameters per compartment. */
+int ngpu_sim_param_rows(const ngpu_sim *s, int32_t *rows_read, int32_t *rows_total);
 int ngpu_jit_build(int32_t mechset, int32_t precision, const uint32_t *masks, int32_t n_masks,
                    int32_t cc_major, int32_t cc_minor, int64_t *cubin_bytes);
 const char *ngpu_jit_log(void);

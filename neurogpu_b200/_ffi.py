@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
             "ngpu_sim_trace_device": (C.c_int, [P, P, P]),
             "ngpu_sim_classes": (C.c_int, [P, P]),
             "ngpu_sim_param_folds": (C.c_int, [P, P]),
+            "ngpu_sim_param_rows": (C.c_int, [P, P, P]),
             "ngpu_trace_features": (C.c_int, [P, I64, I64, I32, I32, C.c_double, C.c_double, C.c_double, F32, P, P]),
             "ngpu_sim_features": (C.c_int, [P, I32, C.c_double, C.c_double, C.c_double, F32, P, P]),
             "ngpu_jit_build": (C.c_int, [I32, I32, P, I32, I32, I32, P]),

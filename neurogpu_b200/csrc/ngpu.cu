@@ -422,6 +422,8 @@ struct ngpu_sim {
     int items_per_warp = 2;       // work items per warp in the tree split
     ngpu_jit::Folds folds;        // parameters the runtime-specialised kernel compiles in
     uint2* d_prange = nullptr;    // [ptab_rows] bit-pattern range of each parameter row
+    unsigned long long* d_phash = nullptr;  // [ptab_rows] hash of each parameter row
+    std::vector<int32_t> prow_canon;  // parameter block start -> the block it reads (identical values)
     bool ch_prefetch = true;      // the runtime-specialised kernel compiles the channel-pass L2 prefetch in
 };
 
@@ -867,7 +869,8 @@ static void sim_free(ngpu_sim* s) {
     if (!s) return;
     void* ptrs[] = {s->d_nodes, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc, s->d_jx,
                     s->d_inst_stim, s->d_bad, s->d_err, s->d_row_param, s->d_row_sec, s->d_amps,
-                    s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv, s->d_prange};
+                    s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv, s->d_prange,
+                    s->d_phash};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete s;
@@ -998,6 +1001,73 @@ static int sim_upload_nodes(ngpu_sim* s);
 // the spills: the TTPC set generated from its .mod files ran 8 % slower
 // folded).  New values
 // after initialisation re-select the kernel before the next launch.
+// Parameter blocks (the rows of one section and mechanism combination) that
+// hold the same values at every instance as another block of the same
+// combination: their nodes read that block's rows instead.  A fit gives its
+// parameters per region, so most sections repeat another section's values;
+// sharing shrinks the parameter rows the kernels touch (TTPC-like cell: 1788
+// rows per group of 32 instances) to the distinct ones, which stay in cache.
+// The values read are the same bits, so results are unchanged.  Candidates
+// are grouped by a hash of each row and confirmed by an exact comparison on
+// the device.  NGPU_PARAM_DEDUP=0 turns it off.
+static int sim_share_param_blocks(ngpu_sim* s, std::vector<int32_t>* canon_out) {
+    const ngpu_model* m = s->m;
+    canon_out->clear();
+    const char* ev = getenv("NGPU_PARAM_DEDUP");
+    if ((ev && ev[0] == '0') || m->ptab_rows < 2) return NGPU_OK;
+    int rc = NGPU_OK;
+    if (!s->d_phash) {
+        s->d_phash = (unsigned long long*)dmalloc(sizeof(unsigned long long) * m->ptab_rows, &rc);
+        if (!s->d_phash) return rc;
+    }
+    k_ptab_hash<<<m->ptab_rows, 256>>>(s->d_ptab, m->ptab_rows, s->n_groups, s->d_phash);
+    g_launches++;
+    std::vector<unsigned long long> h(m->ptab_rows);
+    NGPU_CUDA(cudaMemcpy(h.data(), s->d_phash, sizeof(h[0]) * m->ptab_rows, cudaMemcpyDeviceToHost));
+    // blocks: first row -> (rows, mask), from the nodes that read them
+    std::map<int, std::pair<int, uint32_t>> blocks;
+    for (int i = 0; i < m->n; ++i)
+        if (m->rows[i].y > 0) blocks[m->info[i].prow] = {m->rows[i].y, m->mask[i]};
+    std::map<std::vector<unsigned long long>, int> first;   // (mask, rows, row hashes) -> first block
+    std::vector<int3> pairs;
+    for (const auto& b : blocks) {
+        std::vector<unsigned long long> key = {b.second.second, (unsigned long long)b.second.first};
+        key.insert(key.end(), h.begin() + b.first, h.begin() + b.first + b.second.first);
+        auto it = first.find(key);
+        if (it == first.end()) first.emplace(std::move(key), b.first);
+        else pairs.push_back(make_int3(it->second, b.first, b.second.first));
+    }
+    if (pairs.empty()) return NGPU_OK;
+    int3* d_pairs = (int3*)dmalloc(sizeof(int3) * pairs.size(), &rc);
+    if (!d_pairs) return rc;
+    int* d_same = (int*)dmalloc(sizeof(int) * pairs.size(), &rc);
+    if (!d_same) {
+        cudaFree(d_pairs);
+        return rc;
+    }
+    std::vector<int> same(pairs.size(), 0);
+    cudaError_t e = cudaMemcpy(d_pairs, pairs.data(), sizeof(int3) * pairs.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_ptab_blocks_equal<<<(unsigned)pairs.size(), 256>>>(s->d_ptab, m->ptab_rows, s->n_groups, d_pairs, d_same);
+        g_launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(same.data(), d_same, sizeof(int) * pairs.size(), cudaMemcpyDeviceToHost);
+    cudaFree(d_pairs);
+    cudaFree(d_same);
+    if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("parameter blocks: ") + cudaGetErrorString(e));
+    std::vector<int32_t> canon(m->ptab_rows);
+    for (int r = 0; r < m->ptab_rows; ++r) canon[r] = r;
+    bool any = false;
+    for (size_t k = 0; k < pairs.size(); ++k)
+        if (same[k]) {
+            canon[pairs[k].y] = pairs[k].x;
+            any = true;
+        }
+    if (any) *canon_out = std::move(canon);
+    return NGPU_OK;
+}
+
 static int sim_find_folds(ngpu_sim* s) {
     const ngpu_model* m = s->m;
     ngpu_jit::Folds folds;
@@ -1033,8 +1103,12 @@ static int sim_find_folds(ngpu_sim* s) {
                 folds.emplace_back(p, v);
             }
     }
-    const bool changed = folds != s->folds;
+    std::vector<int32_t> canon;
+    const int rc = sim_share_param_blocks(s, &canon);
+    if (rc != NGPU_OK) return rc;
+    const bool changed = folds != s->folds || canon != s->prow_canon;
     s->folds = std::move(folds);
+    s->prow_canon = std::move(canon);
     if (changed && s->initialized) return sim_upload_nodes(s);
     return NGPU_OK;
 }
@@ -1237,7 +1311,7 @@ static int sim_upload_nodes(ngpu_sim* s) {
             q.pslot = (int16_t)s->part.pslot[i];
             q.rec = (int16_t)rec[i];
             q.mask = (uint16_t)m->mask[i];
-            q.prow = (uint16_t)m->info[i].prow;
+            q.prow = (uint16_t)(s->prow_canon.empty() ? m->info[i].prow : s->prow_canon[m->info[i].prow]);
             q.srows = (uint8_t)m->rows[i].x;
             q.prows = (uint8_t)m->rows[i].y;
             q.cls = (uint8_t)ngpu_jit::class_of(s->jit, (uint32_t)m->mask[i], kGenericClass);
@@ -1565,6 +1639,20 @@ int ngpu_sim_features(ngpu_sim* s, int32_t site, double dt, double stim_on, doub
     a.threshold = threshold;
     a.out = out_dev;
     return launch_features(a, (cudaStream_t)cuda_stream);
+}
+
+int ngpu_sim_param_rows(const ngpu_sim* s, int32_t* rows_read, int32_t* rows_total) {
+    if (!s || !rows_read || !rows_total) return fail(NGPU_E_INVALID, "null argument");
+    const ngpu_model* m = s->m;
+    std::map<int, int> used;   // block start the nodes read -> its rows
+    for (int i = 0; i < m->n; ++i)
+        if (m->rows[i].y > 0)
+            used[s->prow_canon.empty() ? m->info[i].prow : s->prow_canon[m->info[i].prow]] = m->rows[i].y;
+    int n = 0;
+    for (const auto& u : used) n += u.second;
+    *rows_read = n;
+    *rows_total = m->ptab_rows;
+    return NGPU_OK;
 }
 
 int ngpu_sim_param_folds(const ngpu_sim* s, int32_t* n_folds) {

@@ -902,6 +902,54 @@ __global__ void __launch_bounds__(256) k_ptab_range(const float* __restrict__ pt
     }
 }
 
+// Per parameter-table row: a hash of its values at every instance (the sum
+// of a 64-bit mix of each (instance, bit pattern) pair: position-aware and
+// independent of the summation order).  Equal rows hash alike; rows that
+// hash alike are compared exactly (k_ptab_blocks_equal) before they share.
+__device__ __forceinline__ uint64_t ptab_mix(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    return x ^ (x >> 33);
+}
+
+__global__ void __launch_bounds__(256) k_ptab_hash(const float* __restrict__ ptab, int ptab_rows, int n_groups,
+                                                   unsigned long long* __restrict__ out) {
+    __shared__ unsigned long long part[8];
+    const int row = blockIdx.x;
+    unsigned long long h = 0;
+    for (int t = threadIdx.x; t < n_groups * kLanes; t += blockDim.x) {
+        const unsigned b = __float_as_uint(ptab[((size_t)(t >> 5) * ptab_rows + row) * kLanes + (t & 31)]);
+        h += ptab_mix(((uint64_t)t << 32) | b);
+    }
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xFFFFFFFFu, h, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = h;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) h += part[w];
+        out[row] = h;
+    }
+}
+
+// pairs[k] = (first row of block a, first row of block b, rows): same[k] = 1
+// when the two blocks hold the same bits at every instance, else 0
+__global__ void __launch_bounds__(256) k_ptab_blocks_equal(const float* __restrict__ ptab, int ptab_rows,
+                                                           int n_groups, const int3* __restrict__ pairs,
+                                                           int* __restrict__ same) {
+    const int3 pr = pairs[blockIdx.x];
+    int diff = 0;
+    for (int r = 0; r < pr.z && !diff; ++r)
+        for (int t = threadIdx.x; t < n_groups * kLanes; t += blockDim.x) {
+            const size_t g = (size_t)(t >> 5) * ptab_rows;
+            const unsigned x = __float_as_uint(ptab[(g + pr.x + r) * kLanes + (t & 31)]);
+            const unsigned y = __float_as_uint(ptab[(g + pr.y + r) * kLanes + (t & 31)]);
+            diff |= x != y;
+        }
+    diff = __syncthreads_or(diff);
+    if (threadIdx.x == 0) same[blockIdx.x] = !diff;
+}
+
 // out[inst][rec][sample] <- trace[sample][rec][inst], tiled through shared memory.
 __global__ void k_trace_transpose(const float* __restrict__ trace, int n_samples, int n_rec,
                                   int n_inst_pad, int n_inst, float* __restrict__ out) {

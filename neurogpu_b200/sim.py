@@ -200,6 +200,13 @@ class Simulator:
         _ffi.check("ngpu_sim_param_folds", _ffi.lib().ngpu_sim_param_folds(self._h, C.byref(n)))
         return n.value
 
+    def param_rows(self) -> tuple[int, int]:
+        """(parameter rows the kernels read, rows the table holds) per group of
+        32 instances; see ngpu_sim_param_rows."""
+        a, b = C.c_int32(), C.c_int32()
+        _ffi.check("ngpu_sim_param_rows", _ffi.lib().ngpu_sim_param_rows(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def classes(self) -> int:
         """Mechanism masks compiled into the kernel that runs this simulation
         (0: the ahead-of-time kernel, generic channel code); after init()."""

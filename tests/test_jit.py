@@ -159,3 +159,35 @@ def test_new_parameters_mid_run_reselect_the_kernel(ngpu_built, monkeypatch):
     err, mismatched = spike_time_error(a, c, float(w.dt))
     sub = subthreshold_error(a, c, float(w.dt))
     assert mismatched == 0 and err <= 0.05 and sub <= 0.01, (err, sub)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,precision,frac", [("ttpc_like", "fp32", 0.8), ("hh_active", "fp32", 0.1),
+                                                 ("ttpc_like", "fp64", 0.8)])
+def test_shared_parameter_blocks_are_bitwise_neutral(ngpu_built, monkeypatch, name, precision, frac):
+    """Sections whose parameter values repeat another section's read that
+    section's rows: fewer rows are touched (the HH cell's values are per
+    region; the TTPC-like cell's Ih and calcium densities vary with
+    distance, section by section) and the traces are bitwise those of every
+    section reading its own rows."""
+    from neurogpu_b200 import configs
+    from neurogpu_b200.sim import Simulator
+    w = getattr(configs, name)(n_sets=16, t_stop=60.0)
+
+    def run(dedup):
+        monkeypatch.setenv("NGPU_PARAM_DEDUP", "1" if dedup else "0")
+        sim = Simulator(w.cell, w.n_sets, w.n_stim, precision)
+        sim.set_params(w.params)
+        sim.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+        sim.set_recording(w.rec_nodes)
+        sim.init(w.v_init)
+        sim.advance(0, w.nt)
+        out, rows = sim.trace(), sim.param_rows()
+        assert sim.n_bad() == 0
+        sim.close()
+        return out, rows
+    shared, (read_s, total) = run(True)
+    own, (read_o, total_o) = run(False)
+    print(f"{name} {precision}: parameter rows read {read_s} of {total}")
+    assert read_o == total_o == total and read_s < frac * total
+    assert np.array_equal(shared, own)
