@@ -1068,11 +1068,16 @@ static int sim_share_param_blocks(ngpu_sim* s, std::vector<int32_t>* canon_out) 
     return NGPU_OK;
 }
 
+extern "C++" {  // defined with the batch, outside this C-linkage block
+static const ngpu_jit::Folds& batch_folds(const ngpu_batch* b);
+static int batch_refold(ngpu_batch* b);
+}
+
 static int sim_find_folds(ngpu_sim* s) {
     const ngpu_model* m = s->m;
     ngpu_jit::Folds folds;
     const char* ev = getenv("NGPU_PARAM_FOLD");
-    const bool on = s->precision == NGPU_FP32 && !gen_set(m->mechset) && !s->batch && ngpu_jit::enabled() &&
+    const bool on = s->precision == NGPU_FP32 && !gen_set(m->mechset) && ngpu_jit::enabled() &&
                     !(ev && ev[0] == '0') && m->ptab_rows > 0;
     if (on) {
         if (!s->d_prange) {
@@ -1109,6 +1114,12 @@ static int sim_find_folds(ngpu_sim* s) {
     const bool changed = folds != s->folds || canon != s->prow_canon;
     s->folds = std::move(folds);
     s->prow_canon = std::move(canon);
+    if (s->batch) {  // the batch's kernel folds what its members share: still true for this member?
+        bool holds = true;
+        for (const auto& x : batch_folds(s->batch))
+            if (std::find(s->folds.begin(), s->folds.end(), x) == s->folds.end()) holds = false;
+        if (!holds) return batch_refold(s->batch);
+    }
     if (changed && s->initialized) return sim_upload_nodes(s);
     return NGPU_OK;
 }
@@ -1278,7 +1289,42 @@ struct ngpu_batch {
     int graph_kernels = 0;  // kernels one replay launches
     // runtime-specialised kernels over the members' masks (nullptr: ahead of time)
     const ngpu_jit::Module* jit = nullptr;
+    ngpu_jit::Folds folds;  // parameters every member holds at one, the same, value
 };
+
+// The folds that hold for every member (same parameter, same value).
+static ngpu_jit::Folds batch_common_folds(const ngpu_batch* b) {
+    if (b->precision != NGPU_FP32 || gen_set(b->mechset) || b->sims.empty()) return {};
+    ngpu_jit::Folds out = b->sims[0]->folds;
+    for (size_t k = 1; k < b->sims.size(); ++k) {
+        const ngpu_jit::Folds& f = b->sims[k]->folds;
+        ngpu_jit::Folds keep;
+        for (const auto& x : out)
+            if (std::find(f.begin(), f.end(), x) != f.end()) keep.push_back(x);
+        out.swap(keep);
+    }
+    return out;
+}
+
+static const ngpu_jit::Folds& batch_folds(const ngpu_batch* b) { return b->folds; }
+static void batch_drop_graph(ngpu_batch* b);
+static int batch_select_kernels(ngpu_batch* b);
+
+// A member's new parameter values break a fold of the batch's kernel: fold
+// what every member still shares, select that kernel, drop the captured run
+// (it holds the old kernel) and re-upload the initialised members' records.
+static int batch_refold(ngpu_batch* b) {
+    b->folds = batch_common_folds(b);
+    batch_drop_graph(b);
+    const int rc = batch_select_kernels(b);
+    if (rc != NGPU_OK) return rc;
+    for (ngpu_sim* t : b->sims)
+        if (t->initialized) {
+            const int r2 = sim_upload_nodes(t);
+            if (r2 != NGPU_OK) return r2;
+        }
+    return NGPU_OK;
+}
 
 static int sim_upload_nodes(ngpu_sim* s) {
     const ngpu_model* m = s->m;
@@ -1397,6 +1443,27 @@ static void batch_drop_graph(ngpu_batch* b) {
     b->graph_key.clear();
 }
 
+// One specialised kernel over every member's masks, with the parameters all
+// members share compiled in (FP32, or a generated set in either precision).
+static int batch_select_kernels(ngpu_batch* b) {
+    b->jit = nullptr;
+    const GenSet* gs = gen_set(b->mechset);
+    if (b->precision != NGPU_FP32 && !gs) return NGPU_OK;
+    std::vector<uint32_t> all;
+    int64_t pf_ctas = 0;  // the prefetch follows the members that hold most of the CTAs
+    for (ngpu_sim* s : b->sims) {
+        const std::vector<uint32_t> mm = model_masks(s->m);
+        all.insert(all.end(), mm.begin(), mm.end());
+        pf_ctas += s->ch_prefetch ? s->n_groups : -s->n_groups;
+    }
+    b->jit = ngpu_jit::module(b->mechset, b->precision == NGPU_FP64, ngpu_jit::pick_masks(all, kMaxClasses),
+                              gs ? &gs->source : nullptr, pf_ctas >= 0, b->folds);
+    if (gs && !b->jit)
+        return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
+                                     "' runs only through runtime compilation: " + ngpu_jit::last_log());
+    return NGPU_OK;
+}
+
 extern "C" {
 
 int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
@@ -1428,21 +1495,12 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
                                                              : SmemPlan<float>::bytes(s->m->n, ns, s->s2_stage));
     }
     b->threads = kLanes * W;
-    const GenSet* gs = gen_set(b->mechset);
-    if (b->precision == NGPU_FP32 || gs) {  // one specialised kernel over every member's masks
-        std::vector<uint32_t> all;
-        int64_t pf_ctas = 0;   // the prefetch follows the members that hold most of the CTAs
-        for (ngpu_sim* s : b->sims) {
-            const std::vector<uint32_t> mm = model_masks(s->m);
-            all.insert(all.end(), mm.begin(), mm.end());
-            pf_ctas += s->ch_prefetch ? s->n_groups : -s->n_groups;
-        }
-        b->jit = ngpu_jit::module(b->mechset, b->precision == NGPU_FP64, ngpu_jit::pick_masks(all, kMaxClasses),
-                                  gs ? &gs->source : nullptr, pf_ctas >= 0);
-        if (gs && !b->jit) {
+    b->folds = batch_common_folds(b);
+    {
+        const int rc = batch_select_kernels(b);
+        if (rc != NGPU_OK) {
             delete b;
-            return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
-                                         "' runs only through runtime compilation: " + ngpu_jit::last_log());
+            return rc;
         }
     }
     for (ngpu_sim* s : b->sims) {
@@ -1657,7 +1715,7 @@ int ngpu_sim_param_rows(const ngpu_sim* s, int32_t* rows_read, int32_t* rows_tot
 
 int ngpu_sim_param_folds(const ngpu_sim* s, int32_t* n_folds) {
     if (!s || !n_folds) return fail(NGPU_E_INVALID, "null argument");
-    *n_folds = (s->jit && !s->batch) ? (int32_t)s->folds.size() : 0;
+    *n_folds = s->batch ? (int32_t)s->batch->folds.size() : (s->jit ? (int32_t)s->folds.size() : 0);
     return NGPU_OK;
 }
 

@@ -32,15 +32,14 @@ def _sims(workloads, warps=(0, 0, 0, 0), precision="fp32"):
 
 def test_batch_equals_separate_launches(ngpu_built, workloads, monkeypatch):
     """One launch over four morphologies with different warp counts gives
-    bitwise the traces of four separate launches.  A batch's kernel compiles
-    no parameters in as constants, so the separate launches run without
-    folding too."""
+    bitwise the traces of four separate launches.  A batch folds only the
+    parameters its members share, a single launch every uniform one, so both
+    sides run without folding here (folded batches: the tests below)."""
     from neurogpu_b200.sim import Batch
     warps = (2, 4, 6, 8)
     ref = []
     monkeypatch.setenv("NGPU_PARAM_FOLD", "0")
     sims0 = _sims(workloads, warps)
-    monkeypatch.delenv("NGPU_PARAM_FOLD")
     for s, w in zip(sims0, workloads):
         s.init(w.v_init)
         s.advance(0, 300)
@@ -58,6 +57,56 @@ def test_batch_equals_separate_launches(ngpu_built, workloads, monkeypatch):
         assert np.array_equal(got, r)
         assert s.n_bad() == 0
     b.close()
+
+
+def _batch_run(workloads, fold, monkeypatch, change=None):
+    from neurogpu_b200.sim import Batch
+    monkeypatch.setenv("NGPU_PARAM_FOLD", "1" if fold else "0")
+    sims = _sims(workloads)
+    b = Batch(sims)
+    if change is not None:  # new values for member 1 after the batch exists
+        sims[1].set_params(change)
+    n_folds = sims[0].param_folds()
+    b.init(workloads[0].v_init)
+    b.advance(0, workloads[0].nt)
+    out = [s.trace() for s in sims]
+    assert all(s.n_bad() == 0 for s in sims)
+    b.close()
+    for s in sims:
+        s.close()
+    return out, n_folds
+
+
+def _close(a, b, dt):
+    for x, y in zip(a, b):
+        err, mism = spike_time_error(x, y, dt)
+        sub = subthreshold_error(x, y, dt)
+        assert mism == 0 and err <= 0.05 and sub <= 0.01, (err, sub)
+
+
+def test_batch_folds_the_parameters_its_members_share(ngpu_built, workloads, monkeypatch):
+    """The batch's kernel compiles in the parameters that hold one value in
+    every member (the HH kinetic constants): within the FP32 parity bounds of
+    the batch that loads them."""
+    folded, n = _batch_run(workloads, True, monkeypatch)
+    loaded, n0 = _batch_run(workloads, False, monkeypatch)
+    assert n >= 15 and n0 == 0
+    _close(folded, loaded, float(workloads[0].dt))
+
+
+def test_member_with_new_values_refolds_the_batch(ngpu_built, workloads, monkeypatch):
+    """A member given new values after the batch exists (e_pas made to vary
+    by set) breaks one of the batch's folds: the batch's kernel is rebuilt
+    without it, and the run matches the unfolded batch on the same values
+    (a kernel that kept the old constant would miss by millivolts)."""
+    w = workloads[1]
+    p2 = w.params.copy()
+    p2[:, w.cell.mechset.param_index("e_pas"), :] += np.linspace(-3.0, 3.0, w.n_sets, dtype=np.float32)[:, None]
+    folded, n = _batch_run(workloads, True, monkeypatch, change=p2)
+    loaded, _ = _batch_run(workloads, False, monkeypatch, change=p2)
+    base, n_base = _batch_run(workloads, True, monkeypatch)
+    assert n == n_base - 1
+    _close(folded, loaded, float(w.dt))
 
 
 def test_graph_run_equals_batch(ngpu_built, workloads):
