@@ -50,6 +50,7 @@ struct Module {
     int mechset = 0;
     bool fp64 = false;
     bool prefetch = true;                   // channel-pass L2 prefetch compiled in (NGPU_CH_PREFETCH)
+    bool complete = false;                  // the masks cover every node: no generic path (NGPU_CLASSES_COMPLETE)
     std::vector<uint32_t> masks;            // class k runs the code for masks[k]
     cudaLibrary_t lib = nullptr;
     cudaKernel_t init = nullptr;           // (SimArgs<R>)
@@ -117,7 +118,7 @@ inline bool enabled() {
 // 1 Mainen, 2 a generated set, whose channel code comes in as the extra
 // header ngpu_generated.cuh).  prefetch: the channel pass's L2 prefetch.
 inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks, bool prefetch = true,
-                          const Folds& folds = {}) {
+                          const Folds& folds = {}, bool complete = false) {
     std::string list;
     for (size_t k = 0; k < masks.size(); ++k) list += (k ? ", " : "") + std::to_string(masks[k]) + "u";
     const std::string m = std::to_string(ms);
@@ -133,7 +134,8 @@ inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks,
         fold += "}\n";
     }
     return std::string(ms == 2 ? "#define NGPU_GENERATED_NODE 1\n" : "") +
-           std::string(prefetch ? "" : "#define NGPU_CH_PREFETCH 0\n") + fold +
+           std::string(prefetch ? "" : "#define NGPU_CH_PREFETCH 0\n") +
+           std::string(complete ? "#define NGPU_CLASSES_COMPLETE 1\n" : "") + fold +
            "#include \"sim_kernels.cuh\"\n"
            "using JitClasses = ngpu::MaskList<" + list + ">;\n"
            "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps)\n"
@@ -182,13 +184,13 @@ inline std::string cache_dir() {
 // code of a generated mechanism set (ms 2), or nullptr.
 inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, const std::string* generated,
                         const std::string& arch, std::vector<char>* out, std::string* err, bool prefetch = true,
-                        const Folds& folds = {}) {
+                        const Folds& folds = {}, bool complete = false) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) {
         *err = last_log();
         return false;
     }
-    const std::string src = source(ms, fp64, masks, prefetch, folds);
+    const std::string src = source(ms, fp64, masks, prefetch, folds, complete);
     std::vector<std::string> opt_s = {"--gpu-architecture=sm_" + arch, "-std=c++17",
                                       "-lineinfo"};
     int vmaj = 0, vmin = 0;
@@ -274,7 +276,8 @@ inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, c
 // compilation is off or fails.  mechset >= 2 is a generated set whose channel
 // code is *generated.  Modules live until the process exits.
 inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>& masks,
-                            const std::string* generated, bool prefetch = true, const Folds& folds = {}) {
+                            const std::string* generated, bool prefetch = true, const Folds& folds = {},
+                            bool complete = false) {
     if (!generated && (!enabled() || masks.empty())) return nullptr;
     if (generated && !enabled()) {
         last_log() = "runtime compilation is off (NGPU_JIT=0)";
@@ -282,7 +285,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     }
     std::lock_guard<std::mutex> lock(mu());
     static std::map<std::string, std::unique_ptr<Module>> cache;
-    std::string key = std::to_string(mechset) + (fp64 ? "d" : "f") + (prefetch ? "p:" : "n:");
+    std::string key = std::to_string(mechset) + (fp64 ? "d" : "f") + (prefetch ? "p" : "n") + (complete ? "c:" : "g:");
     for (uint32_t m : masks) key += std::to_string(m) + ",";
     for (const auto& f : folds) key += ";" + std::to_string(f.first) + "=" + float_literal(f.second);
     auto it = cache.find(key);
@@ -302,7 +305,8 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     std::vector<char> cubin;
     std::string err;
     const std::string arch = std::to_string(maj) + std::to_string(min) + "a";
-    if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err, prefetch, folds)) {
+    if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err, prefetch, folds,
+                     complete)) {
         last_log() = err;
         cache[key] = nullptr;
         return nullptr;
@@ -311,6 +315,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     mod->mechset = mechset;
     mod->fp64 = fp64;
     mod->prefetch = prefetch;
+    mod->complete = complete;
     mod->masks = masks;
     cudaError_t e = cudaLibraryLoadData(&mod->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->init, mod->lib, "ngpu_jit_init");

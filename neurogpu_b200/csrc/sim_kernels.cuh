@@ -164,7 +164,15 @@ __device__ __forceinline__ void channels_cls(int cls, uint32_t mk, R v, R dt, R*
     } else if constexpr (sizeof...(Ms) > 0) {
         channels_cls<R, MS, INIT, Ms...>(cls - 1, mk, v, dt, st, pr, I, G);
     } else {
+#if NGPU_CLASSES_COMPLETE
+        // every node's mask is one of the classes (the host compiles this only
+        // then): no node comes here, and the generic code's registers are not
+        // reserved for a path that never runs
+        I = (R)0;
+        G = (R)0;
+#else
         channels<R, MS, INIT>(mk, v, dt, st, pr, I, G);
+#endif
     }
 }
 template <typename R, int MS, bool INIT, uint32_t... Ms>
