@@ -242,7 +242,7 @@ int ngpu_sim_classes(const ngpu_sim *s, int32_t *n_classes);
 /* Parameters the simulation's runtime-specialised kernel compiles in as
  * constants (after init): those with one value in every parameter set and
  * every section that uses them, found by set_params; 0 where folding does
- * not apply (FP64, generated sets, NGPU_JIT=0 or NGPU_PARAM_FOLD=0).  For a
+ * not apply (the built-in sets in FP64, NGPU_JIT=0 or NGPU_PARAM_FOLD=0).  For a
  * member of a batch: those its batch's kernel compiles in, the parameters
  * every member holds at the same value.
  * The reference compiles its model's GLOBAL parameters into its generated

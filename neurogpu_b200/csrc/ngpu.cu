@@ -995,11 +995,9 @@ static int sim_upload_nodes(ngpu_sim* s);
 
 // Parameters with one value (the same bits) in every parameter set and every
 // section whose nodes use them: the runtime-specialised kernel compiles them
-// in (param_fold.cuh).  Only for the built-in sets in FP32, not in a batch,
-// with runtime compilation on and NGPU_PARAM_FOLD not 0: generated sets read
-// every parameter (their kernels spill at the register cap, and folding moved
-// the spills: the TTPC set generated from its .mod files ran 8 % slower
-// folded).  New values
+// in (param_fold.cuh).  Wherever that kernel runs (FP32, or a generated set
+// in either precision), with runtime compilation on and NGPU_PARAM_FOLD not
+// 0.  New values
 // after initialisation re-select the kernel before the next launch.
 // Parameter blocks (the rows of one section and mechanism combination) that
 // hold the same values at every instance as another block of the same
@@ -1077,7 +1075,7 @@ static int sim_find_folds(ngpu_sim* s) {
     const ngpu_model* m = s->m;
     ngpu_jit::Folds folds;
     const char* ev = getenv("NGPU_PARAM_FOLD");
-    const bool on = s->precision == NGPU_FP32 && !gen_set(m->mechset) && ngpu_jit::enabled() &&
+    const bool on = (s->precision == NGPU_FP32 || gen_set(m->mechset)) && ngpu_jit::enabled() &&
                     !(ev && ev[0] == '0') && m->ptab_rows > 0;
     if (on) {
         if (!s->d_prange) {
@@ -1307,7 +1305,7 @@ struct ngpu_batch {
 
 // The folds that hold for every member (same parameter, same value).
 static ngpu_jit::Folds batch_common_folds(const ngpu_batch* b) {
-    if (b->precision != NGPU_FP32 || gen_set(b->mechset) || b->sims.empty()) return {};
+    if ((b->precision != NGPU_FP32 && !gen_set(b->mechset)) || b->sims.empty()) return {};
     ngpu_jit::Folds out = b->sims[0]->folds;
     for (size_t k = 1; k < b->sims.size(); ++k) {
         const ngpu_jit::Folds& f = b->sims[k]->folds;
