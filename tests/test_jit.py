@@ -191,3 +191,51 @@ def test_shared_parameter_blocks_are_bitwise_neutral(ngpu_built, monkeypatch, na
     print(f"{name} {precision}: parameter rows read {read_s} of {total}")
     assert read_o == total_o == total and read_s < frac * total
     assert np.array_equal(shared, own)
+
+
+@pytest.mark.gpu
+def test_more_combinations_than_classes_match_the_oracle(ngpu_built, oracle):
+    """A cell whose sections carry random subsets of the TTPC mechanisms has
+    more distinct combinations than the 16 compiled classes: the other nodes
+    run the generic channel code inside the specialised kernel (which is then
+    compiled with it).  FP32 against the FP64 oracle within the parity
+    bounds."""
+    from dataclasses import replace
+
+    from neurogpu_b200 import configs
+    from neurogpu_b200.sim import Simulator
+    w = configs.ttpc_like(n_sets=8, t_stop=80.0)
+    ms = w.cell.mechset
+    rng = np.random.default_rng(12)
+    n_sec = w.cell.n_sections
+    sec_mask = (rng.random((ms.n_mech, n_sec)) < 0.45).astype(np.uint8)
+    sec_mask[ms.mech_index("pas")] = 1
+    ca = [ms.mech_index("Ca_HVA"), ms.mech_index("Ca_LVAst")]
+    sec_mask[ms.mech_index("CaDynamics_E2")] |= sec_mask[ca].max(axis=0)   # calcium currents need the pool
+    mask = sec_mask[:, np.asarray(w.cell.section)]
+    n_comb = len({tuple(c) for c in mask.T})
+    assert n_comb > 16
+    # the workload gives values only where a region has the mechanism (a calcium
+    # pool's decay is 0 elsewhere): kinetic and pool constants take the soma's
+    # values in every section
+    params = w.params.copy()
+    soma = int(w.cell.section[0])
+    for k, name in enumerate(ms.params):
+        if "bar" not in name:
+            params[:, k, :] = params[:, k, soma:soma + 1]
+    wc = replace(w, cell=replace(w.cell, mech_mask=np.ascontiguousarray(mask)), params=np.ascontiguousarray(params))
+    ref = oracle.run_workload(wc)
+    assert np.all(np.isfinite(ref))
+    sim = Simulator(wc.cell, wc.n_sets, wc.n_stim, "fp32")
+    sim.set_params(wc.params)
+    sim.set_stimulus(wc.amps, wc.dts, wc.stim_node, wc.stim_area)
+    sim.set_recording(wc.rec_nodes)
+    sim.init(wc.v_init)
+    sim.advance(0, wc.nt)
+    got = sim.trace().astype(np.float64)
+    assert sim.classes() == 16 and sim.n_bad() == 0
+    sim.close()
+    err, mism = spike_time_error(got, ref, float(wc.dt))
+    sub = subthreshold_error(got, ref, float(wc.dt))
+    print(f"{n_comb} mechanism combinations: spike times {err:.2e} ms, subthreshold {sub:.2e} mV")
+    assert mism == 0 and err <= 0.05 and sub <= 0.1
