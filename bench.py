@@ -162,13 +162,24 @@ def dist_setup(n_gpus: int):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The largest x over the ranks (a CUDA tensor under NCCL, a host one
+    otherwise)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def weak_scaling_rate(units_per_rank: float, seconds: float, world: int) -> tuple[float, float]:
+    """Whole-job rate of N replicas: every rank processed units_per_rank in
+    its own time, and the job lasts as long as the slowest rank.  Returns
+    (units of all ranks / slowest time, slowest time)."""
+    t = max_over_ranks(seconds, world)
+    return units_per_rank * world / t, t
 
 
 def barrier(world: int):
@@ -267,12 +278,13 @@ def run_uneven(args):
     stream.synchronize()
     launches = int(_ffi.lib().ngpu_launch_count(0))
     clk = clocks.stop() if clocks else None
-    el_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     cs = sum(w.cell.n_nodes * w.n_sets * w.n_stim for w in ws) * nt * args.steps
+    rate, el_s = weak_scaling_rate(cs, ev0.elapsed_time(ev1) / 1e3, world)
+    el_ms = el_s * 1e3
     bad = sum(s.n_bad() for s in sims)
     if rank == 0:
         print(json.dumps({
-            "metric": "compartment-steps/s (uneven batch x8192, 5 protocols)", "value": cs * world / (el_ms / 1e3),
+            "metric": "compartment-steps/s (uneven batch x8192, 5 protocols)", "value": rate,
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded)",
@@ -438,11 +450,11 @@ def main():
     launches = int(_ffi.lib().ngpu_launch_count(0))
     barrier(world)
     clk = clocks.stop() if clocks else None
-    el_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     per_launch_ms = float(np.mean([a.elapsed_time(b) for a, b in launch_ms]))
     n_bad = sim.n_bad()
     comp_steps_rank = w.cell.n_nodes * args.chunk * n_inst * args.steps
-    value = comp_steps_rank * world / (el_ms / 1e3)
+    value, el_s = weak_scaling_rate(comp_steps_rank, ev0.elapsed_time(ev1) / 1e3, world)
+    el_ms = el_s * 1e3
 
     # roofline of the advance kernel: algorithmic bytes per launch / launch time
     bytes_per_step = w.cell.algorithmic_bytes_per_step() * n_inst  # one timestep, all instances
