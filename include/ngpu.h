@@ -224,14 +224,14 @@ int ngpu_sim_features(ngpu_sim *s, int32_t site, double dt, double stim_on, doub
                       float *out_dev, void *cuda_stream);
 
 /*
- * Runtime specialisation of the advance kernel.  At initialisation an FP32
- * simulation (or, at creation, an FP32 batch) gets a kernel compiled with
- * NVRTC for its model's mechanism masks (up to 16): nodes with those masks
+ * Runtime specialisation of the advance kernel.  At initialisation a
+ * simulation (or, at creation, a batch), FP32 or FP64, gets a kernel compiled
+ * with NVRTC for its model's mechanism masks (up to 16): nodes with those masks
  * run channel code in which the mask is a compile-time constant.  The
  * reference regenerates and recompiles its simulator per model ahead of time
  * (AllModels.cu / AllModels.cuh); no API counterpart.  Without NVRTC, after a
  * failed compile, or with NGPU_JIT=0 in the environment, the ahead-of-time
- * kernel runs (same results up to FP32 rounding order within a node).
+ * kernel runs (same results up to rounding order within a node).
  *   ngpu_sim_classes  masks compiled for the kernel that runs s (0: the
  *                     ahead-of-time kernel); valid after ngpu_sim_init
  *   ngpu_jit_build    compile only (no device needed) for compute
@@ -242,7 +242,7 @@ int ngpu_sim_classes(const ngpu_sim *s, int32_t *n_classes);
 /* Parameters the simulation's runtime-specialised kernel compiles in as
  * constants (after init): those with one value in every parameter set and
  * every section that uses them, found by set_params; 0 where folding does
- * not apply (the built-in sets in FP64, NGPU_JIT=0 or NGPU_PARAM_FOLD=0).  For a
+ * not apply (NGPU_JIT=0 or NGPU_PARAM_FOLD=0).  For a
  * member of a batch: those its batch's kernel compiles in, the parameters
  * every member holds at the same value.
  * The reference compiles its model's GLOBAL parameters into its generated

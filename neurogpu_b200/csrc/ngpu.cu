@@ -995,9 +995,8 @@ static int sim_upload_nodes(ngpu_sim* s);
 
 // Parameters with one value (the same bits) in every parameter set and every
 // section whose nodes use them: the runtime-specialised kernel compiles them
-// in (param_fold.cuh).  Wherever that kernel runs (FP32, or a generated set
-// in either precision), with runtime compilation on and NGPU_PARAM_FOLD not
-// 0.  New values
+// in (param_fold.cuh).  Wherever that kernel runs (either precision), with
+// runtime compilation on and NGPU_PARAM_FOLD not 0.  New values
 // after initialisation re-select the kernel before the next launch.
 // Parameter blocks (the rows of one section and mechanism combination) that
 // hold the same values at every instance as another block of the same
@@ -1075,7 +1074,7 @@ static int sim_find_folds(ngpu_sim* s) {
     const ngpu_model* m = s->m;
     ngpu_jit::Folds folds;
     const char* ev = getenv("NGPU_PARAM_FOLD");
-    const bool on = (s->precision == NGPU_FP32 || gen_set(m->mechset)) && ngpu_jit::enabled() &&
+    const bool on = ngpu_jit::enabled() &&
                     !(ev && ev[0] == '0') && m->ptab_rows > 0;
     if (on) {
         if (!s->d_prange) {
@@ -1235,7 +1234,7 @@ static std::vector<uint32_t> model_masks(const ngpu_model* m) {
 }
 
 // Node records with this run's split, recording columns and mechanism
-// classes, uploaded to the device.  In FP32 the classes follow the
+// classes, uploaded to the device.  The classes follow the
 // runtime-specialised kernels of the simulation's batch, or its own.
 
 // Host side of an initialisation: node records, the trace buffer (kept when
@@ -1305,7 +1304,7 @@ struct ngpu_batch {
 
 // The folds that hold for every member (same parameter, same value).
 static ngpu_jit::Folds batch_common_folds(const ngpu_batch* b) {
-    if ((b->precision != NGPU_FP32 && !gen_set(b->mechset)) || b->sims.empty()) return {};
+    if (b->sims.empty()) return {};
     ngpu_jit::Folds out = b->sims[0]->folds;
     for (size_t k = 1; k < b->sims.size(); ++k) {
         const ngpu_jit::Folds& f = b->sims[k]->folds;
@@ -1341,7 +1340,7 @@ static int sim_upload_nodes(ngpu_sim* s) {
     const ngpu_model* m = s->m;
     s->jit = nullptr;
     const GenSet* gs = gen_set(m->mechset);
-    if (s->precision == NGPU_FP32 || gs) {
+    {  // FP32 and FP64 alike (generated sets have no other kernel)
         if (s->batch) {
             s->jit = s->batch->jit;
         } else {
@@ -1457,11 +1456,10 @@ static void batch_drop_graph(ngpu_batch* b) {
 }
 
 // One specialised kernel over every member's masks, with the parameters all
-// members share compiled in (FP32, or a generated set in either precision).
+// members share compiled in.
 static int batch_select_kernels(ngpu_batch* b) {
     b->jit = nullptr;
     const GenSet* gs = gen_set(b->mechset);
-    if (b->precision != NGPU_FP32 && !gs) return NGPU_OK;
     std::vector<uint32_t> all;
     int64_t pf_ctas = 0;  // the prefetch follows the members that hold most of the CTAs
     for (ngpu_sim* s : b->sims) {
