@@ -136,6 +136,26 @@ def test_autotuner_picks_a_candidate(ngpu_built, workloads):
                                w.v_init, candidates=(2, 4, 8), items=(2, 3)) is res      # cached
 
 
+def test_uneven_batch_fp64_vs_oracle_sample(ngpu_built, oracle, workloads):
+    """An FP64 batch (its runtime-specialised kernel, shared parameters
+    compiled in) against the FP64 oracle on a sample: 2 sets x every
+    protocol of each morphology, max |dV| <= 1e-5 mV (the float32 output's
+    rounding)."""
+    from neurogpu_b200.sim import Batch
+    sims = _sims(workloads, precision="fp64")
+    b = Batch(sims)
+    assert sims[0].param_folds() >= 15
+    b.init(workloads[0].v_init)
+    b.advance(0, workloads[0].nt)
+    for s, w in zip(sims, workloads):
+        got = s.trace()[:2, :, :1].astype(np.float64)
+        ref = oracle.run_workload(w.subset(n_sets=2))
+        err = float(np.max(np.abs(got - ref)))
+        print(f"{w.name}: FP64 batch max|dV| {err:.2e} mV")
+        assert err <= 1e-5
+    b.close()
+
+
 def test_uneven_batch_fp32_vs_oracle_sample(ngpu_built, oracle, workloads):
     """FP32 batch vs the FP64 oracle on a sample: 2 sets x every protocol of
     each morphology (spike time <= 0.05 ms, <= 0.1 mV away from spikes)."""
