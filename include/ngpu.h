@@ -150,7 +150,12 @@ int ngpu_run(ngpu_model *m, int32_t n_sets, const float *params, int32_t n_stim,
 int ngpu_sim_create(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision,
                     ngpu_sim **out);
 int ngpu_sim_destroy(ngpu_sim *s);
-/* params as in ngpu_run; on_device != 0: a device pointer. */
+/* params as in ngpu_run; on_device != 0: a device pointer.  Synchronous: it
+ * gathers the parameter table, then reads back which parameters hold one
+ * value (compiled into the specialised kernel, ngpu_sim_param_folds) and
+ * which sections repeat another's values (they share rows,
+ * ngpu_sim_param_rows); after ngpu_sim_init, values that change either
+ * re-select the kernel or re-upload the node records before the next launch. */
 int ngpu_sim_set_params(ngpu_sim *s, const float *params, int32_t on_device);
 int ngpu_sim_set_stimulus(ngpu_sim *s, int32_t nt, const float *amps, const float *dts,
                           int32_t stim_node, float stim_area_um2, int32_t on_device);
