@@ -1,6 +1,6 @@
 """GPU parity: the CUDA simulation (through the C ABI) against the CPU oracle.
 
-Tolerances (stated by the north-star target):
+Tolerances:
   * FP64 kernel vs FP64 oracle: max |dV| <= 1e-5 mV (same algorithm, both
     double; the kernel uses the analytic conductance where the oracle uses
     the reference's finite difference, equal to ~1e-10 relative; the bound
