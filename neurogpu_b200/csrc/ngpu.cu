@@ -123,7 +123,11 @@ struct HostNode {
 
 }  // namespace
 
+struct ngpu_sim;
 struct ngpu_model {
+    // ngpu_run's last simulation, reused by the next call of the same shape
+    ngpu_sim* run_cache = nullptr;
+    std::mutex run_mu;
     int n = 0, n_sections = 0, mechset = 0, n_mech = 0, n_params = 0;
     std::vector<int> parent, section;
     std::vector<double> a, b, cm;
@@ -773,7 +777,10 @@ int ngpu_model_create(int32_t n_nodes, const int32_t* parent, const double* a, c
     return NGPU_OK;
 }
 
+static void sim_free(ngpu_sim* s);
+
 int ngpu_model_destroy(ngpu_model* m) {
+    if (m && m->run_cache) sim_free(m->run_cache);
     delete m;
     return NGPU_OK;
 }
@@ -1829,9 +1836,26 @@ int ngpu_run(ngpu_model* m, int32_t n_sets, const float* params, int32_t n_stim,
              const float* amps, const float* dts, int32_t stim_node, float stim_area_um2,
              int32_t n_rec, const int32_t* rec_nodes, float v_init, int32_t precision, float* out) {
     if (!out) return fail(NGPU_E_INVALID, "out is null");
+    if (!m) return fail(NGPU_E_INVALID, "null model");
+    // The last run's simulation stays with the model and serves the next call
+    // of the same shape (sets, stimuli, precision): no device allocation or
+    // release per call.  A call that finds it in use by another thread runs
+    // on a simulation of its own.
+    std::unique_lock<std::mutex> lock(m->run_mu, std::try_to_lock);
     ngpu_sim* s = nullptr;
-    int rc = ngpu_sim_create(m, n_sets, n_stim, precision, &s);
-    if (rc) return rc;
+    int rc = NGPU_OK;
+    ngpu_sim* c = lock.owns_lock() ? m->run_cache : nullptr;
+    if (c && c->n_sets == n_sets && c->n_stim == n_stim && c->precision == precision) {
+        s = c;
+    } else {
+        if (c) {
+            sim_free(c);
+            m->run_cache = nullptr;
+        }
+        rc = ngpu_sim_create(m, n_sets, n_stim, precision, &s);
+        if (rc) return rc;
+    }
+    if (lock.owns_lock()) m->run_cache = nullptr;  // taken; kept again below on success
     if ((rc = ngpu_sim_set_params(s, params, 0)) ||
         (rc = ngpu_sim_set_stimulus(s, nt, amps, dts, stim_node, stim_area_um2, 0)) ||
         (rc = ngpu_sim_set_recording(s, n_rec, rec_nodes, 1)) || (rc = ngpu_sim_init(s, v_init, nullptr)) ||
@@ -1843,7 +1867,8 @@ int ngpu_run(ngpu_model* m, int32_t n_sets, const float* params, int32_t n_stim,
     }
     int32_t nbad = 0;
     rc = ngpu_sim_check(s, &nbad, nullptr);
-    sim_free(s);
+    if (rc == NGPU_OK && lock.owns_lock()) m->run_cache = s;
+    else sim_free(s);
     if (rc) return rc;
     if (nbad) return fail(NGPU_E_NUMERIC, std::to_string(nbad) + " instance(s) produced non-finite voltage");
     return NGPU_OK;

@@ -114,6 +114,25 @@ def test_host_entry_point_matches_resident_sim(ngpu_built, cfg):
     assert np.array_equal(out, _gpu_run(w, "fp32"))
 
 
+def test_host_entry_point_reuses_its_simulation(ngpu_built, cfg):
+    """ngpu_run keeps its simulation with the model between calls: calls of
+    the same shape with new parameters, stimuli and recording sites, a call
+    of another shape, and the same shape again each give the traces of a
+    fresh model."""
+    from neurogpu_b200.sim import Model, run
+    w = cfg["hh"]
+    m = Model(w.cell)
+    p2 = w.params.copy()
+    p2[:, :, :] *= np.float32(1.1)
+    calls = [(w.params, w.amps, w.rec_nodes), (p2, w.amps[::-1].copy(), np.array([0, 3], dtype=np.int32)),
+             (w.params[:5], w.amps[:1], w.rec_nodes), (w.params, w.amps, w.rec_nodes)]
+    for params, amps, rec in calls:
+        got = run(m, params, amps, w.dts, w.stim_node, w.stim_area, rec, w.v_init)
+        fresh = run(Model(w.cell), params, amps, w.dts, w.stim_node, w.stim_area, rec, w.v_init)
+        assert np.array_equal(got, fresh)
+    m.close()
+
+
 def test_ragged_instances_recording_and_cadence(ngpu_built, oracle, cfg):
     """5 sets x 3 stimuli (15 instances, half a warp), duplicated and
     multiple recording sites, recording every 7th step."""
