@@ -471,7 +471,7 @@ def main():
         run(model, we.params, we.amps, we.dts, we.stim_node, we.stim_area, we.rec_nodes, we.v_init)
         torch.cuda.synchronize()
         samples = []
-        for _ in range(3):  # the median of three calls: host-side work makes single calls noisy
+        for _ in range(5):  # the median of five calls: host-side work makes single calls noisy
             barrier(world)
             t0 = time.perf_counter()
             out = run(model, we.params, we.amps, we.dts, we.stim_node, we.stim_area, we.rec_nodes, we.v_init)
