@@ -208,6 +208,25 @@ def test_demo_matches_numpy(tmp_path, init):
             assert G_gen == pytest.approx(G_np, rel=1e-9, abs=1e-14), (on, v)
 
 
+def test_parameter_reads_name_their_index():
+    """Every parameter the generated code reads goes through pload<R, P>
+    with P the parameter's index in the set (the index a folded constant is
+    looked up by): generator and kernel agree on what each constant is."""
+    import re
+    g = _demo()
+    k_of = {f"m{k}_": m for k, m in enumerate(g.mechs)}
+    found = 0
+    for line in g.source.splitlines():
+        m = re.search(r"(m\d+_)(\w+) = pload<R, (\d+)>\(pr, q \+ (\d+)\)", line)
+        if not m:
+            continue
+        found += 1
+        mech = k_of[m.group(1)]
+        assert g.params[int(m.group(3))] == f"{m.group(2)}_{mech}", line
+        assert int(m.group(3)) in g.mech_params[g.mech_index(mech)]
+    assert found == g.n_params
+
+
 def test_symbolic_linear_form_and_derivative():
     from neurogpu_b200 import nmodl
     p = nmodl.Parser(nmodl.tokenize("-ica*(10000)/(2*F*d) + (r - c)/t\n"))
@@ -388,6 +407,32 @@ def test_defined_set_runs_fp32_against_fp64(ngpu_built):
     print(f"demo set: {n_spk} spikes; FP32 vs FP64 spike times {err:.2e} ms, subthreshold {sub:.2e} mV")
     assert n_spk > 0
     assert mism == 0 and err <= 0.05 and sub <= 0.1
+
+
+@pytest.mark.gpu
+def test_defined_set_folded_matches_loaded(ngpu_built, monkeypatch):
+    """The demo set with its uniform parameters compiled in against the same
+    set reading every parameter, FP32: a constant under the wrong index would
+    change the traces by far more than the bounds."""
+    g = _demo().register()
+    w = _demo_workload(g)
+    monkeypatch.setenv("NGPU_PARAM_FOLD", "1")
+    from neurogpu_b200.sim import Simulator
+    probe = Simulator(w.cell, w.n_sets, w.n_stim, "fp32")
+    probe.set_params(w.params)
+    probe.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+    probe.set_recording(w.rec_nodes)
+    probe.init(w.v_init)
+    assert probe.param_folds() >= 5
+    probe.close()
+    a, bad_a = _sim(w, "fp32")
+    monkeypatch.setenv("NGPU_PARAM_FOLD", "0")
+    b, bad_b = _sim(w, "fp32")
+    assert bad_a == 0 and bad_b == 0
+    err, mism = spike_time_error(a, b, w.dt)
+    sub = subthreshold_error(a, b, w.dt)
+    print(f"demo set folded vs loaded: spike times {err:.2e} ms, subthreshold {sub:.2e} mV")
+    assert mism == 0 and err <= 0.05 and sub <= 0.01
 
 
 @pytest.mark.gpu
