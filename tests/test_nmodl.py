@@ -436,6 +436,48 @@ def test_defined_set_folded_matches_loaded(ngpu_built, monkeypatch):
 
 
 @pytest.mark.gpu
+def test_defined_set_batch_matches_separate_runs(ngpu_built, monkeypatch):
+    """Two demo-set simulations of different trees in one batch (one
+    runtime-compiled kernel for both, with the parameters both hold at one
+    value compiled in) against each run alone reading every parameter."""
+    from neurogpu_b200.sim import Batch, Simulator
+    g = _demo().register()
+    ws = [_demo_workload(g, seed=9), _demo_workload(g, seed=10)]
+
+    def sims():
+        out = []
+        for w in ws:
+            s = Simulator(w.cell, w.n_sets, w.n_stim, "fp32")
+            s.set_params(w.params)
+            s.set_stimulus(w.amps, w.dts, w.stim_node, w.stim_area)
+            s.set_recording(w.rec_nodes)
+            out.append(s)
+        return out
+    monkeypatch.setenv("NGPU_PARAM_FOLD", "0")
+    ref = []
+    for s, w in zip(sims(), ws):
+        s.init(w.v_init)
+        s.advance(0, w.nt)
+        ref.append(s.trace())
+        s.close()
+    monkeypatch.setenv("NGPU_PARAM_FOLD", "1")
+    ss = sims()
+    b = Batch(ss)
+    assert ss[0].param_folds() >= 5
+    b.init(ws[0].v_init)
+    b.advance(0, ws[0].nt)
+    for s, r, w in zip(ss, ref, ws):
+        got = s.trace()
+        assert s.n_bad() == 0
+        err, mism = spike_time_error(got, r, w.dt)
+        sub = subthreshold_error(got, r, w.dt)
+        assert mism == 0 and err <= 0.05 and sub <= 0.01, (err, sub)
+    b.close()
+    for s in ss:
+        s.close()
+
+
+@pytest.mark.gpu
 def test_generated_pas_matches_builtin(ngpu_built):
     """A set generated from nothing but NEURON's pas, on the passive cable
     workload, against the built-in TTPC set's pas."""
