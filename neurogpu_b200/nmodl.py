@@ -18,7 +18,8 @@ RANGE / GLOBAL), PARAMETER, CONSTANT, ASSIGNED, STATE, UNITS (FARADAY, R,
 PI), INITIAL, BREAKPOINT with SOLVE ... METHOD cnexp (DERIVATIVE) or METHOD
 sparse (KINETIC), DERIVATIVE, KINETIC with first-order reactions
 (~ a <-> b (kf, kb)), sources (~ a << (f)) and CONSERVE, SOLVE ...
-STEADYSTATE sparse in INITIAL, PROCEDURE, FUNCTION, LOCAL, if / else,
+STEADYSTATE sparse in INITIAL, PROCEDURE, FUNCTION, FUNCTION_TABLE of one
+argument (values given to generate()), LOCAL, if / else,
 UNITSON / UNITSOFF, TABLE (ignored: rates are computed directly), comments.
 VERBATIM, NET_RECEIVE, point processes, higher-order reactions and other
 integration methods raise NmodlError.
@@ -501,6 +502,8 @@ class Mechanism:
     initial: list = field(default_factory=list)
     procedures: dict = field(default_factory=dict)    # name -> (args, stmts)
     functions: dict = field(default_factory=dict)
+    tables: dict = field(default_factory=dict)        # FUNCTION_TABLE name -> argument names
+    table_data: dict = field(default_factory=dict)    # name -> (xs, ys), given to generate()
 
     def ion_names(self) -> set:
         out = set()
@@ -674,6 +677,20 @@ def parse_mod(text: str, name_hint: str = "") -> Mechanism:
             p.skip_units()
             body = p.stmts()
             (mech.procedures if v == "PROCEDURE" else mech.functions)[name] = (args, body)
+        elif v == "FUNCTION_TABLE":
+            name = p.ident()
+            p.expect("(")
+            args = []
+            while p.peek().val != ")":
+                args.append(p.ident())
+                p.skip_units()
+                if p.peek().val == ",":
+                    p.next()
+            p.expect(")")
+            p.skip_units()
+            if len(args) != 1:
+                raise NmodlError(f"line {tok.line}: FUNCTION_TABLE {name}: one argument only")
+            mech.tables[name] = args
         elif v in ("NET_RECEIVE", "VERBATIM", "LINEAR", "NONLINEAR", "DISCRETE", "PARTIAL"):
             raise NmodlError(f"line {tok.line}: {v} blocks are not supported")
         else:
@@ -1013,19 +1030,36 @@ def _mech_order_key(name: str) -> str:
 
 
 def generate(mods: dict, name: str = "generated", celsius: float = 34.0, reversal: dict | None = None,
-             cao: float = 2.0, constants: dict | None = None) -> GeneratedMechSet:
+             cao: float = 2.0, constants: dict | None = None, tables: dict | None = None) -> GeneratedMechSet:
     """mods: suffix or file name -> .mod text (NEURON's pas is added unless
     given).  reversal: fixed reversal potentials of ions whose concentrations
     no mechanism writes (e.g. {"na": 50, "k": -85}).  constants: per
     mechanism, PARAMETERs to compile in as constants instead of taking a
-    parameter row ({"na": {"vshift": -5}}).  Mechanisms are ordered as the
-    reference orders them (case-insensitive name order)."""
+    parameter row ({"na": {"vshift": -5}}).  tables: per mechanism, the values
+    of its FUNCTION_TABLEs, which NEURON fills from hoc: {"kt": {"tau": (xs,
+    ys)}}, xs strictly increasing; read by linear interpolation, the end
+    values outside [xs[0], xs[-1]].  Mechanisms are ordered as the reference
+    orders them (case-insensitive name order)."""
     reversal = dict(reversal or {})
     constants = constants or {}
+    tables = tables or {}
     parsed = {}
     for key, text in mods.items():
         m = parse_mod(text, key)
         parsed[m.suffix] = m
+    for m in parsed.values():
+        for tname in m.tables:
+            data = tables.get(m.suffix, {}).get(tname)
+            if data is None:
+                raise NmodlError(f"{m.suffix}: FUNCTION_TABLE {tname} needs its values "
+                                 f"(tables={{'{m.suffix}': {{'{tname}': (xs, ys)}}}})")
+            xs = [float(x) for x in data[0]]
+            ys = [float(y) for y in data[1]]
+            if len(xs) < 2 or len(xs) != len(ys) or any(not math.isfinite(x) for x in xs + ys) or \
+                    any(b <= a for a, b in zip(xs, xs[1:])):
+                raise NmodlError(f"{m.suffix}: FUNCTION_TABLE {tname}: xs strictly increasing, xs and ys "
+                                 "finite, of one length >= 2")
+            m.table_data[tname] = (xs, ys)
     if "pas" not in parsed:
         parsed["pas"] = parse_mod(PAS_MOD)
     order = sorted(parsed, key=_mech_order_key)
@@ -1296,6 +1330,7 @@ class _MechBody:
         self.k = k
         self.consts = consts or {}
         self.funcs = {f: f"f{k}_{f}" for f in m.functions}
+        self.funcs.update({t: f"t{k}_{t}" for t in m.tables})
         self.procs = {p: f"p{k}_{p}" for p in m.procedures}
         self._tmp = 0
 
@@ -1304,6 +1339,25 @@ class _MechBody:
 
     def callables(self, w):
         m = self.m
+        for tname, (xs, ys) in m.table_data.items():
+            # FUNCTION_TABLE: linear interpolation between the given points, the
+            # end values outside them (binary search for the interval)
+            n = len(xs)
+            fn = self.funcs[tname]
+            w(f"        auto {fn} = [&](R a_x) -> R {{")
+            w(f"            static const R xs[{n}] = {{{', '.join(_lit(x) for x in xs)}}};")
+            w(f"            static const R ys[{n}] = {{{', '.join(_lit(y) for y in ys)}}};")
+            w(f"            if (!(a_x > xs[0])) return ys[0];")
+            w(f"            if (a_x >= xs[{n - 1}]) return ys[{n - 1}];")
+            w(f"            int lo = 0, hi = {n - 1};")
+            w(f"            while (hi - lo > 1) {{")
+            w(f"                const int mid = (lo + hi) >> 1;")
+            w(f"                if (xs[mid] <= a_x) lo = mid;")
+            w(f"                else hi = mid;")
+            w(f"            }}")
+            w(f"            return ys[lo] + M::dv(a_x - xs[lo], xs[hi] - xs[lo]) * (ys[hi] - ys[lo]);")
+            w(f"        }};")
+            w(f"        (void){fn};")
         for fname, (args, body) in m.functions.items():
             env = dict(self.env)
             for a in args:
