@@ -15,8 +15,9 @@ which the library compiles at run time into the advance kernel
 
 Supported NMODL: NEURON (SUFFIX, USEION ... READ/WRITE, NONSPECIFIC_CURRENT,
 RANGE / GLOBAL), PARAMETER, CONSTANT, ASSIGNED, STATE, UNITS (FARADAY, R,
-PI), INITIAL, BREAKPOINT with SOLVE ... METHOD cnexp (DERIVATIVE) or METHOD
-sparse (KINETIC), DERIVATIVE, KINETIC with first-order reactions
+PI), INITIAL, BREAKPOINT with SOLVE ... METHOD cnexp, derivimplicit (equations
+linear in their own state: one exact implicit-Euler step) or euler
+(DERIVATIVE), or METHOD sparse (KINETIC), DERIVATIVE, KINETIC with first-order reactions
 (~ a <-> b (kf, kb)), sources (~ a << (f)) and CONSERVE, SOLVE ...
 STEADYSTATE sparse in INITIAL, PROCEDURE, FUNCTION, FUNCTION_TABLE of one
 argument (values given to generate()), LOCAL, if / else,
@@ -1252,11 +1253,12 @@ def _emit_set(mechs, mech_params, params, celsius, ktf, reversal, cao, constants
                                      "(sparse only)")
                 body.kinetic(w, sv.block, 3, dict(body.env), steady=False)
                 continue
-            if sv.method not in (None, "cnexp"):
-                raise NmodlError(f"{m.suffix}: METHOD {sv.method} is not supported (cnexp only)")
+            modes = {None: "deriv", "cnexp": "deriv", "derivimplicit": "deriv_be", "euler": "deriv_euler"}
+            if sv.method not in modes:
+                raise NmodlError(f"{m.suffix}: METHOD {sv.method} is not supported (cnexp, derivimplicit, euler)")
             if sv.block not in m.derivatives:
                 raise NmodlError(f"{m.suffix}: no DERIVATIVE {sv.block}")
-            body.stmts(w, m.derivatives[sv.block], 3, mode="deriv")
+            body.stmts(w, m.derivatives[sv.block], 3, mode=modes[sv.method])
         w("        }")
         for s in m.states:  # a concentration the mechanism keeps as a state
             if m.writes(s):
@@ -1457,6 +1459,20 @@ class _MechBody:
                     env[st.name] = _lit(e.v)
         return consts
 
+    def _derived(self, body) -> list:
+        """States with a derivative in the body (also inside if / else), in order."""
+        out = []
+
+        def walk(ss):
+            for st_ in ss:
+                if isinstance(st_, Deriv) and st_.name not in out:
+                    out.append(st_.name)
+                elif isinstance(st_, If):
+                    walk(st_.then)
+                    walk(st_.other)
+        walk(body)
+        return out
+
     def _locals(self, body, env) -> list:
         """Names assigned in a body that are not mechanism variables: block locals."""
         out = []
@@ -1482,7 +1498,12 @@ class _MechBody:
         for l in locs:
             if not env[l].startswith("(R)"):
                 w(f"{pad}R l_{l} = 0;")
+        integrated = self._derived(body) if mode == "deriv_euler" else []
+        for x in integrated:  # euler: every derivative at the step's starting states, then the updates
+            w(f"{pad}R eu{self.k}_{x} = 0;")
         self._block(w, body, ind, env, mode)
+        for x in integrated:
+            w(f"{pad}{env[x]} = {env[x]} + dt * eu{self.k}_{x};")
         self.consts = saved
 
     def _block(self, w, body, ind, env, mode):
@@ -1500,13 +1521,30 @@ class _MechBody:
                 if s.name + "@rate" in env:
                     w(f"{pad}{env[s.name + '@rate']} = {em.e(recip(s.e))};")
             elif isinstance(s, Deriv):
-                if mode != "deriv":
+                if not mode.startswith("deriv"):
                     raise NmodlError(f"{self.m.suffix}: {s.name}' outside a DERIVATIVE block")
                 x = s.name
                 if x not in self.m.states:
                     raise NmodlError(f"{self.m.suffix}: {x}' of a non-STATE")
                 e = simplify(s.e)
                 xv = env[x]
+                if mode == "deriv_euler":
+                    w(f"{pad}eu{self.k}_{x} = {em.e(e)};")
+                    continue
+                if mode == "deriv_be":
+                    # implicit Euler of x' = a + b x, exact for an equation linear in x:
+                    # x_new = (x + dt a) / (1 - dt b)
+                    coupled = free_vars(e) & (set(self.m.states) - {x})
+                    if coupled:
+                        raise NmodlError(f"{self.m.suffix}: derivimplicit {x}' depends on other STATEs "
+                                         f"({', '.join(sorted(coupled))}): coupled systems are not supported")
+                    try:
+                        a, b = linear_form(e, x)
+                    except NmodlError:
+                        raise NmodlError(f"{self.m.suffix}: {x}' is not linear in {x}: derivimplicit is supported "
+                                         "for equations linear in their state") from None
+                    w(f"{pad}{xv} = M::dv({xv} + dt * ({em.e(a)}), (R)1 - dt * ({em.e(b)}));")
+                    continue
                 if (isinstance(e, Bin) and e.op == "/" and isinstance(e.l, Bin) and e.l.op == "-"
                         and isinstance(e.l.r, Var) and e.l.r.name == x and x not in free_vars(e.l.l)
                         and x not in free_vars(e.r)):

@@ -263,8 +263,8 @@ def _py(x):
     ("NEURON { SUFFIX k1 }\nSTATE { a }\nNET_RECEIVE (w) { a = a + w }\n", "NET_RECEIVE"),
     ("NEURON { SUFFIX q }\nSTATE { x }\nBREAKPOINT { SOLVE d METHOD cnexp }\nDERIVATIVE d { x' = -x*x }\n",
      "not linear"),
-    ("NEURON { SUFFIX q }\nSTATE { x }\nBREAKPOINT { SOLVE d METHOD euler }\nDERIVATIVE d { x' = -x }\n",
-     "cnexp only"),
+    ("NEURON { SUFFIX q }\nSTATE { x }\nBREAKPOINT { SOLVE d METHOD runge }\nDERIVATIVE d { x' = -x }\n",
+     "not supported"),
     ("NEURON { SUFFIX q NONSPECIFIC_CURRENT i }\nASSIGNED { i }\nBREAKPOINT { i = gx*v }\n", "unknown name"),
 ])
 def test_unsupported_input_is_an_error(text, msg):
