@@ -41,6 +41,10 @@ UNIT = "compartment-steps/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 TRAFFIC_FILE = ROOT / "profiles" / "ngpu_jit_advance_ttpc_like_x4096.md"
+# the other model family, for profiling (--model hh_active): its own metric name and ncu summary
+MODELS = {"ttpc_like": (METRIC, TRAFFIC_FILE),
+          "hh_active": ("compartment-steps/s (HH 500-compartment x4096)",
+                        ROOT / "profiles" / "ngpu_jit_advance_hh_x4096.md")}
 
 
 def parse_args():
@@ -58,14 +62,20 @@ def parse_args():
     ap.add_argument("--cpu-sample-steps", type=int, default=400)
     ap.add_argument("--ga-pop", type=int, default=8192)
     ap.add_argument("--ga-gens", type=int, default=20)
+    ap.add_argument("--model", default="ttpc_like", choices=sorted(MODELS),
+                    help="the cell of the default workload: the TTPC-like headline, or the HH-type cell")
     ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga", "ga_ops"],
                     help="uneven_batch: 8192 sets over 200/800/1500/3000-compartment trees x 5 protocols, "
                          "one launch per chunk, the run captured as a CUDA graph (auxiliary line)")
     return ap.parse_args()
 
 
-def workload(n_sets: int):
+def workload(n_sets: int, model: str = "ttpc_like"):
+    """The TTPC-like headline workload (2000 ms), or the HH-type cell of the
+    other model family (500 compartments, 500 ms) for profiling."""
     from neurogpu_b200 import configs
+    if model == "hh_active":
+        return configs.hh_active(n_sets=n_sets)
     return configs.ttpc_like(n_sets=n_sets)
 
 
@@ -77,11 +87,11 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_comp_step():
+def traffic_per_comp_step(model: str = "ttpc_like"):
     """DRAM bytes per compartment-step of the advance kernel from the
     committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum)."""
     try:
-        m = re.search(r"traffic_bytes_per_compartment_step:\s*([0-9.eE+-]+)", TRAFFIC_FILE.read_text())
+        m = re.search(r"traffic_bytes_per_compartment_step:\s*([0-9.eE+-]+)", MODELS[model][1].read_text())
         return float(m.group(1)) if m else None
     except Exception:
         return None
@@ -208,7 +218,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    w = workload(args.n_sets)
+    w = workload(args.n_sets, args.model)
     threads = os.cpu_count() or 1
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle_py
@@ -225,10 +235,10 @@ def run_reference(args):
     el = float(np.mean(times))
     v = sub.compartment_steps() / el
     line = {
-        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "metric": MODELS[args.model][0], "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": "ttpc_like", "n_nodes": w.cell.n_nodes, "n_sets": args.n_sets,
+        "config": {"workload": args.model, "n_nodes": w.cell.n_nodes, "n_sets": args.n_sets,
                    "n_stim": w.n_stim, "dt_ms": w.dt},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{sub.n_sets} sets x {sub.n_stim} stimuli x {sub.nt} steps per step"},
@@ -408,7 +418,7 @@ def main():
     from neurogpu_b200 import _ffi
     from neurogpu_b200.sim import Model, Simulator, run
     rank, world, local = dist_setup(args.gpus)
-    w = workload(args.n_sets)
+    w = workload(args.n_sets, args.model)
     n_inst = w.n_sets * w.n_stim
     total_steps = (args.warmup + args.steps) * args.chunk
     if total_steps > w.nt:
@@ -461,7 +471,7 @@ def main():
     alg_bytes_launch = bytes_per_step * args.chunk
     achieved_gbs = alg_bytes_launch / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
-    tpcs = traffic_per_comp_step()
+    tpcs = traffic_per_comp_step(args.model)
     traffic = None if tpcs is None else tpcs * w.cell.n_nodes * n_inst * args.chunk
 
     # end to end through the public host-buffer entry point (ngpu_run)
@@ -489,10 +499,10 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": MODELS[args.model][0], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "ttpc_like", "n_nodes": w.cell.n_nodes, "n_sets": w.n_sets,
+            "config": {"workload": args.model, "n_nodes": w.cell.n_nodes, "n_sets": w.n_sets,
                        "n_stim": w.n_stim, "instances_per_gpu": n_inst, "dt_ms": w.dt,
                        "timesteps_per_step": args.chunk, "l2": "state larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}"},
