@@ -49,7 +49,9 @@ NGPU_HD R efun(R z) {
 }
 // efun(z) and efun(-z) from one exponential: efun(-z) = efun(z) e^z, with the
 // series 1 -+ z/2 + z^2/12 near 0.  The alpha/beta pairs of NaTa_t, NaTs2_t
-// and Nap_Et2's activation are efun of opposite arguments.
+// and Nap_Et2's activation are efun of opposite arguments.  Above z = 80,
+// efun(-z) = z / (1 - e^-z) is z to well below FP64 rounding; there e^z may
+// overflow FP32, where efun(z) e^z would be 0 * inf.
 template <typename R>
 NGPU_HD void efun_pair(R z, R& pos, R& neg) {
     if (fabs(z) < (R)1e-2) {
@@ -60,7 +62,7 @@ NGPU_HD void efun_pair(R z, R& pos, R& neg) {
     }
     const R e = Math<R>::ex(z);
     pos = Math<R>::dv(z, e - (R)1);
-    neg = pos * e;
+    neg = z > (R)80 ? z : pos * e;
 }
 // 1/(1 + e^z)
 template <typename R>
