@@ -142,3 +142,39 @@ def test_all_mechanisms_together(probe, oracle, mechset_name):
     for v in np.linspace(-90, 30, 13):
         for init in (True, False):
             _compare(probe, oracle, mechset_name, list(range(n_mech)), float(v), 0.1, rng, init)
+
+
+EFUN_PROBE = r'''
+#include "channels_ttpc.cuh"
+extern "C" void probe_pair_f32(float z, float* pos, float* neg) { ngpu::efun_pair<float>(z, *pos, *neg); }
+extern "C" void probe_pair_f64(double z, double* pos, double* neg) { ngpu::efun_pair<double>(z, *pos, *neg); }
+'''
+
+
+def test_efun_pair_against_two_efuns(tmp_path):
+    """efun_pair (one exponential for efun(z) and efun(-z)), compiled for the
+    host from the channel header, against z/(e^z - 1) in FP64 over |z| <= 100:
+    through the series switch at 1e-2 and past FP32's overflow of e^z
+    (z > 88.7), where efun(-z) -> z.  The FP64 bound is the series' own
+    truncation, z^4/720 < 1.4e-11 for |z| < 1e-2 (efun uses the same series)."""
+    (tmp_path / "p.cu").write_text(EFUN_PROBE)
+    r = subprocess.run(["nvcc", "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
+                        "-I", str(ROOT / "neurogpu_b200" / "csrc"), str(tmp_path / "p.cu"), "-o",
+                        str(tmp_path / "libp.so")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    L = C.CDLL(str(tmp_path / "libp.so"))
+    L.probe_pair_f32.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.probe_pair_f64.argtypes = [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+
+    def efun(z):   # z / (e^z - 1), from expm1 so that it is exact near 0
+        return 1.0 if z == 0.0 else z / np.expm1(z)
+
+    zs = np.concatenate([np.linspace(-100, 100, 2001), [-1e-2, -9.9e-3, 0.0, 9.9e-3, 1e-2, 79.9, 80.1, 88.5, 89.0, 95.0]])
+    for fn, ctype, rel in ((L.probe_pair_f64, C.c_double, 2e-11), (L.probe_pair_f32, C.c_float, 1e-5)):
+        for z in zs:
+            z = float(ctype(z).value)
+            p, n = ctype(), ctype()
+            fn(z, C.byref(p), C.byref(n))
+            assert np.isfinite(p.value) and np.isfinite(n.value), z
+            assert p.value == pytest.approx(efun(z), rel=rel, abs=1e-30), z
+            assert n.value == pytest.approx(efun(-z), rel=rel, abs=1e-30), z
