@@ -8,8 +8,10 @@ host in FP64, against numpy statements of their .mod files (Ca.mod rates();
 KdShu2007.mod trates(), with its ek a PARAMETER, not an ion read), to 1e-9
 relative: the generator writes (-27 - v) / (exp((-27 - v)/3.8) - 1) as efun
 with its series near 0, and the .mod's own nudge v += 1e-4 at v = -27 holds
-for the rates only, as in NEURON.  NVRTC builds the whole 14-mechanism set
-for sm_100a."""
+for the rates only, as in NEURON.  The whole 14-mechanism set has the
+mechanism order, parameter indices and state rows of the reference's own
+build of the model (CParsed/AllModels.cuh), and NVRTC builds it for
+sm_100a."""
 import ctypes as C
 import math
 from pathlib import Path
@@ -100,3 +102,23 @@ def test_whole_cc_set_builds_for_sm100a(ngpu_built, tmp_path, monkeypatch):
     masks = np.array([full, 1 << g.mech_index("pas"), full & ~(1 << g.mech_index("Ca"))], dtype=np.uint32)
     assert L.ngpu_jit_build(g.id, 0, masks.ctypes.data, len(masks), 10, 0, C.byref(n)) == 0, L.ngpu_last_error()
     assert n.value > 0
+
+
+def test_cc_set_layout_matches_reference_build():
+    """Mechanism order, parameter indices and channel-state rows of the
+    generated set against the reference's own build of this model
+    (CParsed/AllModels.cuh CALL_TO_BREAK_CU: CuBreakpointModel_<mech>(...,
+    state_macro(s, ...), param_macro(p, ...), ...)); the calcium pool keeps
+    cai in its own array there and in two state rows (cai, ica) here."""
+    import re
+    g = _gen(sorted(p for p in CC_MODS.glob("*.mod") if p.stem != "branching"))
+    text = (CC_MODS / "CParsed" / "AllModels.cuh").read_text()
+    line = next(ln for ln in text.splitlines() if ln.startswith("#define CALL_TO_BREAK_CU"))
+    calls = re.findall(r"CuBreakpointModel_(\w+)\(([^;]*?)\);", line)
+    assert tuple(name for name, _ in calls) == g.mechs
+    for k, (name, args) in enumerate(calls):
+        params = tuple(int(i) for i in re.findall(r"param_macro\((\d+),", args))
+        assert params == tuple(g.mech_params[k]), name
+        states = re.findall(r"state_macro\((\d+),", args)
+        assert len(states) == (g.state_rows[k] if name != "CaDynamics_E2" else 0), name
+    assert g.n_params == 1 + max(max(p) for p in g.mech_params if p)
