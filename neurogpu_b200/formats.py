@@ -294,11 +294,18 @@ class ReferenceModel:
     raw: dict = field(default_factory=dict)
 
 
-def mechset_for(n_models: int, n_params: int) -> tuple[MechSet, list[int], list[int] | None]:
+def mechset_for(n_models: int, n_params: int, mechset=None) -> tuple[MechSet, list[int], list[int] | None]:
     """Library mechanism set for a reference build, the library mechanism of
     each of the file's boolModel rows, and (when the reference build's
     parameter list differs) the library parameter index of each file
-    parameter."""
+    parameter.  A set given as `mechset` (e.g. one generated from the
+    model's .mod files, whose mechanism and parameter order is the reference
+    build's) is taken as is when its sizes match the files'."""
+    if mechset is not None:
+        if mechset.n_mech != n_models or mechset.n_params != n_params:
+            raise ValueError(f"mechanism set {getattr(mechset, 'name', '?')} has {mechset.n_mech} mechanisms and "
+                             f"{mechset.n_params} parameters; the files have {n_models} and {n_params}")
+        return mechset, list(range(n_models)), None
     if n_params == TTPC.n_params and n_models == TTPC.n_mech:
         return TTPC, list(range(TTPC.n_mech)), None
     if n_params == MAINEN.n_params and n_models <= MAINEN.n_mech:
@@ -311,11 +318,11 @@ def mechset_for(n_models: int, n_params: int) -> tuple[MechSet, list[int], list[
                      f"and {n_params} parameters")
 
 
-def cell_from_basic_const(bc: dict[str, np.ndarray], n_params: int) -> CellModel:
+def cell_from_basic_const(bc: dict[str, np.ndarray], n_params: int, mechset=None) -> CellModel:
     n = int(bc["N"][0])
     ncomps = int(bc["NComps"][0])
     nmod = int(bc["NModels"][0])
-    ms, mech_map, _ = mechset_for(nmod, n_params)
+    ms, mech_map, _ = mechset_for(nmod, n_params, mechset)
     parent = parent_from_ks(bc["Ks"])
     e, f = bc["e"], bc["f"]
     a = f[::-1][:n].copy()        # the reference's f, reversed into node order
@@ -363,9 +370,9 @@ def write_allparams_csv(path: str | os.PathLike, params: np.ndarray) -> None:
             fh.write(", ".join(f"{x:.5E}" for x in p) + ",\n")
 
 
-def map_params(file_params: np.ndarray, n_models: int, ms_params: int) -> np.ndarray:
+def map_params(file_params: np.ndarray, n_models: int, ms_params: int, mechset=None) -> np.ndarray:
     """File parameter order -> library mechanism-set order."""
-    ms, _, pmap = mechset_for(n_models, file_params.shape[1])
+    ms, _, pmap = mechset_for(n_models, file_params.shape[1], mechset)
     if pmap is None:
         return file_params
     out = np.zeros((file_params.shape[0], ms.n_params, file_params.shape[2]), dtype=np.float32)
@@ -399,10 +406,12 @@ def read_rows(path: str | os.PathLike, n_rows: int, n_cols: int) -> np.ndarray:
 
 
 def read_data_dir(data: str | os.PathLike, stim_index: int | None = None,
-                  params_file: str | None = None) -> ReferenceModel:
+                  params_file: str | None = None, mechset=None) -> ReferenceModel:
     """Everything a reference run reads from its Data/ directory.  stim_index:
     the device / stimulus number the reference appends to Stim_raw (argv[1],
-    src/Util.cu:359-364); None reads Stim_raw.csv."""
+    src/Util.cu:359-364); None reads Stim_raw.csv.  mechset: the model's
+    mechanism set when it is none of the built-in ones (a set generated from
+    the model's .mod files by nmodl.generate_from_files, registered)."""
     d = Path(data)
     bc = read_basic_const_segp(d / "BasicConstSegP.csv")
     n_comps = int(bc["NComps"][0])
@@ -417,8 +426,8 @@ def read_data_dir(data: str | os.PathLike, stim_index: int | None = None,
     row = first[1] if has_count else first[0]
     n_params = _csv_line(row).size // n_comps
     fparams = read_params_csv(d / params_file, n_comps, n_params, has_count)
-    cell = cell_from_basic_const(bc, n_params)
-    params = map_params(fparams, n_models, n_params)
+    cell = cell_from_basic_const(bc, n_params, mechset)
+    params = map_params(fparams, n_models, n_params, mechset)
     v_init, _, rec = read_sim_csv(d / "Sim.csv")
     n_stim, nt, loc, area = read_stim_meta(d / "Stim_meta.csv")
     raw_name = "Stim_raw.csv" if stim_index is None else f"Stim_raw{stim_index}.csv"

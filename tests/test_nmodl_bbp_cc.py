@@ -122,3 +122,25 @@ def test_cc_set_layout_matches_reference_build():
         states = re.findall(r"state_macro\((\d+),", args)
         assert len(states) == (g.state_rows[k] if name != "CaDynamics_E2" else 0), name
     assert g.n_params == 1 + max(max(p) for p in g.mech_params if p)
+
+
+def test_cc_data_dir_reads_with_the_generated_set():
+    """The reference's own input files for this model (Data/: 224 nodes in
+    103 compartments, 14 boolModel rows, 26 parameters per compartment) read
+    with the generated set: its mechanism masks are the file's boolModel
+    rows and its parameters the file's, unpermuted.  A set whose sizes do
+    not match the files is refused."""
+    from neurogpu_b200 import formats
+    g = _gen(sorted(p for p in CC_MODS.glob("*.mod") if p.stem != "branching"))
+    data = CC_MODS / "Data"
+    m = formats.read_data_dir(data, mechset=g)
+    c = m.cell
+    assert c.mechset is g and c.n_nodes == 224 and c.n_sections == 103
+    bc = m.raw["basic_const"]
+    np.testing.assert_array_equal(c.mech_mask, (bc["boolModel"].reshape(14, 224) != 0).astype(np.uint8))
+    assert m.params.shape[1:] == (26, 103) and m.params is m.raw["file_params"]
+    assert c.mech_mask.any(axis=1).all()     # every mechanism on some node
+    with pytest.raises(ValueError, match="mechanisms"):
+        formats.read_data_dir(data, mechset=_gen([CC_MODS / "Ca.mod"]))
+    with pytest.raises(ValueError, match="no library mechanism set"):
+        formats.read_data_dir(data)
