@@ -144,3 +144,26 @@ def test_cc_data_dir_reads_with_the_generated_set():
         formats.read_data_dir(data, mechset=_gen([CC_MODS / "Ca.mod"]))
     with pytest.raises(ValueError, match="no library mechanism set"):
         formats.read_data_dir(data)
+
+
+def test_cc_basic_const_regenerates_byte_for_byte(tmp_path):
+    """The reference's BasicConstSegP.csv of this model (224 nodes), read with
+    the generated set into a CellModel and written again: the same bytes;
+    the whole Data/ directory written and read back with the set."""
+    from neurogpu_b200 import formats
+    g = _gen(sorted(p for p in CC_MODS.glob("*.mod") if p.stem != "branching"))
+    data = CC_MODS / "Data"
+    r = formats.read_data_dir(data, mechset=g)
+    bm = r.raw["basic_const"]["boolModel"].reshape(14, -1)
+    out = tmp_path / "BasicConstSegP.csv"
+    formats.write_basic_const_segp(out, r.cell, bm)
+    assert out.read_text() == (data / "BasicConstSegP.csv").read_text()
+    d2 = tmp_path / "Data"
+    formats.write_data_dir(d2, r.cell, r.params, r.amps, r.dts, r.stim_node, r.stim_area, r.rec_nodes, r.v_init,
+                           0.025, bool_model=bm)
+    s = formats.read_data_dir(d2, mechset=g)
+    for k in ("parent", "a", "b", "mech_mask", "section", "cm"):
+        np.testing.assert_array_equal(getattr(s.cell, k), getattr(r.cell, k), err_msg=k)
+    np.testing.assert_allclose(s.params, r.params, rtol=5e-6, atol=0)   # AllParams.csv: %.5E
+    np.testing.assert_array_equal(s.amps, r.amps)
+    np.testing.assert_array_equal(s.dts, r.dts)
