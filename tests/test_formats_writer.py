@@ -128,3 +128,42 @@ def test_root_with_two_children_is_rejected(tmp_path):
     w = configs.passive_cable(n_sets=2, t_stop=1.0)
     with pytest.raises(ValueError, match="more than two children"):
         F.write_basic_const_segp(tmp_path / "x.csv", w.cell)
+
+
+
+REF = Path("/root/reference")
+# parameters of the built-in sets' reference builds, by boolModel row count
+BUILT_IN_PARAMS = {13: 19, 7: 34, 1: 2}      # TTPC, Mainen, single-mechanism passive
+
+
+def _shipped_models():
+    if not REF.exists():
+        return []
+    return sorted(str(p.parent.relative_to(REF)) for p in REF.rglob("Data/BasicConstSegP.csv")
+                  if not p.is_relative_to(REF / "Code") and "CoreNeuron" not in p.parts)
+
+
+@pytest.mark.skipif(not REF.exists(), reason="the reference tree is not present")
+@pytest.mark.parametrize("sub", _shipped_models())
+def test_every_shipped_model_regenerates(sub, tmp_path):
+    """Every model Data/ directory of the reference tree (outside the bare
+    Code/ snapshots, which ship no parameter files): its BasicConstSegP.csv,
+    read into a CellModel with the mechanism set of its build (built-in, or
+    generated from the model's own .mod files) and written again, is the same
+    text.  Parameters are not read here: Figure4_DEAP's AllParams rows (the
+    GA's scratch output) hold 4577-4578 of the build's 19 x 241 values."""
+    from neurogpu_b200 import nmodl
+    d = REF / sub
+    bc = F.read_basic_const_segp(d / "BasicConstSegP.csv")
+    nm = int(bc["NModels"][0])
+    ms = None
+    n_params = BUILT_IN_PARAMS.get(nm)
+    if n_params is None:
+        mods = sorted(q for q in d.parent.glob("*.mod") if q.stem != "branching")
+        ms = nmodl.generate_from_files(mods, name="shipped", celsius=34.0,
+                                       reversal={"na": 50.0, "k": -85.0, "ca": 132.458})
+        n_params = ms.n_params
+    cell = F.cell_from_basic_const(bc, n_params, ms)
+    out = tmp_path / "BasicConstSegP.csv"
+    F.write_basic_const_segp(out, cell, _bool_model(bc))
+    assert out.read_text() == (d / "BasicConstSegP.csv").read_text()
