@@ -76,6 +76,14 @@ class Workload:
                         self.stim_area, self.rec_nodes, self.v_init,
                         None if self.free is None else self.free[:ns], self.seed, dict(self.info))
 
+    def take(self, sets) -> "Workload":
+        """The workload restricted to the parameter sets `sets` (indices into
+        this workload's sets, in the given order), every protocol, every step."""
+        idx = np.asarray(sets, dtype=np.int64).reshape(-1)
+        return Workload(self.name, self.cell, np.ascontiguousarray(self.params[idx]),
+                        self.amps, self.dt, self.stim_node, self.stim_area, self.rec_nodes, self.v_init,
+                        None if self.free is None else self.free[idx], self.seed, dict(self.info))
+
 
 def step_amps(levels, nt: int, dt: float, t_on: float, t_off: float) -> np.ndarray:
     t = np.arange(nt) * dt

@@ -216,6 +216,20 @@ inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, c
     }
     char hex[17];
     snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
+    if (const char* dump = std::getenv("NGPU_JIT_DUMP")) {
+        // the translation unit (and a generated set's header) as compiled,
+        // for offline inspection with nvcc (register use, spills)
+        const std::string base = std::string(dump) + "/" + hex;
+        if (FILE* f = fopen((base + ".cu").c_str(), "wb")) {
+            fwrite(src.data(), 1, src.size(), f);
+            fclose(f);
+        }
+        if (generated)
+            if (FILE* f = fopen((base + "_ngpu_generated.cuh").c_str(), "wb")) {
+                fwrite(generated->data(), 1, generated->size(), f);
+                fclose(f);
+            }
+    }
     const std::string dir = cache_dir();
     const std::string path = dir.empty() ? "" : dir + "/" + hex + ".cubin";
     if (!path.empty()) {

@@ -370,11 +370,17 @@ __device__ __forceinline__ void record(const SimArgs<R>& A, const NodeRec<R>& n,
     if (rec_now && n.rec >= 0) trace[(size_t)n.rec * A.n_inst_pad] = (float)V;
 }
 
+// A voltage that is NaN, infinite or beyond 1e6 mV: the instance has blown up.
+template <typename R>
+__device__ __forceinline__ bool v_bad(R V) {
+    return !(fabs(V) < (R)1e6);
+}
+
 // Back-substitution result x = dV_i of node i: V update (Kahan), dV for the
-// node's far children, recording.
+// node's far children, recording; bad is set when the new V is not finite.
 template <typename R>
 __device__ __forceinline__ void backsub_node(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n, int i,
-                                             R x, bool rec_now, float* trace) {
+                                             R x, bool rec_now, float* trace, int& bad) {
     R* vo = G.vbuf + (size_t)i * 2 * kLanes;
     R V = vo[0], vc = vo[kLanes];
     kahan_add(V, vc, x);
@@ -382,6 +388,7 @@ __device__ __forceinline__ void backsub_node(const SimArgs<R>& A, const Group<R>
     vo[kLanes] = vc;
     if (n.jslot >= 0) G.jx[(size_t)n.jslot * kLanes] = x;
     record(A, n, V, rec_now, trace);
+    bad |= v_bad(V);
 }
 
 template <typename R>
@@ -549,7 +556,7 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
 // blocks of four nodes, four nodes ahead.
 template <typename R>
 __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
-                                             const DevComp& c, bool rec_now, float* trace) {
+                                             const DevComp& c, bool rec_now, float* trace, int& bad) {
     constexpr int kBlk = 4;
     if (c.l >= 0) {
         R xp = G.jx[(size_t)nr[c.u].jslot * kLanes];
@@ -560,7 +567,7 @@ __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>
             const R* row = G.scr + (size_t)i * 3 * kLanes;
             const R xi = row[0] - row[kLanes] * xp + row[2 * kLanes] * xl;
             xp = xi;
-            backsub_node(A, G, nr[i], i, xi, rec_now, trace);
+            backsub_node(A, G, nr[i], i, xi, rec_now, trace, bad);
         }
     }
     R x_prev = 0;
@@ -572,7 +579,7 @@ __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>
         const R xp = n.pslot < 0 ? x_prev : G.jx[(size_t)n.pslot * kLanes];
         const R x = row[0] - row[kLanes] * xp;
         x_prev = x;
-        backsub_node(A, G, n, i, x, rec_now, trace);
+        backsub_node(A, G, n, i, x, rec_now, trace, bad);
     }
 }
 
@@ -708,7 +715,7 @@ __device__ __forceinline__ void skeleton_staged(const SimArgs<R>& A, const Group
         vo[0] = V;
         vo[kLanes] = vc;
         record(A, s, V, rec_now, trace);
-        if (k == 0 && !(fabs(V) < (R)1e6)) bad = 1;  // NaN / Inf / blow-up
+        bad |= v_bad(V);
     }
 }
 
@@ -795,7 +802,7 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
                 vo[0] = V;
                 vo[kLanes] = vc;
                 record(A, s, V, rec_now, trace);
-                if (k == 0 && !(fabs(V) < (R)1e6)) bad = 1;  // NaN / Inf / blow-up
+                bad |= v_bad(V);
             }
         }
         __syncthreads();
@@ -804,7 +811,7 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
             int lo = 0, hi = 0, sep = -1, r = 0, lk = -1;
             if (k < A.n_comps) {
                 const DevComp c = A.comps[k];
-                backsub_item(A, G, nr, c, rec_now, trace);
+                backsub_item(A, G, nr, c, rec_now, trace, bad);
                 lo = c.lo;
                 hi = c.hi;
                 sep = c.l;
@@ -818,7 +825,8 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
         }
         __syncthreads();
     }
-    if (w == 0 && bad) A.bad[G.inst] = 1;
+    // any warp that saw a non-finite voltage of this group's instance (lane)
+    if (bad) A.bad[G.inst] = 1;
 }
 
 template <typename R, int MS>

@@ -16,6 +16,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
+# the reference project's source tree, read by the pins and fixture scripts
+# where it is present (the same variable and default as build_ref.sh)
+REFERENCE_DIR = Path(os.environ.get("NGPU_REFERENCE_DIR", "/root/reference"))
 
 MECHSET_TTPC = 0
 MECHSET_MAINEN = 1

@@ -29,7 +29,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF = Path("/root/reference")
+sys.path.insert(0, str(ROOT / "oracle"))
+from oracle_py import REFERENCE_DIR as REF  # noqa: E402
 
 MODELS = {
     "ttpc512": ("GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/Data",

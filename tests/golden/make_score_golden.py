@@ -22,10 +22,12 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF_SCORES = Path("/root/reference/GUI/score_functions.py")
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(HERE))
+from oracle_py import REFERENCE_DIR  # noqa: E402
+
+REF_SCORES = REFERENCE_DIR / "GUI" / "score_functions.py"
 
 NAMES = ["chi_square_normal", "abs_cumsum_diff", "comp_rest_potential", "comp_width", "comp_width_avg",
          "comp_height", "comp_height_avg", "traj_score_1", "traj_score_2", "traj_score_3", "isi",

@@ -131,7 +131,7 @@ def test_root_with_two_children_is_rejected(tmp_path):
 
 
 
-REF = Path("/root/reference")
+from oracle_py import REFERENCE_DIR as REF
 # parameters of the built-in sets' reference builds, by boolModel row count
 BUILT_IN_PARAMS = {13: 19, 7: 34, 1: 2}      # TTPC, Mainen, single-mechanism passive
 

@@ -30,7 +30,7 @@ from helpers import spike_time_error, subthreshold_error
 
 ROOT = Path(__file__).resolve().parent.parent
 MOD_DIR = ROOT / "tests" / "golden" / "mod"
-REF = Path("/root/reference")
+from oracle_py import REFERENCE_DIR as REF
 TTPC_MODS = REF / "NeuroGPU_Base" / "scripts" / "template"
 MAINEN_MODS = REF / "Figures" / "FigureS4_mainen"
 MAINEN_CONSTANTS = {
