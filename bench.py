@@ -42,6 +42,7 @@ PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 TRAFFIC_FILE = ROOT / "profiles" / "ngpu_jit_advance_ttpc_like_x4096.md"
 # the other model family, for profiling (--model hh_active): its own metric name and ncu summary
+UNEVEN_TRAFFIC_FILE = ROOT / "profiles" / "ngpu_jit_batch_advance_uneven_x8192.md"
 MODELS = {"ttpc_like": (METRIC, TRAFFIC_FILE),
           "hh_active": ("compartment-steps/s (HH 500-compartment x4096)",
                         ROOT / "profiles" / "ngpu_jit_advance_hh_x4096.md")}
@@ -53,18 +54,24 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ngpu", choices=["ngpu", "reference"])
-    ap.add_argument("--chunk", type=int, default=800, help="timesteps per bench step")
+    ap.add_argument("--chunk", type=int, default=800,
+                    help="timesteps per bench step (uneven_batch: per launch within the run's graph)")
+    ap.add_argument("--uneven-ms", type=float, default=500.0, help="uneven_batch: simulated ms per bench step")
+    ap.add_argument("--uneven-sets", type=int, default=8192, help="uneven_batch: parameter sets over the four trees")
     ap.add_argument("--n-sets", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=2000, help="timesteps of the end-to-end run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-sets", type=int, default=16)
-    ap.add_argument("--cpu-sample-steps", type=int, default=400)
+    ap.add_argument("--cpu-sample-sets", type=int, default=64)
+    ap.add_argument("--cpu-sample-steps", type=int, default=800)
     ap.add_argument("--ga-pop", type=int, default=8192)
     ap.add_argument("--ga-gens", type=int, default=20)
+    ap.add_argument("--ga-fits", type=int, default=3, help="ga: targets fitted (the line reports the median)")
+    ap.add_argument("--ga-train", type=int, default=200_000, help="ga: the surrogate's training simulations")
+    ap.add_argument("--ga-epochs", type=int, default=30)
     ap.add_argument("--model", default="ttpc_like", choices=sorted(MODELS),
                     help="the cell of the default workload: the TTPC-like headline, or the HH-type cell")
-    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga", "ga_ops"],
+    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga", "ga_ops", "gemm"],
                     help="uneven_batch: 8192 sets over 200/800/1500/3000-compartment trees x 5 protocols, "
                          "one launch per chunk, the run captured as a CUDA graph (auxiliary line)")
     return ap.parse_args()
@@ -87,14 +94,18 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_comp_step(model: str = "ttpc_like"):
-    """DRAM bytes per compartment-step of the advance kernel from the
-    committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum)."""
+def traffic_per_comp_step_file(path: Path):
+    """DRAM bytes per compartment-step of an advance kernel from a committed
+    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum)."""
     try:
-        m = re.search(r"traffic_bytes_per_compartment_step:\s*([0-9.eE+-]+)", MODELS[model][1].read_text())
+        m = re.search(r"traffic_bytes_per_compartment_step:\s*([0-9.eE+-]+)", path.read_text())
         return float(m.group(1)) if m else None
     except Exception:
         return None
+
+
+def traffic_per_comp_step(model: str = "ttpc_like"):
+    return traffic_per_comp_step_file(MODELS[model][1])
 
 
 class ClockSampler:
@@ -198,20 +209,36 @@ def barrier(world: int):
         dist.barrier()
 
 
+def _oracle_rate(sub, threads: int, precision: str) -> tuple[float, float]:
+    """(compartment-steps/s, seconds) of one oracle run of workload `sub`."""
+    import oracle_py
+    t = time.perf_counter()
+    oracle_py.run_workload(sub, precision=precision, n_threads=threads)
+    el = time.perf_counter() - t
+    return sub.compartment_steps() / el, el
+
+
 def cpu_baseline(w, n_sets: int, n_steps: int) -> dict:
-    """Oracle (FP64 C restatement, OpenMP over instances) on a bounded sample."""
+    """The oracle (the C restatement of the reference's step, OpenMP over
+    instances) on bounded samples of the same workload: FP64 on every host
+    thread (the value), the FP32 build on every thread, and FP64 on one
+    thread."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle_py
     sub = w.subset(n_sets=n_sets, nt=n_steps)
     threads = os.cpu_count() or 1
     oracle_py.run_workload(sub.subset(n_sets=1, n_stim=1, nt=10), n_threads=threads)  # warm
-    t = time.perf_counter()
-    oracle_py.run_workload(sub, n_threads=threads)
-    el = time.perf_counter() - t
+    v64, el64 = _oracle_rate(sub, threads, "f64")
+    v32, el32 = _oracle_rate(sub, threads, "f32")
+    one = w.subset(n_sets=1, nt=n_steps)
+    v1, el1 = _oracle_rate(one, 1, "f64")
     cs = sub.compartment_steps()
-    return {"value": cs / el, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": v64, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{sub.n_sets} sets x {sub.n_stim} stimuli x {n_steps} steps of the same "
-                      f"{w.cell.n_nodes}-compartment model ({cs:.3e} compartment-steps, {el:.1f} s, FP64)"}
+                      f"{w.cell.n_nodes}-compartment model ({cs:.3e} compartment-steps, {el64:.1f} s, FP64)",
+            "fp32_all_cores": {"value": v32, "seconds": el32, "sample": "the same sample, FP32 build"},
+            "fp64_one_core": {"value": v1, "seconds": el1, "cores": 1,
+                              "sample": f"1 set x {one.n_stim} stimuli x {n_steps} steps, FP64"}}
 
 
 def run_reference(args):
@@ -238,8 +265,9 @@ def run_reference(args):
         "metric": MODELS[args.model][0], "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": args.model, "n_nodes": w.cell.n_nodes, "n_sets": args.n_sets,
-                   "n_stim": w.n_stim, "dt_ms": w.dt},
+        "config": {"workload": args.model, "n_nodes": w.cell.n_nodes, "n_sets": sub.n_sets,
+                   "n_stim": w.n_stim, "dt_ms": w.dt, "timesteps_per_step": sub.nt,
+                   "sample_of": f"{args.n_sets} sets x {w.n_stim} protocols (rate per compartment-step)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{sub.n_sets} sets x {sub.n_stim} stimuli x {sub.nt} steps per step"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -249,14 +277,18 @@ def run_reference(args):
 
 
 def run_uneven(args):
-    """Config-4 line: the uneven batch, autotuned warps and items per warp per morphology, init +
-    `chunk` timesteps of every member captured once as a CUDA graph; each
-    timed step replays it.  Inputs are resident; the state exceeds L2."""
+    """Config-4 line: the uneven batch (8192 sets over 200/800/1500/3000-
+    compartment HH-type trees x 5 protocols), autotuned warps and items per
+    warp per morphology.  One bench step is the whole run -- init and every
+    `--chunk`-step launch of the 500 ms protocols (20,000 steps) -- captured
+    once as a CUDA graph and replayed.  Warm-up: `--warmup` replays of a
+    400-step graph, then one untimed run of the full graph (its capture).
+    Inputs are resident; the state exceeds L2."""
     import torch
     from neurogpu_b200 import _ffi, autotune, configs
     from neurogpu_b200.sim import Batch, Model, Simulator
     rank, world, local = dist_setup(args.gpus)
-    ws = configs.uneven_batch(n_sets=8192, t_stop=max(args.chunk, 150) * 0.025)
+    ws = configs.uneven_batch(n_sets=args.uneven_sets, t_stop=args.uneven_ms)
     sims, tuned = [], {}
     for w in ws:
         m = Model(w.cell)
@@ -270,9 +302,11 @@ def run_uneven(args):
         sims.append(s)
     batch = Batch(sims)
     stream = torch.cuda.Stream()
-    nt = min(args.chunk, ws[0].nt)
+    nt = ws[0].nt
+    chunk = min(args.chunk, nt)
     for _ in range(args.warmup):
-        batch.run_graph(ws[0].v_init, nt, nt, stream)
+        batch.run_graph(ws[0].v_init, min(400, nt), chunk, stream)
+    batch.run_graph(ws[0].v_init, nt, chunk, stream)  # captures the full run's graph
     stream.synchronize()
     barrier(world)
     clocks = ClockSampler(local) if rank == 0 else None
@@ -283,65 +317,107 @@ def run_uneven(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        batch.run_graph(ws[0].v_init, nt, nt, stream)
+        batch.run_graph(ws[0].v_init, nt, chunk, stream)
     ev1.record(stream)
     stream.synchronize()
     launches = int(_ffi.lib().ngpu_launch_count(0))
     clk = clocks.stop() if clocks else None
-    cs = sum(w.cell.n_nodes * w.n_sets * w.n_stim for w in ws) * nt * args.steps
-    rate, el_s = weak_scaling_rate(cs, ev0.elapsed_time(ev1) / 1e3, world)
+    cs_step = sum(w.cell.n_nodes * w.n_sets * w.n_stim for w in ws) * nt
+    rate, el_s = weak_scaling_rate(cs_step * args.steps, ev0.elapsed_time(ev1) / 1e3, world)
     el_ms = el_s * 1e3
     bad = sum(s.n_bad() for s in sims)
+    # roofline: bytes per compartment-step as in the default line (algorithmic,
+    # or the DRAM bytes ncu measured for the batch kernel where fewer)
+    peak, peak_kind = hbm_peak()
+    bc = sum(w.cell.algorithmic_bytes_per_step() * w.n_sets * w.n_stim for w in ws) / \
+        sum(w.cell.n_nodes * w.n_sets * w.n_stim for w in ws)
+    tpcs = traffic_per_comp_step_file(UNEVEN_TRAFFIC_FILE)
+    bytes_cs = bc if tpcs is None else min(bc, tpcs)
+    ach = bytes_cs * cs_step * args.steps / el_s / 1e9
     if rank == 0:
         print(json.dumps({
-            "metric": "compartment-steps/s (uneven batch x8192, 5 protocols)", "value": rate,
+            "metric": f"compartment-steps/s (uneven batch x{args.uneven_sets}, 5 protocols)", "value": rate,
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": "uneven_batch", "trees": [w.cell.n_nodes for w in ws],
                        "sets_per_tree": ws[0].n_sets, "protocols": ws[0].n_stim, "timesteps_per_step": nt,
-                       "warps_and_items_per_warp": tuned, "graph": "init + one batch launch per step, replayed",
+                       "simulated_ms_per_step": nt * ws[0].dt, "launch_chunk": chunk,
+                       "warps_and_items_per_warp": tuned,
+                       "graph": "init + every chunk of the run, one graph, replayed once per step",
                        "l2": "state larger than L2 (no flush)"},
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_source": peak_kind, "bytes_per_compartment_step": bytes_cs,
+                         "algorithmic_bytes_per_compartment_step": bc, "dram_bytes_per_compartment_step": tpcs,
+                         "traffic": None if tpcs is None else tpcs * cs_step * args.steps,
+                         "note": "graph time (all launches of the run), not one launch"},
             "gpu_launches": launches, "clocks": clk, "non_finite_instances": bad}))
     batch.close()
 
 
 def run_ga(args):
     """Config-5 line: GA time-to-score, surrogate-screened vs plain, on one
-    GPU.  Both fit the same 12 parameters of the 500-node HH-type cell to a
-    target's features over 3 step protocols (500 ms, dt 0.025 ms).  The plain
-    GA simulates every offspring for `ga_gens` generations; its final best
-    score is the target.  The screened GA simulates only the surrogate's top
-    10 % of offspring (its wall time includes simulating its training set and
-    training the network) and runs until it reaches the target or until the
-    plain GA's total wall time has passed.  value = the screened GA's time to
-    the target (s); null if it did not reach it within that time."""
+    GPU.  The cell: the 500-node HH-type cell, 12 free parameters (8
+    conductances, 4 rate constants), 3 step protocols of 500 ms at dt 0.025
+    ms.  The surrogate (4-layer MLP, width 512, GELU; in = 12 parameters +
+    protocol one-hot, out = the 20 features) is trained once for the cell on
+    `--ga-train` simulations drawn over the whole search space -- independent
+    of any target, so one training serves every fit of the cell -- with the
+    project's BF16 tcgen05 kernels.  Then, for each of `--ga-fits` targets
+    (seeded parameter vectors): the plain GA (population `--ga-pop`, every
+    offspring simulated, `--ga-gens` generations, every step on the device)
+    sets the target score, its final best; the screened GA (the network
+    ranks the offspring, the top 10 % are simulated, the network checked and
+    fine-tuned every generation, every step on the device) runs until it
+    reaches that score or until the plain GA's wall time has passed.
+    value = the median over the fits of (screened time to the plain GA's
+    final best score) / (plain GA wall time); null if a fit did not reach
+    it.  The training cost is reported beside it, with the number of fits
+    after which it has paid for itself."""
+    import torch
     from neurogpu_b200 import ga
-    prob = ga.FitProblem()
-    plain = ga.run_plain(prob, args.ga_pop, args.ga_gens, seed=1)
-    sims_plain = prob.sim_count
-    prob.sim_count = 0
-    target = plain.best[-1]
-    scr = ga.run_screened(prob, args.ga_pop, 10 * args.ga_gens, seed=1, target=target,
-                          time_budget=plain.time[-1])
-    t_scr = scr.time_to(target)
-    # the plain GA's own time to the best score the screened GA reached, for context
+    torch.cuda.set_device(0)
+    cell_prob = ga.FitProblem()
+    fit = ga.train_surrogate(cell_prob, n_train=args.ga_train, epochs=args.ga_epochs, seed=0)
+    fits = []
+    for k in range(args.ga_fits):
+        tu = np.random.default_rng(100 + k).uniform(-0.8, 0.8, cell_prob.n_params)
+        prob = ga.FitProblem(target_u=tu)
+        plain = ga.run_device(prob, args.ga_pop, args.ga_gens, seed=k + 1)
+        sims_plain = prob.sim_count
+        prob.sim_count = 0
+        target = plain.best[-1]
+        scr = ga.run_screened_device(prob, fit.net, args.ga_pop, 10 * args.ga_gens, seed=k + 1, target=target,
+                                     time_budget=plain.time[-1])
+        t_scr = scr.time_to(target)
+        fits.append({
+            "target_u": [round(float(x), 4) for x in tu],
+            "plain": {"final_best": target, "seconds": plain.time[-1], "simulations": sims_plain,
+                      "best_per_generation": plain.best, "time_per_generation": plain.time},
+            "screened": {"final_best": scr.best[-1], "seconds": scr.time[-1], "generations": len(scr.best),
+                         "simulations": prob.sim_count, "best_per_generation": scr.best,
+                         "time_per_generation": scr.time, "time_to_plain_final_best": t_scr,
+                         "surrogate_error_per_generation": [(g, round(e, 4), m) for g, e, m in scr.notes]},
+            "time_ratio": None if t_scr is None else t_scr / plain.time[-1]})
+    ratios = [f["time_ratio"] for f in fits]
+    value = None if any(r is None for r in ratios) else float(np.median(ratios))
+    saved = [f["plain"]["seconds"] - (f["screened"]["time_to_plain_final_best"] or f["plain"]["seconds"])
+             for f in fits]
+    train_s = fit.sim_seconds + fit.train_seconds
     print(json.dumps({
-        "metric": "GA time-to-score (surrogate-screened vs plain)", "value": t_scr, "unit": "s",
-        "higher_is_better": False, "n_gpus": 1, "steps": len(scr.best), "warmup": 0,
+        "metric": "GA time-to-score ratio (surrogate-screened / plain)", "value": value, "unit": "ratio",
+        "higher_is_better": False, "n_gpus": 1, "steps": len(fits), "warmup": 0,
         "dtype": "f32 sim, bf16 net", "data": "synthetic (seeded)", "vs_baseline": None,
         "config": {"workload": "ga", "population": args.ga_pop, "plain_generations": args.ga_gens,
                    "model": "hh 500 compartments, 12 parameters, 3 protocols x 500 ms", "screen_keep": 0.1,
-                   "target": "the plain GA's final best score", "screened_budget_s": plain.time[-1]},
-        "plain": {"final_best": target, "seconds": plain.time[-1], "simulations": sims_plain,
-                  "best_per_generation": plain.best, "time_per_generation": plain.time},
-        "screened": {"final_best": scr.best[-1], "seconds": scr.time[-1], "generations": len(scr.best),
-                     "simulations": prob.sim_count, "best_per_generation": scr.best,
-                     "time_per_generation": scr.time,
-                     "time_to_plain_final_best": t_scr,
-                     "surrogate_error_per_generation": [(g, round(e, 4), k) for g, e, k in scr.notes]},
-        "plain_time_to_screened_best": plain.time_to(scr.best[-1]),
-        "time_ratio": None if t_scr is None else t_scr / plain.time[-1]}))
+                   "fits": args.ga_fits, "target": "each fit's plain GA final best score",
+                   "surrogate_training_simulations": args.ga_train},
+        "surrogate_training": {"simulations": fit.n_train, "simulation_seconds": fit.sim_seconds,
+                               "training_seconds": fit.train_seconds, "epochs": args.ga_epochs,
+                               "final_loss": fit.final_loss,
+                               "fits_to_pay_back": None if min(saved) <= 0 else train_s / float(np.mean(saved))},
+        "time_ratio_per_fit": ratios, "fits": fits}), flush=True)
+    return 0
 
 
 def run_ga_ops(args):
@@ -404,6 +480,81 @@ def run_ga_ops(args):
         "steps_ms": out}))
 
 
+def run_gemm(args):
+    """The surrogate network's hand-written tcgen05 BF16 GEMM (ngpu_gemm_bf16_tn,
+    FP32 accumulation in tensor memory) at the network's training shapes
+    (batch 8192, width 512: forward layers, the weight gradients over the
+    batch) and at square sizes, against torch.matmul (cuBLAS) on the same
+    operands.  Device time with CUDA events over `--steps` calls after
+    `--warmup`; value = TFLOP/s of the 8192^3 GEMM, frac of the measured
+    cuBLAS bf16 peak (MEASURED_PEAKS.json bf16_tflops, burst)."""
+    import torch
+    from neurogpu_b200 import _ffi
+    L = _ffi.lib()
+    try:
+        peak = float(json.loads(PEAKS_FILE.read_text())["bf16_tflops"])
+        peak_kind = "measured"
+    except Exception:
+        peak, peak_kind = 1590.0, "fallback"
+
+    def dev_ms(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    rows = {}
+    g = torch.Generator(device="cuda").manual_seed(0)
+    # (name, M, N, K, bn, epilogue): epilogue 0 store fp32, 1 bias + GELU (three outputs)
+    shapes = [("fwd_hidden_8192x512x512", 8192, 512, 512, 128, 1), ("fwd_input_8192x512x64", 8192, 512, 64, 128, 1),
+              ("fwd_out_8192x32x512", 8192, 32, 512, 32, 0), ("dW_512x512x8192", 512, 512, 8192, 128, 0),
+              ("square_4096", 4096, 4096, 4096, 256, 0), ("square_8192", 8192, 8192, 8192, 256, 0)]
+    for name, M, N, K, bn, epi in shapes:
+        A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+        B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+        out = torch.empty(M, N, device="cuda", dtype=torch.float32)
+        ob = torch.empty(M, N, device="cuda", dtype=torch.bfloat16)
+        obt = torch.empty(N, M, device="cuda", dtype=torch.bfloat16)
+        bias = torch.zeros(N, device="cuda", dtype=torch.float32)
+        st = torch.cuda.current_stream().cuda_stream
+
+        def ours():
+            _ffi.check("ngpu_gemm_bf16_tn", L.ngpu_gemm_bf16_tn(
+                A.data_ptr(), B.data_ptr(), M, N, K, K, K, epi, bn, out.data_ptr(),
+                ob.data_ptr() if epi == 1 else None, obt.data_ptr() if epi == 1 else None, N, M,
+                bias.data_ptr() if epi == 1 else None, None, st))
+        ms = dev_ms(ours)
+        ref = torch.matmul(A.float(), B.float().t()) if M * N * K <= 4096 ** 3 else None
+        ours()
+        torch.cuda.synchronize()
+        err = None
+        if ref is not None:
+            got = out if epi == 0 else out - bias
+            err = float((got - ref).abs().max() / ref.abs().max())
+        ms_cublas = dev_ms(lambda: torch.matmul(A, B.t()))
+        fl = 2.0 * M * N * K
+        rows[name] = {"ms": ms, "tflops": fl / ms / 1e9, "cublas_ms": ms_cublas,
+                      "cublas_tflops": fl / ms_cublas / 1e9, "bn": bn,
+                      "epilogue": "bias+gelu (f32, bf16, bf16^T)" if epi == 1 else "store f32",
+                      "max_rel_err_vs_fp32": err}
+        del A, B, out, ob, obt
+    v = rows["square_8192"]["tflops"]
+    print(json.dumps({
+        "metric": "tcgen05 BF16 GEMM TFLOP/s (8192^3)", "value": v, "unit": "TFLOP/s", "higher_is_better": True,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "bf16 (fp32 accumulate)",
+        "data": "synthetic (seeded normal)", "vs_baseline": None,
+        "config": {"workload": "gemm", "surrogate": "MLP width 512, batch 8192"},
+        "roofline": {"bound": "tensor", "achieved": v, "peak": peak, "unit": "TFLOP/s", "frac": v / peak,
+                     "peak_source": peak_kind},
+        "shapes": rows}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -414,6 +565,8 @@ def main():
         return run_ga_ops(args)
     if args.workload == "uneven_batch":
         return run_uneven(args)
+    if args.workload == "gemm":
+        return run_gemm(args)
     import torch
     from neurogpu_b200 import _ffi
     from neurogpu_b200.sim import Model, Simulator, run
@@ -466,13 +619,18 @@ def main():
     value, el_s = weak_scaling_rate(comp_steps_rank, ev0.elapsed_time(ev1) / 1e3, world)
     el_ms = el_s * 1e3
 
-    # roofline of the advance kernel: algorithmic bytes per launch / launch time
-    bytes_per_step = w.cell.algorithmic_bytes_per_step() * n_inst  # one timestep, all instances
-    alg_bytes_launch = bytes_per_step * args.chunk
-    achieved_gbs = alg_bytes_launch / (per_launch_ms / 1e3) / 1e9
+    # roofline of the advance kernel: bytes per launch / launch time.  The
+    # bytes are the algorithmic B_c per compartment-step, or the DRAM bytes
+    # ncu measured where fewer reach DRAM (parameter rows shared by many
+    # nodes are read from L2): only bytes that move are credited.
     peak, peak_kind = hbm_peak()
+    bc = w.cell.algorithmic_bytes_per_step() / w.cell.n_nodes
     tpcs = traffic_per_comp_step(args.model)
-    traffic = None if tpcs is None else tpcs * w.cell.n_nodes * n_inst * args.chunk
+    bytes_cs = bc if tpcs is None else min(bc, tpcs)
+    cs_launch = w.cell.n_nodes * n_inst * args.chunk
+    achieved_gbs = bytes_cs * cs_launch / (per_launch_ms / 1e3) / 1e9
+    achieved_alg_gbs = bc * cs_launch / (per_launch_ms / 1e3) / 1e9
+    traffic = None if tpcs is None else tpcs * cs_launch
 
     # end to end through the public host-buffer entry point (ngpu_run)
     e2e = None
@@ -509,8 +667,12 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": traffic,
                          "peak_source": peak_kind,
-                         "algorithmic_bytes_per_compartment_step":
-                             w.cell.algorithmic_bytes_per_step() / w.cell.n_nodes},
+                         "bytes_per_compartment_step": bytes_cs,
+                         "bytes_basis": "algorithmic" if bytes_cs == bc else "dram (ncu), below algorithmic",
+                         "algorithmic_bytes_per_compartment_step": bc,
+                         "dram_bytes_per_compartment_step": tpcs,
+                         "frac_algorithmic": achieved_alg_gbs / peak,
+                         "launch_ms": per_launch_ms},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -42,6 +42,8 @@ enum {
  * Figures/FigureS4_mainen/CParsed/AllModels.cu for the Mainen cell). */
 enum { NGPU_MECHSET_TTPC = 0, NGPU_MECHSET_MAINEN = 1, NGPU_MECHSET_GENERATED = 2 /* first defined set */ };
 enum { NGPU_FP32 = 0, NGPU_FP64 = 1 };
+/* How instances map onto the GPU (ngpu_sim_create_layout). */
+enum { NGPU_LAYOUT_LANE_INSTANCE = 0, NGPU_LAYOUT_WARP_INSTANCE = 1 };
 
 typedef struct ngpu_model ngpu_model;
 typedef struct ngpu_sim ngpu_sim;
@@ -186,6 +188,29 @@ int ngpu_sim_create_ex(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t pr
  * the reference (one thread per compartment group, no split). */
 int ngpu_sim_create_shaped(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
                            int32_t items_per_warp, ngpu_sim **out);
+/*
+ * As ngpu_sim_create with the layout chosen by the caller.
+ *   NGPU_LAYOUT_LANE_INSTANCE  one lane per instance, 32 instances per CTA,
+ *       cta_warps warps sharing the tree (1..16; above 8 only through the
+ *       runtime-compiled kernel, bounded for 3 CTAs per SM), items work
+ *       items per warp (1..8); 0 = the library's choice.  With up to 8 warps
+ *       this is ngpu_sim_create_shaped.
+ *       A B200 fills from about 148 x 32 x 2 instances on.
+ *   NGPU_LAYOUT_WARP_INSTANCE  one warp per instance (its lanes share the
+ *       instance's tree, split into `items` work items, 1..512; 0 = 32),
+ *       cta_warps instances per CTA (1..8; 0 = enough CTAs for every SM):
+ *       for batches too small to fill the GPU 32 instances per CTA.
+ * Both compute the same step (U/CudaStuff.cu:227-330) on the same buffers;
+ * traces, features and checks read the same.  The reference's kernel is
+ * one CTA per parameter set, 32 threads x NILP compartments each
+ * (U/CudaStuff.cu:164-167); neurogpu_b200.autotune times both layouts.
+ * Batches (ngpu_batch_create) hold lane-instance simulations.
+ */
+int ngpu_sim_create_layout(ngpu_model *m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t layout,
+                           int32_t cta_warps, int32_t items, ngpu_sim **out);
+/* The simulation's layout, CTA warps and items (as ngpu_sim_create_layout's
+ * arguments, with the library's choices filled in); any pointer may be NULL. */
+int ngpu_sim_layout(const ngpu_sim *s, int32_t *layout, int32_t *cta_warps, int32_t *items);
 
 /*
  * Several simulations in one launch (morphologies of different sizes, one

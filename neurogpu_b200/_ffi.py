@@ -15,6 +15,8 @@ LIB_PATH = _HERE / "libngpu.so"
 
 NGPU_FP32 = 0
 NGPU_FP64 = 1
+NGPU_LAYOUT_LANE_INSTANCE = 0
+NGPU_LAYOUT_WARP_INSTANCE = 1
 MECHSET_TTPC = 0
 MECHSET_MAINEN = 1
 
@@ -56,6 +58,8 @@ def lib() -> C.CDLL:
             "ngpu_sim_create": (C.c_int, [P, I32, I32, I32, P]),
             "ngpu_sim_create_ex": (C.c_int, [P, I32, I32, I32, I32, P]),
             "ngpu_sim_create_shaped": (C.c_int, [P, I32, I32, I32, I32, I32, P]),
+            "ngpu_sim_create_layout": (C.c_int, [P, I32, I32, I32, I32, I32, I32, P]),
+            "ngpu_sim_layout": (C.c_int, [P, P, P, P]),
             "ngpu_batch_create": (C.c_int, [P, I32, P]),
             "ngpu_batch_destroy": (C.c_int, [P]),
             "ngpu_batch_init": (C.c_int, [P, F32, P]),

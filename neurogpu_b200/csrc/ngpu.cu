@@ -429,6 +429,9 @@ struct ngpu_sim {
     unsigned long long* d_phash = nullptr;  // [ptab_rows] hash of each parameter row
     std::vector<int32_t> prow_canon;  // parameter block start -> the block it reads (identical values)
     bool ch_prefetch = true;      // the runtime-specialised kernel compiles the channel-pass L2 prefetch in
+    int layout = NGPU_LAYOUT_LANE_INSTANCE;  // lane = instance, or one warp per instance (thread-item)
+    int ti_warps = 4;             // thread-item layout: instances (warps) per CTA
+    int ti_items = 32;            // thread-item layout: work items per instance's tree
 };
 
 // Rows (state and parameter) a node's channel update reads, on average; the
@@ -437,6 +440,15 @@ struct ngpu_sim {
 // the TTPC-like cell (~12) 7 % faster without it.
 constexpr double kPrefetchRowsPerNode = 20.0;
 
+// Thread-item layout: work items per instance at most / by default, and the
+// SM count the default CTA shape spreads a small batch over.
+constexpr int kMaxTiItems = 512;
+// Lane-instance CTAs of up to 16 warps (runtime-compiled kernels bounded for
+// 3 CTAs per SM; the ahead-of-time kernels take up to kMaxWarps).
+constexpr int kMaxWideWarps = 16;
+constexpr int kDefaultTiItems = 32;
+constexpr int kSmCount = 148;
+
 static double rows_per_node(const ngpu_model* m) {
     return m->n > 0 ? (double)(m->state_vars + m->param_reads) / m->n : 0.0;
 }
@@ -444,7 +456,8 @@ static double rows_per_node(const ngpu_model* m) {
 // CTAs per SM that `smem` bytes of dynamic shared memory and W warps of 80
 // registers allow (228 KB per SM, 1 KB of it reserved per CTA).
 static int ctas_per_sm(size_t smem, int W) {
-    const int by_regs = 65536 / (kLanes * W * 80);
+    // kernels of up to 8 warps use 80 registers; wider ones are compiled for 3 CTAs per SM
+    const int by_regs = W > kMaxWarps ? 3 : 65536 / (kLanes * W * 80);
     const int by_smem = (int)((228 * 1024) / (smem + 1024));
     return std::max(1, std::min(std::min(by_regs, by_smem), 64 / W));
 }
@@ -482,6 +495,7 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.n_rec = s->n_rec_unique;
     A.rec_every = s->rec_every;
     A.n_inst_pad = s->n_pad;
+    A.n_inst = s->n_inst;
     A.v_init = s->v_init;
     A.bad = s->d_bad;
     A.err = s->d_err;
@@ -498,7 +512,7 @@ static SimArgs<R> make_args(ngpu_sim* s) {
 template <typename R>
 static cudaError_t launch_init(ngpu_sim* s, cudaStream_t st) {
     SimArgs<R> A = make_args<R>(s);
-    const int threads = kLanes * s->n_warps;
+    const int threads = kLanes * std::min(s->n_warps, kMaxWarps);  // any warp count serves the init
     if (s->jit) {
         void* args[] = {(void*)&A};
         const cudaError_t e = cudaLaunchKernel((const void*)s->jit->init, dim3(s->n_groups), dim3(threads), args, 0, st);
@@ -511,8 +525,30 @@ static cudaError_t launch_init(ngpu_sim* s, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// Thread-item layout: one warp per instance, ti_warps instances per CTA.
+template <typename R>
+static cudaError_t launch_advance_ti(ngpu_sim* s, int t0, int n, cudaStream_t st) {
+    SimArgs<R> A = make_args<R>(s);
+    const int W = s->ti_warps;
+    const int ctas = (s->n_inst + W - 1) / W;
+    const size_t smem = SmemPlan<R>::ti_bytes(s->m->n, (int)s->part.seps.size(), W);
+    cudaError_t e;
+    const void* k;
+    if (s->jit) k = (const void*)s->jit->advance_ti;
+    else if (s->m->mechset == NGPU_MECHSET_TTPC) k = (const void*)k_sim_advance_ti<R, 0>;
+    else k = (const void*)k_sim_advance_ti<R, 1>;
+    if (!k) return cudaErrorInvalidDeviceFunction;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {(void*)&A, (void*)&t0, (void*)&n};
+    e = cudaLaunchKernel(k, dim3(ctas), dim3(kLanes * W), args, smem, st);
+    g_launches++;
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <typename R>
 static cudaError_t launch_advance(ngpu_sim* s, int t0, int n, cudaStream_t st) {
+    if (s->layout == NGPU_LAYOUT_WARP_INSTANCE) return launch_advance_ti<R>(s, t0, n, st);
     SimArgs<R> A = make_args<R>(s);
     const int threads = kLanes * s->n_warps;
     const size_t smem = SmemPlan<R>::bytes(s->m->n, (int)s->part.seps.size(), s->s2_stage);
@@ -822,7 +858,8 @@ int ngpu_model_arrays(const ngpu_model* m, int32_t* parent, double* a, double* b
 int ngpu_model_partition(const ngpu_model* m, int32_t n_warps, int32_t* sep_flag, int32_t* item,
                          int32_t* jslot, int32_t* pslot, int32_t* n_jslots) {
     if (!m) return fail(NGPU_E_INVALID, "null model");
-    if (n_warps < 1 || n_warps > kMaxWarps) return fail(NGPU_E_INVALID, "n_warps out of range");
+    // warps of a CTA, or (up to kMaxTiItems) the lanes of one instance's warp
+    if (n_warps < 1 || n_warps > kMaxTiItems) return fail(NGPU_E_INVALID, "n_warps out of range");
     Partition P = make_partition(m, n_warps);
     std::vector<int> owner(m->n, -1), sep(m->n, 0);
     for (int i : P.seps) sep[i] = 1;
@@ -847,7 +884,8 @@ int ngpu_model_split_info(const ngpu_model* m, int32_t n_warps, int32_t* perm, i
                           int32_t* comps, int32_t max_comps, int32_t* n_seps, int32_t* seps,
                           int32_t max_seps, int32_t* jslot, int32_t* pslot) {
     if (!m) return fail(NGPU_E_INVALID, "null model");
-    if (n_warps < 1 || n_warps > kMaxWarps) return fail(NGPU_E_INVALID, "n_warps out of range");
+    // warps of a CTA, or (up to kMaxTiItems) the lanes of one instance's warp
+    if (n_warps < 1 || n_warps > kMaxTiItems) return fail(NGPU_E_INVALID, "n_warps out of range");
     Partition P = make_partition(m, n_warps);
     if (perm)
         for (int i = 0; i < m->n; ++i) perm[i] = m->perm[i];
@@ -895,12 +933,26 @@ int ngpu_sim_create_ex(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t pr
 
 int ngpu_sim_create_shaped(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t n_warps,
                            int32_t items_per_warp, ngpu_sim** out) {
-    if (!out) return fail(NGPU_E_INVALID, "out is null");
-    if (items_per_warp < 0 || items_per_warp > 8)
-        return fail(NGPU_E_INVALID, "items_per_warp must be 0 (automatic) or 1..8");
     if (n_warps < 0 || n_warps > kMaxWarps)
         return fail(NGPU_E_INVALID, "n_warps must be 0 (automatic) or 1.." + std::to_string(kMaxWarps));
+    return ngpu_sim_create_layout(m, n_sets, n_stim, precision, NGPU_LAYOUT_LANE_INSTANCE, n_warps, items_per_warp,
+                                  out);
+}
+
+int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision, int32_t layout,
+                           int32_t cta_warps, int32_t items, ngpu_sim** out) {
+    if (!out) return fail(NGPU_E_INVALID, "out is null");
     *out = nullptr;
+    if (layout != NGPU_LAYOUT_LANE_INSTANCE && layout != NGPU_LAYOUT_WARP_INSTANCE)
+        return fail(NGPU_E_INVALID, "layout must be NGPU_LAYOUT_LANE_INSTANCE or NGPU_LAYOUT_WARP_INSTANCE");
+    const bool ti = layout == NGPU_LAYOUT_WARP_INSTANCE;
+    const int32_t n_warps = cta_warps, items_per_warp = ti ? 0 : items;
+    if (ti ? (items < 0 || items > kMaxTiItems) : (items < 0 || items > 8))
+        return fail(NGPU_E_INVALID, ti ? "items must be 0 (automatic) or 1.." + std::to_string(kMaxTiItems)
+                                       : std::string("items_per_warp must be 0 (automatic) or 1..8"));
+    const int max_w = ti ? kMaxWarps : kMaxWideWarps;
+    if (n_warps < 0 || n_warps > max_w)
+        return fail(NGPU_E_INVALID, "n_warps must be 0 (automatic) or 1.." + std::to_string(max_w));
     if (!m) return fail(NGPU_E_INVALID, "null model");
     if (n_sets < 1 || n_stim < 1) return fail(NGPU_E_INVALID, "need n_sets >= 1 and n_stim >= 1");
     if (precision != NGPU_FP32 && precision != NGPU_FP64)
@@ -926,7 +978,7 @@ int ngpu_sim_create_shaped(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
     int rc = NGPU_OK;
     // warps per CTA and the tree split over them
     int W = std::min(8, std::max(1, m->n / 48));
-    if (const char* ev = getenv("NGPU_WARPS")) W = std::max(1, std::min(kMaxWarps, atoi(ev)));
+    if (const char* ev = getenv("NGPU_WARPS")) W = std::max(1, std::min(kMaxWideWarps, atoi(ev)));
     if (n_warps > 0) W = n_warps;
     W = std::min(W, m->n);
     s->n_warps = W;
@@ -937,9 +989,31 @@ int ngpu_sim_create_shaped(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
     s->items_per_warp = s->ch_prefetch ? 2 : 3;
     if (const char* ev = getenv("NGPU_ITEMS_PER_WARP")) s->items_per_warp = std::max(1, std::min(8, atoi(ev)));
     if (items_per_warp > 0) s->items_per_warp = items_per_warp;
-    s->part = make_partition(m, W, s->items_per_warp);
-    s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W)
-                                         : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W);
+    if (ti) {
+        // one warp per instance: the tree split into ti_items items for the
+        // warp's lanes; CTAs of ti_warps instances, enough CTAs for every SM
+        // first (the layout serves batches too small to fill the GPU)
+        s->layout = NGPU_LAYOUT_WARP_INSTANCE;
+        s->n_warps = kMaxWarps;  // the initialisation kernel's warps (any count serves it)
+        s->ti_items = items > 0 ? items : kDefaultTiItems;
+        s->ti_items = std::min(s->ti_items, m->n);
+        s->ti_warps = n_warps > 0 ? n_warps
+                                  : std::min(kMaxWarps, std::max(1, (s->n_inst + kSmCount - 1) / kSmCount));
+        s->part = make_partition(m, s->ti_items, 1);
+        s->s2_stage = 0;
+        const size_t need = precision == NGPU_FP64
+                                ? SmemPlan<double>::ti_bytes(m->n, (int)s->part.seps.size(), s->ti_warps)
+                                : SmemPlan<float>::ti_bytes(m->n, (int)s->part.seps.size(), s->ti_warps);
+        if (need > 227 * 1024) {
+            sim_free(s);
+            return fail(NGPU_E_INVALID, "thread-item layout: " + std::to_string(need) +
+                                            " bytes of shared memory per CTA; use fewer instances per CTA or items");
+        }
+    } else {
+        s->part = make_partition(m, W, s->items_per_warp);
+        s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W)
+                                             : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W);
+    }
     const int nj = s->part.n_jslots;
 #define ALLOC(field, type, bytes)                              \
     s->field = (type)dmalloc((bytes), &rc);                    \
@@ -995,6 +1069,15 @@ int ngpu_sim_create_shaped(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
 
 int ngpu_sim_destroy(ngpu_sim* s) {
     sim_free(s);
+    return NGPU_OK;
+}
+
+int ngpu_sim_layout(const ngpu_sim* s, int32_t* layout, int32_t* cta_warps, int32_t* items) {
+    if (!s) return fail(NGPU_E_INVALID, "null sim");
+    const bool ti = s->layout == NGPU_LAYOUT_WARP_INSTANCE;
+    if (layout) *layout = s->layout;
+    if (cta_warps) *cta_warps = ti ? s->ti_warps : s->n_warps;
+    if (items) *items = ti ? s->ti_items : s->items_per_warp;
     return NGPU_OK;
 }
 
@@ -1353,11 +1436,16 @@ static int sim_upload_nodes(ngpu_sim* s) {
         } else {
             const std::vector<uint32_t> all = model_masks(m), picked = ngpu_jit::pick_masks(all, kMaxClasses);
             s->jit = ngpu_jit::module(m->mechset, s->precision == NGPU_FP64, picked, gs ? &gs->source : nullptr,
-                                      s->ch_prefetch, s->folds, masks_cover(picked, all, s->ch_prefetch));
+                                      s->ch_prefetch, s->folds, masks_cover(picked, all, s->ch_prefetch),
+                                      s->layout == NGPU_LAYOUT_WARP_INSTANCE,
+                                      s->layout == NGPU_LAYOUT_LANE_INSTANCE ? std::max(8, s->n_warps) : 8);
         }
         if (gs && !s->jit)
             return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
                                          "' runs only through runtime compilation: " + ngpu_jit::last_log());
+        if (!s->jit && s->layout == NGPU_LAYOUT_LANE_INSTANCE && s->n_warps > kMaxWarps)
+            return fail(NGPU_E_CUDA, "CTAs of more than " + std::to_string(kMaxWarps) +
+                                         " warps run only through runtime compilation: " + ngpu_jit::last_log());
     }
     std::vector<int> uniq(s->n_rec_unique, -1);
     for (size_t r = 0; r < s->rec_nodes.size(); ++r) uniq[s->rec_cols[r]] = s->rec_nodes[r];
@@ -1499,6 +1587,11 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
         if (sims[k]->m->mechset != sims[0]->m->mechset)
             return fail(NGPU_E_INVALID, "a batch needs one mechanism set");
         if (sims[k]->batch) return fail(NGPU_E_INVALID, "a simulation belongs to one batch at a time");
+        if (sims[k]->layout != NGPU_LAYOUT_LANE_INSTANCE)
+            return fail(NGPU_E_INVALID, "a batch holds lane-instance simulations only");
+        if (sims[k]->n_warps > kMaxWarps)
+            return fail(NGPU_E_INVALID, "a batch holds simulations of at most " + std::to_string(kMaxWarps) +
+                                            " warps per CTA");
     }
     ngpu_batch* b = new (std::nothrow) ngpu_batch();
     if (!b) return fail(NGPU_E_NOMEM, "host allocation failed");
@@ -2080,6 +2173,7 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     A.n_rec = n_rec_u;
     A.rec_every = 1;
     A.n_inst_pad = n_pad;
+    A.n_inst = n_inst;
     A.v_init = v_init;
     A.bad = (int*)(base + o_bad);
     A.err = (int*)(base + o_err);

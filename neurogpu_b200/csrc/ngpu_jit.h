@@ -51,12 +51,15 @@ struct Module {
     bool fp64 = false;
     bool prefetch = true;                   // channel-pass L2 prefetch compiled in (NGPU_CH_PREFETCH)
     bool complete = false;                  // the masks cover every node: no generic path (NGPU_CLASSES_COMPLETE)
+    bool ti = false;                        // the thread-item layout's advance kernel compiled in
+    int adv_warps = 8;                      // the advance kernels' CTA size bound (warps), 3 CTAs per SM
     std::vector<uint32_t> masks;            // class k runs the code for masks[k]
     cudaLibrary_t lib = nullptr;
     cudaKernel_t init = nullptr;           // (SimArgs<R>)
     cudaKernel_t advance = nullptr;        // (SimArgs<R>, int t0, int n_steps)
     cudaKernel_t batch_init = nullptr;     // (BatchArgs<R>)
     cudaKernel_t batch_advance = nullptr;  // (BatchArgs<R>, int t0, int n_steps)
+    cudaKernel_t advance_ti = nullptr;     // (SimArgs<R>, int t0, int n_steps), thread-item layout
 };
 
 struct Nvrtc {
@@ -117,13 +120,18 @@ inline bool enabled() {
 // batch) over `masks`.  ms: the kernel template's mechanism set (0 TTPC,
 // 1 Mainen, 2 a generated set, whose channel code comes in as the extra
 // header ngpu_generated.cuh).  prefetch: the channel pass's L2 prefetch.
+// ti: also the thread-item layout's advance kernel.
+// adv_warps: the advance kernels are bounded for CTAs of up to this many
+// warps, 3 per SM (8: 80 registers; 10: 64; 12: 56; 16: 40).
 inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks, bool prefetch = true,
-                          const Folds& folds = {}, bool complete = false) {
+                          const Folds& folds = {}, bool complete = false, bool ti = false, int adv_warps = 8) {
     std::string list;
     for (size_t k = 0; k < masks.size(); ++k) list += (k ? ", " : "") + std::to_string(masks[k]) + "u";
     const std::string m = std::to_string(ms);
     const std::string R = fp64 ? "double" : "float";
-    const std::string lb = "__launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)";
+    const std::string lb = adv_warps > 8
+                               ? "__launch_bounds__(" + std::to_string(32 * adv_warps) + ", 3)"
+                               : "__launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)";
     std::string fold;
     if (!folds.empty()) {
         fold = "#include \"param_fold.cuh\"\nnamespace ngpu {\n";
@@ -162,7 +170,14 @@ inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks,
            "    const int k = ngpu::batch_member(B.cta0, B.n);\n"
            "    ngpu::advance_body<" + R + ", " + m + ", JitClasses>(B.sim[k], blockIdx.x - B.cta0[k], t0, n_steps,\n"
            "                                                   smem, ctr);\n"
-           "}\n";
+           "}\n" +
+           (ti ? "extern \"C\" __global__ void __launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_TI_MIN_BLOCKS)\n"
+                 "ngpu_jit_advance_ti(ngpu::SimArgs<" + R + "> A, int t0, int n_steps) {\n"
+                 "    extern __shared__ __align__(128) char smem[];\n"
+                 "    __shared__ int q[2 * ngpu::kMaxWarps];\n"
+                 "    ngpu::advance_body_ti<" + R + ", " + m + ", JitClasses>(A, t0, n_steps, smem, q);\n"
+                 "}\n"
+               : std::string());
 }
 
 inline uint64_t fnv1a(uint64_t h, const std::string& s) {
@@ -184,13 +199,13 @@ inline std::string cache_dir() {
 // code of a generated mechanism set (ms 2), or nullptr.
 inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, const std::string* generated,
                         const std::string& arch, std::vector<char>* out, std::string* err, bool prefetch = true,
-                        const Folds& folds = {}, bool complete = false) {
+                        const Folds& folds = {}, bool complete = false, bool ti = false, int adv_warps = 8) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) {
         *err = last_log();
         return false;
     }
-    const std::string src = source(ms, fp64, masks, prefetch, folds, complete);
+    const std::string src = source(ms, fp64, masks, prefetch, folds, complete, ti, adv_warps);
     std::vector<std::string> opt_s = {"--gpu-architecture=sm_" + arch, "-std=c++17",
                                       "-lineinfo"};
     int vmaj = 0, vmin = 0;
@@ -291,7 +306,7 @@ inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, c
 // code is *generated.  Modules live until the process exits.
 inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>& masks,
                             const std::string* generated, bool prefetch = true, const Folds& folds = {},
-                            bool complete = false) {
+                            bool complete = false, bool ti = false, int adv_warps = 8) {
     if (!generated && (!enabled() || masks.empty())) return nullptr;
     if (generated && !enabled()) {
         last_log() = "runtime compilation is off (NGPU_JIT=0)";
@@ -299,7 +314,8 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     }
     std::lock_guard<std::mutex> lock(mu());
     static std::map<std::string, std::unique_ptr<Module>> cache;
-    std::string key = std::to_string(mechset) + (fp64 ? "d" : "f") + (prefetch ? "p" : "n") + (complete ? "c:" : "g:");
+    std::string key = std::to_string(mechset) + (fp64 ? "d" : "f") + (prefetch ? "p" : "n") + (complete ? "c" : "g") +
+                      (ti ? "t" : "") + (adv_warps > 8 ? "w" + std::to_string(adv_warps) : std::string()) + ":";
     for (uint32_t m : masks) key += std::to_string(m) + ",";
     for (const auto& f : folds) key += ";" + std::to_string(f.first) + "=" + float_literal(f.second);
     auto it = cache.find(key);
@@ -320,7 +336,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     std::string err;
     const std::string arch = std::to_string(maj) + std::to_string(min) + "a";
     if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err, prefetch, folds,
-                     complete)) {
+                     complete, ti, adv_warps)) {
         last_log() = err;
         cache[key] = nullptr;
         return nullptr;
@@ -330,12 +346,15 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     mod->fp64 = fp64;
     mod->prefetch = prefetch;
     mod->complete = complete;
+    mod->ti = ti;
+    mod->adv_warps = adv_warps;
     mod->masks = masks;
     cudaError_t e = cudaLibraryLoadData(&mod->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->init, mod->lib, "ngpu_jit_init");
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->advance, mod->lib, "ngpu_jit_advance");
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->batch_init, mod->lib, "ngpu_jit_batch_init");
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->batch_advance, mod->lib, "ngpu_jit_batch_advance");
+    if (e == cudaSuccess && ti) e = cudaLibraryGetKernel(&mod->advance_ti, mod->lib, "ngpu_jit_advance_ti");
     if (e != cudaSuccess) {
         last_log() = std::string("loading the compiled kernels: ") + cudaGetErrorString(e);
         cudaGetLastError();

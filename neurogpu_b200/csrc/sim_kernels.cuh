@@ -129,6 +129,7 @@ struct SimArgs {
     int n_rec;
     int rec_every;
     int n_inst_pad;
+    int n_inst;            // instances holding a (set, stimulus) pair; the rest pad the last group
     float v_init;
     int* bad;              // [n_inst_pad] non-finite voltage flags
     int* err;              // device error word
@@ -216,9 +217,9 @@ struct Group {  // per-CTA pointers (lane offset included)
     int inst;
 };
 
+// Pointers of group g at lane `lane` (instance g * 32 + lane).
 template <typename R>
-__device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A, int g) {
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ Group<R> group_lane(const SimArgs<R>& A, int g, int lane) {
     const size_t N = (size_t)A.n_nodes;
     Group<R> p;
     p.vbuf = A.vbuf + (size_t)g * N * 2 * kLanes + lane;
@@ -232,6 +233,12 @@ __device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A, int g) {
     return p;
 }
 
+// Lane = instance: this thread's lane of group g.
+template <typename R>
+__device__ __forceinline__ Group<R> group_of(const SimArgs<R>& A, int g) {
+    return group_lane(A, g, (int)(threadIdx.x & 31));
+}
+
 // Shared memory: the node records, then (s2_stage) the skeleton's staging
 // rows, [n_seps][32] each: two FP64 accumulators (excess, right-hand side)
 // and five R rows (coupling A / later c, coupling B / later r, axial term
@@ -243,6 +250,14 @@ struct SmemPlan {
     }
     static __host__ __device__ size_t bytes(int n_nodes, int n_seps = 0, int stage = 0) {
         return nodes(n_nodes) + (stage ? (size_t)n_seps * 32 * (2 * sizeof(double) + 5 * sizeof(R)) : 0);
+    }
+    // thread-item layout: the node records, then per warp (one instance) the
+    // skeleton's staging rows, [n_seps] each of the same seven
+    static __host__ __device__ size_t ti_stage(int n_seps) {
+        return ((size_t)n_seps * (2 * sizeof(double) + 5 * sizeof(R)) + 15) / 16 * 16;
+    }
+    static __host__ __device__ size_t ti_bytes(int n_nodes, int n_seps, int warps) {
+        return nodes(n_nodes) + (size_t)warps * ti_stage(n_seps);
     }
 };
 
@@ -554,16 +569,18 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
 // (dV_i = r_i - c_i dV_parent + w_i dV_l, from separator u down), then the
 // light nodes; V update of each node.  Rows are prefetched into L2 in
 // blocks of four nodes, four nodes ahead.
-template <typename R>
+// TI: thread-item layout (lanes on different items; no lane-0 prefetch).
+template <typename R, bool TI = false>
 __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
                                              const DevComp& c, bool rec_now, float* trace, int& bad) {
     constexpr int kBlk = 4;
     if (c.l >= 0) {
         R xp = G.jx[(size_t)nr[c.u].jslot * kLanes];
         const R xl = G.jx[(size_t)nr[c.l].jslot * kLanes];
-        prefetch_backsub(G, c.r, min(kBlk, c.l - c.r));
+        if constexpr (!TI) prefetch_backsub(G, c.r, min(kBlk, c.l - c.r));
         for (int i = c.r; i < c.l; ++i) {
-            if (((i - c.r) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.l - i - kBlk));
+            if constexpr (!TI)
+                if (((i - c.r) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.l - i - kBlk));
             const R* row = G.scr + (size_t)i * 3 * kLanes;
             const R xi = row[0] - row[kLanes] * xp + row[2 * kLanes] * xl;
             xp = xi;
@@ -571,9 +588,10 @@ __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>
         }
     }
     R x_prev = 0;
-    prefetch_backsub(G, c.lo, min(kBlk, c.hi - c.lo));
+    if constexpr (!TI) prefetch_backsub(G, c.lo, min(kBlk, c.hi - c.lo));
     for (int i = c.lo; i < c.hi; ++i) {
-        if (((i - c.lo) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.hi - i - kBlk));
+        if constexpr (!TI)
+            if (((i - c.lo) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.hi - i - kBlk));
         const NodeRec<R> n = nr[i];
         const R* row = G.scr + (size_t)i * 3 * kLanes;
         const R xp = n.pslot < 0 ? x_prev : G.jx[(size_t)n.pslot * kLanes];
@@ -591,7 +609,7 @@ __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>
 // skeleton: its row goes to the skeleton), and, for a segment (lk >= 0),
 // the spine sep-1 .. r.  Every channel update of a step goes through this
 // one loop, so the channel code is inlined once.
-template <typename R, int MS, typename Classes>
+template <typename R, int MS, typename Classes, bool TI = false>
 __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
                                               int lo, int hi, int sep, int r, int lk, R dt, R dtn_inv,
                                               R istim_amp) {
@@ -611,7 +629,7 @@ __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R
     R e_l = 0;
     int vi = -1;  // node whose V was read last as a parent voltage
     R vv = 0;
-    constexpr bool pf = NGPU_CH_PREFETCH != 0;
+    constexpr bool pf = NGPU_CH_PREFETCH != 0 && !TI;
     if (pf && n > 0) prefetch_channels(G, nr[node_at(0)]);
     if (pf && n > 1) prefetch_channels(G, nr[node_at(1)]);
     for (int p = 0; p < n; ++p) {
@@ -719,6 +737,28 @@ __device__ __forceinline__ void skeleton_staged(const SimArgs<R>& A, const Group
     }
 }
 
+// Work item k of a step: an item's back-substitution pass, then its channel
+// pass; k >= n_comps: a separator linked directly to the skeleton (its
+// channel update and its row for the skeleton solve).
+template <typename R, int MS, typename Classes, bool TI>
+__device__ __forceinline__ void run_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr, int k,
+                                         R dt, R dtn_inv, R istim_amp, bool rec_now, float* trace, int& bad) {
+    int lo = 0, hi = 0, sep = -1, r = 0, lk = -1;
+    if (k < A.n_comps) {
+        const DevComp c = A.comps[k];
+        backsub_item<R, TI>(A, G, nr, c, rec_now, trace, bad);
+        lo = c.lo;
+        hi = c.hi;
+        sep = c.l;
+        r = c.r;
+        lk = c.lk;
+    } else {
+        const DevSep sp = A.seps[k - A.n_comps];
+        if (sp.seg < 0) sep = sp.node;  // separators ending a segment are their segment's
+    }
+    channels_item<R, MS, Classes, TI>(A, G, nr, lo, hi, sep, r, lk, dt, dtn_inv, istim_amp);
+}
+
 // Per timestep (two barriers, three with a staged skeleton):
 //   S2  warp 0 solves the skeleton (the separators, a few dozen nodes) with
 //       the reduced couplings of the segments, and updates (and records)
@@ -807,22 +847,8 @@ __device__ __forceinline__ void advance_body(const SimArgs<R>& A, int g, int t0,
         }
         __syncthreads();
         // S3: items
-        for (int k = next_item(q); k < n_items; k = next_item(q)) {
-            int lo = 0, hi = 0, sep = -1, r = 0, lk = -1;
-            if (k < A.n_comps) {
-                const DevComp c = A.comps[k];
-                backsub_item(A, G, nr, c, rec_now, trace, bad);
-                lo = c.lo;
-                hi = c.hi;
-                sep = c.l;
-                r = c.r;
-                lk = c.lk;
-            } else {
-                const DevSep sp = A.seps[k - A.n_comps];
-                if (sp.seg < 0) sep = sp.node;  // separators ending a segment are their segment's
-            }
-            channels_item<R, MS, Classes>(A, G, nr, lo, hi, sep, r, lk, dt, dtn_inv, istim_amp);
-        }
+        for (int k = next_item(q); k < n_items; k = next_item(q))
+            run_item<R, MS, Classes, false>(A, G, nr, k, dt, dtn_inv, istim_amp, rec_now, trace, bad);
         __syncthreads();
     }
     // any warp that saw a non-finite voltage of this group's instance (lane)
@@ -834,6 +860,147 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_ADV_MIN_BLOCKS) k_sim
     extern __shared__ __align__(128) char smem[];
     __shared__ int ctr[2];
     advance_body<R, MS, NoClasses>(A, blockIdx.x, t0, n_steps, smem, ctr);
+}
+
+// ---------------------------------------------------------------------------
+// Thread-item layout, for batches too small to fill the GPU 32 instances per
+// CTA: one warp per instance, a CTA holds blockDim.x / 32 instances.
+//
+// The instance's tree is split for the warp's 32 lanes (make_partition with
+// 32 units): every lane takes work items from the warp's queue in
+// shared memory, largest first, and runs on each the same two passes as the
+// layout above; lane 0 solves the skeleton from shared memory between
+// __syncwarp()s, the other lanes load and write back its rows.  Storage and
+// its [group][row][32 lanes] layout are those of the lane-instance layout
+// (one simulation's buffers, traces and features serve both): a lane touches
+// its instance's element of each row, four bytes, which the L1 and L2 serve
+// well at the batch sizes this layout is for.  The channel code is the same
+// inlined call site; lanes on nodes of different mechanism classes take
+// turns through it.
+
+// S2 of one instance (warp): staged rows, lane 0's serial elimination and
+// back-substitution over the separators, all lanes' write-back.
+template <typename R>
+__device__ __forceinline__ void skeleton_ti(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
+                                            char* st, bool rec_now, float* trace, int& bad) {
+    using M = Math<R>;
+    const int lane = threadIdx.x & 31;
+    const int S = A.n_seps;
+    double* acx = (double*)st;
+    double* acr = acx + S;
+    R* sA = (R*)(acr + S);
+    R* sB = sA + S;
+    R* sE = sB + S;
+    R* sV = sE + S;
+    R* sC = sV + S;
+    for (int k = lane; k < S; k += kLanes) {
+        const DevSep sp = A.seps[k];
+        const NodeRec<R> s = nr[sp.node];
+        const R* row = G.scr + (size_t)sp.node * 3 * kLanes;
+        double* ja = G.jacc + (size_t)(2 * s.jslot) * kLanes;
+        const R* vo = G.vbuf + (size_t)sp.node * 2 * kLanes;
+        double x = (double)row[0] + ja[0], rh = (double)row[kLanes] + ja[kLanes];
+        R a = s.a, b = s.b, e = row[2 * kLanes];
+        if (sp.seg >= 0) {
+            const R* sv = G.sepv + (size_t)k * 4 * kLanes;
+            a = sv[0];
+            b = sv[kLanes];
+            x += (double)sv[2 * kLanes];
+            rh += (double)sv[3 * kLanes];
+            e = 0;  // the segment already folded this node's axial term in
+        }
+        ja[0] = 0.0;
+        ja[kLanes] = 0.0;
+        acx[k] = x;
+        acr[k] = rh;
+        sA[k] = a;
+        sB[k] = b;
+        sE[k] = e;
+        sV[k] = vo[0];
+        sC[k] = vo[kLanes];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int k = S - 1; k >= 0; --k) {
+            const R x = (R)acx[k], rh = (R)acr[k];
+            if (k == 0) {
+                sB[0] = M::dv(rh, x);
+                break;
+            }
+            const R Acp = sA[k], Bcp = sB[k], e_up = sE[k];
+            const R inv = M::rc(x - Acp);
+            const R rr = rh * inv, cc = Acp * inv;
+            sA[k] = cc;
+            sB[k] = rr;
+            const int p = A.seps[k].par;
+            acx[p] += (double)(-Bcp * (x * inv));
+            acr[p] += (double)(e_up - Bcp * rr);
+        }
+        for (int k = 0; k < S; ++k) sE[k] = k == 0 ? sB[0] : sB[k] - sA[k] * sE[A.seps[k].par];
+    }
+    __syncwarp();
+    for (int k = lane; k < S; k += kLanes) {
+        const DevSep sp = A.seps[k];
+        const NodeRec<R> s = nr[sp.node];
+        const R x = sE[k];
+        G.jx[(size_t)s.jslot * kLanes] = x;
+        R* vo = G.vbuf + (size_t)sp.node * 2 * kLanes;
+        R V = sV[k], vc = sC[k];
+        kahan_add(V, vc, x);
+        vo[0] = V;
+        vo[kLanes] = vc;
+        record(A, s, V, rec_now, trace);
+        bad |= v_bad(V);
+    }
+    __syncwarp();
+}
+
+// n_steps timesteps of instance blockIdx.x * (blockDim.x / 32) + warp.
+// q: [warps][2] shared-memory queue counters.
+template <typename R, int MS, typename Classes>
+__device__ __forceinline__ void advance_body_ti(const SimArgs<R>& A, int t0, int n_steps, char* smem, int* q) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const NodeRec<R>* nr = stage_nodes(A, smem);  // the CTA's only block-wide barrier
+    const int inst = blockIdx.x * nw + w;
+    if (inst >= A.n_inst) return;
+    const Group<R> G = group_lane(A, inst / kLanes, inst % kLanes);
+    char* st = smem + SmemPlan<R>::nodes(A.n_nodes) + (size_t)w * SmemPlan<R>::ti_stage(A.n_seps);
+    int* const qw = q + 2 * w;
+    if (lane == 0) {
+        qw[0] = 0;
+        qw[1] = 0;
+    }
+    __syncwarp();
+    int bad = 0;
+    const int n_items = A.n_comps + A.n_seps;
+    for (int t = t0; t < t0 + n_steps; ++t) {
+        // this step's queue is qw[t & 1]; the other was last used by the
+        // previous step's queue, which the warp barrier ended
+        int* const qs = &qw[t & 1];
+        if (lane == 0) qw[(t + 1) & 1] = 0;
+        R dt, dtn_inv, istim_amp;
+        bool rec_now;
+        float* trace;
+        step_inputs(A, G, t, false, dt, dtn_inv, istim_amp, rec_now, trace);
+        skeleton_ti<R>(A, G, nr, st, rec_now, trace, bad);
+        for (int k = atomicAdd(qs, 1); k < n_items; k = atomicAdd(qs, 1))
+            run_item<R, MS, Classes, true>(A, G, nr, k, dt, dtn_inv, istim_amp, rec_now, trace, bad);
+        __syncwarp();
+    }
+    if (bad) A.bad[G.inst] = 1;
+}
+
+// The thread-item layout runs small batches (a few warps per SM at most):
+// registers are plentiful, so the kernel is compiled for 2 CTAs per SM.
+#ifndef NGPU_TI_MIN_BLOCKS
+#define NGPU_TI_MIN_BLOCKS 2
+#endif
+template <typename R, int MS>
+__global__ void __launch_bounds__(kLanes * kMaxWarps, NGPU_TI_MIN_BLOCKS)
+    k_sim_advance_ti(SimArgs<R> A, int t0, int n_steps) {
+    extern __shared__ __align__(128) char smem[];
+    __shared__ int q[2 * kMaxWarps];
+    advance_body_ti<R, MS, NoClasses>(A, t0, n_steps, smem, q);
 }
 
 // Several simulations (morphologies of different sizes, one mechanism set)

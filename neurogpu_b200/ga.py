@@ -351,3 +351,101 @@ def run_screened(prob: FitProblem, pop_size: int, generations: int, keep_frac: f
             break
     res.best_u = pop[0]
     return res
+
+
+# ------------------------------------------- surrogate trained once, screened GA on the device
+def inputs_device(u, n_stim: int):
+    """_inputs on the device: (parameters, protocol one-hot) rows [n * n_stim, 12 + n_stim] float32 for
+    u [n, 12] (a CUDA tensor)."""
+    import torch
+    n, k = u.shape
+    x = torch.zeros((n * n_stim, k + n_stim), dtype=torch.float32, device=u.device)
+    x[:, :k] = u.float().repeat_interleave(n_stim, dim=0)
+    x[torch.arange(n * n_stim, device=u.device), k + torch.arange(n_stim, device=u.device).repeat(n)] = 1.0
+    return x
+
+
+@dataclass
+class SurrogateFit:
+    net: object
+    n_train: int          # simulated parameter sets (each over every protocol)
+    sim_seconds: float    # wall time of the training simulations
+    train_seconds: float  # wall time of the network's training
+    final_loss: float
+
+
+def train_surrogate(prob: FitProblem, n_train: int = 200_000, epochs: int = 30, batch: int = 4096,
+                    lr: float = 1e-3, seed: int = 0) -> SurrogateFit:
+    """The surrogate of prob's cell and protocols: n_train parameter sets
+    drawn uniformly over the whole search space (independent of any fit's
+    target, so one network serves every fit of this cell), simulated on the
+    device, features kept in HBM, and the network trained on them with its
+    own BF16 tensor-core kernels."""
+    import torch
+
+    from .surrogate import SurrogateMLP
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    t0 = time.perf_counter()
+    u = torch.rand((n_train, prob.n_params), generator=gen, device="cuda", dtype=torch.float64) * 2.0 - 1.0
+    f = prob.simulate_device(u)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    net = SurrogateMLP(prob.n_params + prob.n_stim, features.N_FEATURES, seed=seed, lr=lr)
+    hist = net.train(inputs_device(u, prob.n_stim), f.reshape(-1, f.shape[-1]).float(), epochs=epochs, batch=batch,
+                     lr=lr, seed=seed)
+    torch.cuda.synchronize()
+    return SurrogateFit(net, n_train, t1 - t0, time.perf_counter() - t1, float(hist[-1]) if hist else float("nan"))
+
+
+def run_screened_device(prob: FitProblem, net, pop_size: int, generations: int, keep_frac: float = 0.1,
+                        err_bound: float = 0.5, tune_epochs: int = 1, seed: int = 0, target: float | None = None,
+                        time_budget: float | None = None) -> GAResult:
+    """The surrogate-screened GA with a trained network, every step on the
+    device: offspring by the variation kernel (csrc/ga.cuh), the network's
+    predicted features and scores for all of them, the best-predicted
+    keep_frac simulated, (mu + lambda) truncation among simulated
+    individuals.  Every generation the network's error on the simulated
+    individuals (mean |predicted - simulated| in units of each feature's
+    spread) is measured; above err_bound that generation simulates every
+    offspring instead (the plain GA's step).  The network is fine-tuned on
+    each generation's simulations.  Stops after `generations`, once the best
+    score is <= target, or once time_budget wall seconds have passed.  The
+    host reads two numbers per generation (the error and the best score)."""
+    import torch
+
+    from .ga_device import DeviceGA, select_truncation
+    ga = DeviceGA(prob.n_params, seed=seed)
+    res = GAResult()
+    t0 = time.perf_counter()
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    pop = torch.rand((pop_size, prob.n_params), generator=gen, device="cuda", dtype=torch.float64) * 2.0 - 1.0
+    score = prob.score_device(prob.simulate_device(pop))
+    rank = torch.zeros(pop_size, dtype=torch.int32, device="cuda")
+    _, _, _, scale = prob._tables()
+    n_keep = max(1, int(round(keep_frac * pop_size)))
+    for g in range(generations):
+        kids = ga.offspring(pop, rank, -score, pop_size, g)
+        pred = net.predict(inputs_device(kids, prob.n_stim)).reshape(pop_size, prob.n_stim, -1)
+        order = torch.argsort(prob.score_device(pred))
+        chosen = kids[order[:n_keep]]
+        fk = prob.simulate_device(chosen)
+        err = float(((pred[order[:n_keep]].double() - fk.double()) / scale[None, None, :]).abs().mean())
+        if err > err_bound:  # the network is off here: simulate every offspring
+            rest = kids[order[n_keep:]]
+            chosen, fk = torch.cat([chosen, rest]), torch.cat([fk, prob.simulate_device(rest)])
+            res.notes.append((g, err, "fallback"))
+        else:
+            res.notes.append((g, err, "screened"))
+        if tune_epochs > 0:
+            net.train(inputs_device(chosen, prob.n_stim), fk.reshape(-1, fk.shape[-1]).float(), epochs=tune_epochs,
+                      batch=4096, lr=3e-4, seed=seed + g + 1)
+        allp, alls = torch.cat([pop, chosen]), torch.cat([score, prob.score_device(fk)])
+        idx = select_truncation(alls, pop_size)
+        pop, score = allp[idx], alls[idx]
+        res.best.append(float(score[0]))
+        res.time.append(time.perf_counter() - t0)
+        res.sims.append(prob.sim_count)
+        if (target is not None and res.best[-1] <= target) or (time_budget is not None and res.time[-1] >= time_budget):
+            break
+    res.best_u = pop[0].cpu().numpy()
+    return res

@@ -108,21 +108,31 @@ class Model:
             pass
 
 
+LAYOUTS = {"lane": _ffi.NGPU_LAYOUT_LANE_INSTANCE, "warp": _ffi.NGPU_LAYOUT_WARP_INSTANCE}
+
+
 class Simulator:
     """Resident simulation of n_sets x n_stim instances of one model."""
 
     def __init__(self, model: Model | CellModel, n_sets: int, n_stim: int, precision: str = "fp32",
-                 n_warps: int = 0, items_per_warp: int = 0):
-        """n_warps: warps per CTA (1..8), items_per_warp: work items per warp
-        in the tree split (1..8); 0 = the library's choice for either; see
-        neurogpu_b200.autotune for timing-based selection."""
+                 n_warps: int = 0, items_per_warp: int = 0, layout: str = "lane"):
+        """layout "lane" (one lane per instance, 32 instances per CTA; the
+        default): n_warps warps per CTA share the tree (1..16; above 8 the
+        runtime-compiled kernel, bounded for 3 CTAs per SM), items_per_warp
+        work items per warp (1..8).  layout "warp" (one warp per instance, for
+        batches too small to fill the GPU): n_warps instances per CTA (1..8),
+        items_per_warp the work items the instance's tree is split into
+        (1..512).  0 = the library's choice; see neurogpu_b200.autotune for
+        timing-based selection."""
         self.model = model if isinstance(model, Model) else Model(model)
         self.n_sets, self.n_stim = int(n_sets), int(n_stim)
         self.precision = precision
+        if layout not in LAYOUTS:
+            raise ValueError(f"layout must be one of {sorted(LAYOUTS)}")
         h = C.c_void_p()
-        _ffi.check("ngpu_sim_create_shaped", _ffi.lib().ngpu_sim_create_shaped(
-            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], int(n_warps), int(items_per_warp),
-            C.byref(h)))
+        _ffi.check("ngpu_sim_create_layout", _ffi.lib().ngpu_sim_create_layout(
+            self.model.handle, self.n_sets, self.n_stim, _PREC[precision], LAYOUTS[layout], int(n_warps),
+            int(items_per_warp), C.byref(h)))
         self._h = h
         self.nt = 0
         self.n_rec = 1
@@ -192,6 +202,13 @@ class Simulator:
             self._h, int(site), float(dt), float(stim_on), float(stim_off), float(threshold),
             C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
         return out
+
+    def layout(self) -> dict:
+        """{"layout": "lane" | "warp", "cta_warps": .., "items": ..} with the
+        library's choices filled in (ngpu_sim_layout)."""
+        lay, w, it = C.c_int32(), C.c_int32(), C.c_int32()
+        _ffi.check("ngpu_sim_layout", _ffi.lib().ngpu_sim_layout(self._h, C.byref(lay), C.byref(w), C.byref(it)))
+        return {"layout": {v: k for k, v in LAYOUTS.items()}[lay.value], "cta_warps": w.value, "items": it.value}
 
     def param_folds(self) -> int:
         """Parameters compiled into this simulation's kernel as constants

@@ -24,8 +24,18 @@ The GPU test runs the whole batch and compares these sets.  The sampled
 voltages are the oracle's float64 values rounded to float32 (4e-6 mV at
 100 mV), far below the 0.1 mV bound they are checked against.
 
-Run: python tests/golden/make_long_runs.py [--only name] (about 8 minutes on
-8 cores; the oracle is OpenMP-parallel over instances).
+The model's own sensitivity, for configs 2 and 3: the same sampled sets
+rerun by the FP64 oracle with every parameter nudged by one part in 1e7
+(about one float32 ulp; a seeded random sign per value, rounded to float32),
+and by the oracle's float32 build, each compared with the FP64 run as the
+GPU run is (sens_* and f32_*: spike_ms, mismatches, dv_away_mV at the 1 ms
+samples).  A model whose spike times move this far under perturbations at
+float32 rounding scale cannot be followed more closely by any float32
+arithmetic.
+
+Run: python tests/golden/make_long_runs.py [--only name] [--sensitivity]
+(about 8 minutes on 8 cores, 3 more with --sensitivity; the oracle is
+OpenMP-parallel over instances).
 """
 from __future__ import annotations
 
@@ -86,13 +96,79 @@ def summarise(traces: np.ndarray, dt: float):
     return v, (np.concatenate(spk) if spk else np.zeros(0)), np.asarray(off, dtype=np.int64)
 
 
+SENS_EPS = 1e-7
+
+
+def perturbed(w, eps: float = SENS_EPS, seed: int = 1):
+    """w with every parameter multiplied by 1 +- eps (seeded signs), in float32."""
+    from dataclasses import replace
+    rng = np.random.default_rng(seed)
+    p = w.params.astype(np.float64) * (1.0 + eps * rng.choice([-1.0, 1.0], w.params.shape))
+    return replace(w, params=p.astype(np.float32))
+
+
+def deviation(a: np.ndarray, b: np.ndarray, dt: float, window_ms: float = 2.0, stride: int = 1):
+    """(max spike-time difference over matched spikes, spike-count
+    mismatches, max |a - b| farther than window_ms from any spike) of traces
+    [..., nt], at every stride-th sample."""
+    from helpers import spike_times
+    a2, b2 = a.reshape(-1, a.shape[-1]), b.reshape(-1, b.shape[-1])
+    win = int(round(window_ms / dt))
+    worst_t, mism, worst_v = 0.0, 0, 0.0
+    for x, y in zip(a2, b2):
+        sx, sy = spike_times(x, dt), spike_times(y, dt)
+        if sx.size != sy.size:
+            mism += 1
+        elif sx.size:
+            worst_t = max(worst_t, float(np.max(np.abs(sx - sy))))
+        keep = np.ones(x.size, dtype=bool)
+        for t in np.concatenate([sx, sy]):
+            k = int(t / dt)
+            keep[max(0, k - win):k + win + 1] = False
+        keep[np.arange(x.size) % stride != 0] = False
+        if keep.any():
+            worst_v = max(worst_v, float(np.max(np.abs(x[keep] - y[keep]))))
+    return worst_t, mism, worst_v
+
+
+def sensitivity(name: str, data: dict):
+    import oracle_py
+    (w, idx, _), = workloads()[name]
+    ws = w.take(idx)
+    ref = oracle_py.run_workload(ws)[:, :, 0, :]
+    per = oracle_py.run_workload(perturbed(ws))[:, :, 0, :]
+    t, mism, v = deviation(per, ref, ws.dt, stride=STRIDE)
+    data[f"{name}/sens_eps"] = np.float64(SENS_EPS)
+    data[f"{name}/sens_spike_ms"] = np.float64(t)
+    data[f"{name}/sens_mismatches"] = np.int64(mism)
+    data[f"{name}/sens_dv_away_mV"] = np.float64(v)
+    print(f"{name}: parameters x (1 +- {SENS_EPS:g}): spikes move {t:.4f} ms, {mism} count changes, "
+          f"{v:.4f} mV away from spikes", flush=True)
+    # the oracle's float32 build (storage and channel arithmetic in float32,
+    # libm's correctly rounded functions) against its float64 build
+    f32 = oracle_py.run_workload(ws, precision="f32")[:, :, 0, :]
+    t, mism, v = deviation(f32, ref, ws.dt, stride=STRIDE)
+    data[f"{name}/f32_spike_ms"] = np.float64(t)
+    data[f"{name}/f32_mismatches"] = np.int64(mism)
+    data[f"{name}/f32_dv_away_mV"] = np.float64(v)
+    print(f"{name}: the oracle's float32 build: spikes {t:.4f} ms, {mism} count changes, "
+          f"{v:.4f} mV away from spikes", flush=True)
+
+
 def main():
     import oracle_py
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
+    ap.add_argument("--sensitivity", action="store_true", help="only the sensitivity runs of configs 2 and 3")
     args = ap.parse_args()
     data = dict(np.load(OUT)) if OUT.exists() else {}
     data["stride"] = np.int64(STRIDE)
+    if args.sensitivity:
+        for name in ("hh_500ms", "ttpc_2000ms"):
+            if not args.only or name == args.only:
+                sensitivity(name, data)
+        np.savez_compressed(OUT, **data)
+        return
     for name, parts in workloads().items():
         if args.only and name != args.only:
             continue

@@ -95,6 +95,45 @@ def test_items_per_warp_split_matches_oracle(ngpu_built, refs, cfg, name, items)
     assert err <= TOL_FP64_MV, f"{name}, {items} items per warp: FP64 max|dV| = {err:.3e} mV"
 
 
+@pytest.mark.parametrize("name", ["passive", "hh", "ttpc"])
+def test_warp_layout_fp64_matches_oracle(ngpu_built, refs, cfg, name):
+    """The warp-instance layout (one warp per instance, the tree split over
+    its lanes) computes the same step: FP64 against the oracle."""
+    w = cfg[name]
+    got = _gpu_run(w, "fp64", layout="warp")
+    err = np.max(np.abs(got.astype(np.float64) - refs[name]))
+    assert err <= TOL_FP64_MV, f"{name}, warp layout: FP64 max|dV| = {err:.3e} mV"
+
+
+@pytest.mark.parametrize("name", ["passive", "hh", "ttpc"])
+def test_warp_layout_fp32_matches_oracle(ngpu_built, refs, cfg, name):
+    w = cfg[name]
+    ref = refs[name]
+    got = _gpu_run(w, "fp32", layout="warp").astype(np.float64)
+    sub = subthreshold_error(got, ref, w.dt)
+    st, mism = spike_time_error(got, ref, w.dt)
+    print(f"{name}, warp layout: FP32 away from spikes {sub:.4e} mV, spike-time err {st:.4e} ms, "
+          f"count mismatches {mism}")
+    assert mism == 0 and st <= TOL_SPIKE_MS and sub <= TOL_FP32_MV
+
+
+@pytest.mark.parametrize("name,cta_warps,items", [("hh", 1, 8), ("hh", 3, 64), ("ttpc", 2, 128), ("passive", 8, 16)])
+def test_warp_layout_shapes_match_oracle(ngpu_built, refs, cfg, name, cta_warps, items):
+    """Other CTA shapes and splits of the warp-instance layout, on a ragged
+    instance count (the last CTA partly empty): FP64 against the oracle."""
+    w = cfg[name].subset(n_sets=5)
+    got = _gpu_run(w, "fp64", layout="warp", n_warps=cta_warps, items_per_warp=items)
+    err = np.max(np.abs(got.astype(np.float64) - refs[name][:5]))
+    assert err <= TOL_FP64_MV, f"{name}, warp layout {cta_warps}x{items}: FP64 max|dV| = {err:.3e} mV"
+
+
+def test_warp_layout_chunked_and_deterministic(ngpu_built, cfg):
+    w = cfg["hh"]
+    a = _gpu_run(w, "fp32", layout="warp")
+    b = _gpu_run(w, "fp32", chunks=[1, 999, 2000, w.nt - 3000], layout="warp")
+    assert np.array_equal(a, b)
+
+
 def test_chunked_advance_is_bitwise_identical(ngpu_built, cfg):
     w = cfg["hh"]
     a = _gpu_run(w, "fp32")

