@@ -312,14 +312,18 @@ const char *ngpu_jit_log(void);
  *     sites, and the run must fit the 16 MiB array (nodes x instances x
  *     states plus the nt-sample trace); larger runs are rejected with
  *     NGPU_E_INVALID and a message giving the bytes needed.
- *   Work is enqueued on cuda_stream; the call returns once its small host
- *     copies are done, before the simulation finishes.  Non-finite voltages
+ *   Each call copies its small host tables (node records, work items,
+ *     recording columns) to the array with cudaMemcpyAsync on cuda_stream and
+ *     synchronises cuda_stream before it enqueues the simulation, so all
+ *     earlier work on that stream has finished when the call returns; the
+ *     simulation itself runs on after the call returns.  Non-finite voltages
  *     are not reported.
- *   The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.  All calls share the array and find the
- *     previous call's contents in it (each call resets what it relies on), so
- *     calls that overlap on the GPU race: serialise them.
+ *   Every call looks up the array's device address (cudaGetSymbolAddress)
+ *     with the caller's device current, which allocates nothing; the first
+ *     call on a device also loads the library's kernels onto it, so make that
+ *     first call before any stream capture.  All calls share the array and
+ *     find the previous call's contents in it (each call resets what it
+ *     relies on), so calls that overlap on the GPU race: serialise them.
  */
 int ngpu_run_static(ngpu_model *m, int32_t n_sets, const float *params_dev, int32_t n_stim,
                     int32_t nt, const float *amps_dev, const float *dts_dev, int32_t stim_node,

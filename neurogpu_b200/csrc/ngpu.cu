@@ -392,7 +392,6 @@ struct ngpu_sim {
     void* d_slab = nullptr;
     float* d_ptab = nullptr;
     void* d_scr = nullptr;
-    int* d_err = nullptr;
     DevComp* d_comps = nullptr;
     DevSep* d_seps = nullptr;
     void* d_sepv = nullptr;
@@ -498,7 +497,6 @@ static SimArgs<R> make_args(ngpu_sim* s) {
     A.n_inst = s->n_inst;
     A.v_init = s->v_init;
     A.bad = s->d_bad;
-    A.err = s->d_err;
     A.n_warps = s->n_warps;
     A.comps = s->d_comps;
     A.n_comps = (int)s->part.comps.size();
@@ -913,7 +911,7 @@ int ngpu_model_split_info(const ngpu_model* m, int32_t n_warps, int32_t* perm, i
 static void sim_free(ngpu_sim* s) {
     if (!s) return;
     void* ptrs[] = {s->d_nodes, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc, s->d_jx,
-                    s->d_inst_stim, s->d_bad, s->d_err, s->d_row_param, s->d_row_sec, s->d_amps,
+                    s->d_inst_stim, s->d_bad, s->d_row_param, s->d_row_sec, s->d_amps,
                     s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv, s->d_prange,
                     s->d_phash};
     for (void* p : ptrs)
@@ -1028,7 +1026,6 @@ int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
     ALLOC(d_scr, void*, G * 3 * m->n * L * esz);
     ALLOC(d_jacc, double*, G * 2 * std::max(1, nj) * L * sizeof(double));
     ALLOC(d_jx, void*, G * std::max(1, nj) * L * esz);
-    ALLOC(d_err, int*, sizeof(int));
     ALLOC(d_comps, DevComp*, sizeof(DevComp) * std::max<size_t>(1, s->part.comps.size()));
     ALLOC(d_seps, DevSep*, sizeof(DevSep) * std::max<size_t>(1, s->part.seps.size()));
     ALLOC(d_sepv, void*, G * 4 * std::max<size_t>(1, s->part.seps.size()) * L * esz);
@@ -1046,7 +1043,6 @@ int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
         if (!dc.empty()) cudaMemcpy(s->d_comps, dc.data(), sizeof(DevComp) * dc.size(), cudaMemcpyHostToDevice);
         cudaMemcpy(s->d_seps, ds.data(), sizeof(DevSep) * ds.size(), cudaMemcpyHostToDevice);
     }
-    cudaMemset(s->d_err, 0, sizeof(int));
     std::vector<int> inst_stim(s->n_pad);
     for (int k = 0; k < s->n_pad; ++k) inst_stim[k] = std::min(k, s->n_inst - 1) % n_stim;
     cudaMemcpy(s->d_inst_stim, inst_stim.data(), sizeof(int) * s->n_pad, cudaMemcpyHostToDevice);
@@ -1919,9 +1915,6 @@ int ngpu_sim_check(ngpu_sim* s, int32_t* n_bad, void* cuda_stream) {
     int c = 0;
     for (int i = 0; i < s->n_inst; ++i) c += bad[i] != 0;
     *n_bad = c;
-    int err = 0;
-    NGPU_CUDA(cudaMemcpy(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) return fail(NGPU_E_CUDA, "a shared-memory pipeline wait timed out in the solve phase");
     return NGPU_OK;
 }
 
@@ -1994,29 +1987,19 @@ constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // held by every GPU t
 constexpr int kStaticMaxNodes = 512;
 constexpr int kStaticMaxInstances = 256;
 constexpr int kStaticMaxRec = 16;
-constexpr int kStaticMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-static std::mutex g_static_mu;
-static unsigned char* g_static_addr[kStaticMaxDevices] = {};
-
-// Device address of g_static_scratch on the current device (set-up on first use).
+// Device address of g_static_scratch on the current device, looked up on
+// every call (it allocates nothing, and a device reset that reloads the
+// module moves the array).  In host code the array's name is only a stand-in.
 static int static_scratch_address(unsigned char** out) {
-    int dev = -1;
-    NGPU_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kStaticMaxDevices)
-        return fail(NGPU_E_INVALID, "device ordinal beyond the static-scratch table");
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(NGPU_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
-        g_static_addr[dev] = (unsigned char*)p;
-    }
-    *out = g_static_addr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(NGPU_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    *out = (unsigned char*)p;
     return NGPU_OK;
 }
 
@@ -2119,7 +2102,6 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     const size_t o_seps = take(sizeof(DevSep));
     const size_t o_istim = take(sizeof(int) * n_pad);
     const size_t o_bad = take(sizeof(int) * n_pad);
-    const size_t o_err = take(sizeof(int));
     const size_t o_rowp = take(sizeof(int) * m->row_param.size());
     const size_t o_rows = take(sizeof(int) * m->row_sec.size());
     const size_t o_vbuf = take(G * N * 2 * L * sizeof(float));
@@ -2147,7 +2129,6 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
                               cudaMemcpyHostToDevice, st));
     NGPU_CUDA(cudaMemcpyAsync(base + o_rows, m->row_sec.data(), sizeof(int) * m->row_sec.size(),
                               cudaMemcpyHostToDevice, st));
-    NGPU_CUDA(cudaMemsetAsync(base + o_err, 0, sizeof(int), st));  // left over from an earlier call
     // the copies above read host stack memory: make sure they are done before returning
     NGPU_CUDA(cudaStreamSynchronize(st));
 
@@ -2176,7 +2157,6 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
     A.n_inst = n_inst;
     A.v_init = v_init;
     A.bad = (int*)(base + o_bad);
-    A.err = (int*)(base + o_err);
     A.n_warps = 1;
     A.comps = (const DevComp*)(base + o_comps);
     A.n_comps = n_comps;

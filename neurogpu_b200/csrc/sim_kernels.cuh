@@ -132,7 +132,6 @@ struct SimArgs {
     int n_inst;            // instances holding a (set, stimulus) pair; the rest pad the last group
     float v_init;
     int* bad;              // [n_inst_pad] non-finite voltage flags
-    int* err;              // device error word
     int n_warps;
     const DevComp* comps;  // work items, by decreasing cost
     int n_comps;

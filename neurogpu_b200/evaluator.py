@@ -105,17 +105,38 @@ def _peaks(v: np.ndarray, thr: float) -> np.ndarray:
 
 def efel_features(t: np.ndarray, v: np.ndarray, stim_start: float = STIM_START, stim_end: float = STIM_END,
                   threshold: float = THRESHOLD) -> dict[str, np.ndarray | None]:
-    """The eFEL features efel_ext.py requests (feature_list, :13), per eFEL's
-    definitions: voltage_base = mean V over [0.9 stim_start, stim_start];
-    peak_time = times of the maxima of excursions above threshold;
-    AP_begin = first sample before a peak (after the previous peak) where
-    dV/dt exceeds 10 mV/ms; AP_amplitude = peak V - AP begin V for peaks
-    within the stimulus; min_AHP = the minimum between consecutive peaks
-    (after the last, up to stim_end); AHP_depth = min_AHP - voltage_base;
-    spike_half_width = width at half of (peak - AP begin V), by linear
-    interpolation; voltage_after_stim = mean V over stim_end + [25 %, 75 %] of
-    the remaining time.  A feature that cannot be computed is None (eFEL
-    returns None too)."""
+    """The eFEL features efel_ext.py requests (feature_list, :13).
+
+    Each restates the feature's published definition in eFEL's feature
+    documentation (BlueBrain eFEL, the eFeatures descriptions; the reference
+    pins eFEL by git commit, GUI/requirements.txt:23, and calls it at
+    P/efel_ext.py:62 with Threshold -30 mV and the default
+    DerivativeThreshold 10 mV/ms):
+
+    * voltage_base -- the mean voltage over the last 10 % of the time before
+      the stimulus: mean V over [0.9 stim_start, stim_start].
+    * peak_indices / peak_time -- for every excursion above Threshold (from
+      an upward crossing to the next downward one, or the trace's end), the
+      sample of its maximum; peak_time is its time.  Only peaks within
+      [stim_start, stim_end] are kept.
+    * AP_begin_indices -- for each peak, the first sample after the previous
+      peak (the first: after stim_start) where dV/dt >= DerivativeThreshold
+      (dV/dt by central differences, numpy.gradient).
+    * AP_amplitude -- V at the peak minus V at its AP begin.
+    * min_AHP_values / AHP_depth -- the minimum of V between a peak and the
+      next (after the last peak: up to stim_end); AHP_depth = min_AHP_values
+      - voltage_base.
+    * spike_half_width -- the time between the upward and the downward
+      crossing of the half level 0.5 (V_peak + V_AP_begin), each crossing
+      time linearly interpolated between samples; spikes whose fall does not
+      reach the half level before the trace ends are left out.
+    * voltage_after_stim -- the mean voltage over [stim_end + 25 %, stim_end
+      + 75 %] of the time after the stimulus.
+
+    A feature that cannot be computed (no peak in the window; no samples) is
+    None, as eFEL returns None.  tests/test_efel_features.py checks every
+    definition on traces whose features follow by hand from it: no spikes,
+    one spike, spikes at both window edges, two spikes."""
     t = np.asarray(t, dtype=np.float64)
     v = np.asarray(v, dtype=np.float64)
     out: dict[str, np.ndarray | None] = {}

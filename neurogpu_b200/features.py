@@ -7,6 +7,38 @@ generation needs the features of all traces in one pass, and the surrogate
 network is trained to predict exactly this vector.  Spikes are upward
 crossings of -20 mV inside the stimulus window; every feature has a defined
 value without spikes (stated per feature) so the vector is always finite.
+
+These 20 are this project's own definitions (the surrogate's target vector),
+modelled on eFEL features (the eFEL feature documentation, BlueBrain eFEL;
+the reference pins its version at GUI/requirements.txt:23) but not equal to
+them; the evaluator's eFEL features proper are neurogpu_b200.evaluator.
+efel_features.  Correspondence, and where they differ:
+
+  spike_count           eFEL Spikecount (eFEL counts peaks; here crossings)
+  first_spike_latency   time_to_first_spike (eFEL: to the peak; here to the
+                        first sample at or above threshold)
+  mean_isi, isi_cv      mean of ISI_values, ISI_CV (ISIs between crossings)
+  first_isi, last_isi   ISI_values[0], ISI_values[-1]
+  adaptation            last ISI / first ISI (eFEL's adaptation_index is a
+                        normalised average of consecutive ISI differences)
+  ap_peak_mean, _std    mean and std of peak_voltage (the maximum between
+                        consecutive crossings)
+  ahp_mean              mean of min_AHP_values (the minimum between
+                        consecutive crossings, the last to the window end)
+  ap_amplitude_mean     ap_peak_mean - ahp_mean (eFEL's AP_amplitude is
+                        peak - AP begin voltage)
+  time_above_half       the mean time per spike above the half level between
+                        those means (eFEL's spike_half_width uses each AP's
+                        own begin voltage)
+  voltage_base          mean V over the 10 ms before stim_on (eFEL: the last
+                        10 % of the time before the stimulus)
+  steady_state          mean V over the last 50 ms of the stimulus
+                        (eFEL steady_state_voltage_stimend: the last 10 %)
+  voltage_after_stim    mean V from stim_off + 10 ms to the trace's end
+                        (eFEL: stim_off + 25 % .. 75 % of the remaining time)
+  v_max, v_min_stim, v_mean_stim, v_std_stim, last_spike_time
+                        maximum_voltage (whole trace), minimum_voltage,
+                        mean and std of V in the window, the last crossing
 """
 from __future__ import annotations
 
