@@ -569,6 +569,48 @@ __global__ void __launch_bounds__(kLanes * kMaxWarps) k_sim_init(SimArgs<R> A) {
 // light nodes; V update of each node.  Rows are prefetched into L2 in
 // blocks of four nodes, four nodes ahead.
 // TI: thread-item layout (lanes on different items; no lane-0 prefetch).
+// One node's back-substitution operands: its eliminated row (r, c; on a
+// spine also w) and its voltage with the Kahan term.
+template <typename R>
+struct BackRow {
+    R r, c, w, V, C;
+};
+template <typename R, bool SPINE>
+__device__ __forceinline__ BackRow<R> load_back_row(const Group<R>& G, int i) {
+    BackRow<R> b;
+    const R* row = G.scr + (size_t)i * 3 * kLanes;
+    const R* vo = G.vbuf + (size_t)i * 2 * kLanes;
+    b.r = row[0];
+    b.c = row[kLanes];
+    b.w = SPINE ? row[2 * kLanes] : (R)0;
+    b.V = vo[0];
+    b.C = vo[kLanes];
+    return b;
+}
+
+// The V update of node i from its loaded (V, Kahan term) and dV = x: store,
+// dV for the node's far children, recording, non-finite check.
+template <typename R>
+__device__ __forceinline__ void backsub_store(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>& n, int i,
+                                              R x, R V, R vc, bool rec_now, float* trace, int& bad) {
+    R* vo = G.vbuf + (size_t)i * 2 * kLanes;
+    kahan_add(V, vc, x);
+    vo[0] = V;
+    vo[kLanes] = vc;
+    if (n.jslot >= 0) G.jx[(size_t)n.jslot * kLanes] = x;
+    record(A, n, V, rec_now, trace);
+    bad |= v_bad(V);
+}
+
+// Back-substitution pass of an item, root -> leaf: the spine of a segment
+// (dV_i = r_i - c_i dV_parent + w_i dV_l, from separator u down), then the
+// light nodes; V update of each node.  Software-pipelined one node deep: the
+// next node's operands (row, V, Kahan term, and a far child's parent dV) are
+// loaded before this node's update, so a node's memory latency overlaps the
+// previous node's arithmetic and stores (no node writes what the next one
+// reads: its own V and, for a junction, a dV its later children read).  Rows
+// are also prefetched into L2 in blocks of four nodes, four nodes ahead.
+// TI: thread-item layout (lanes on different items; no lane-0 prefetch).
 template <typename R, bool TI = false>
 __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>& G, const NodeRec<R>* nr,
                                              const DevComp& c, bool rec_now, float* trace, int& bad) {
@@ -577,26 +619,43 @@ __device__ __forceinline__ void backsub_item(const SimArgs<R>& A, const Group<R>
         R xp = G.jx[(size_t)nr[c.u].jslot * kLanes];
         const R xl = G.jx[(size_t)nr[c.l].jslot * kLanes];
         if constexpr (!TI) prefetch_backsub(G, c.r, min(kBlk, c.l - c.r));
+        BackRow<R> cur = load_back_row<R, true>(G, c.r);
         for (int i = c.r; i < c.l; ++i) {
             if constexpr (!TI)
                 if (((i - c.r) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.l - i - kBlk));
-            const R* row = G.scr + (size_t)i * 3 * kLanes;
-            const R xi = row[0] - row[kLanes] * xp + row[2 * kLanes] * xl;
+            const BackRow<R> nxt = i + 1 < c.l ? load_back_row<R, true>(G, i + 1) : cur;
+            const R xi = cur.r - cur.c * xp + cur.w * xl;
             xp = xi;
-            backsub_node(A, G, nr[i], i, xi, rec_now, trace, bad);
+            backsub_store(A, G, nr[i], i, xi, cur.V, cur.C, rec_now, trace, bad);
+            cur = nxt;
         }
     }
+    if (c.hi <= c.lo) return;
     R x_prev = 0;
     if constexpr (!TI) prefetch_backsub(G, c.lo, min(kBlk, c.hi - c.lo));
+    NodeRec<R> n = nr[c.lo];
+    BackRow<R> cur = load_back_row<R, false>(G, c.lo);
+    R xj = n.pslot < 0 ? (R)0 : G.jx[(size_t)n.pslot * kLanes];
     for (int i = c.lo; i < c.hi; ++i) {
         if constexpr (!TI)
             if (((i - c.lo) & (kBlk - 1)) == 0) prefetch_backsub(G, i + kBlk, min(kBlk, c.hi - i - kBlk));
-        const NodeRec<R> n = nr[i];
-        const R* row = G.scr + (size_t)i * 3 * kLanes;
-        const R xp = n.pslot < 0 ? x_prev : G.jx[(size_t)n.pslot * kLanes];
-        const R x = row[0] - row[kLanes] * xp;
+        // the next node: its parent is this node (a chain child, pslot < 0)
+        // or an earlier one, whose dV is already stored
+        NodeRec<R> nn = n;
+        BackRow<R> nxt = cur;
+        R xjn = 0;
+        if (i + 1 < c.hi) {
+            nn = nr[i + 1];
+            nxt = load_back_row<R, false>(G, i + 1);
+            if (nn.pslot >= 0) xjn = G.jx[(size_t)nn.pslot * kLanes];
+        }
+        const R xp = n.pslot < 0 ? x_prev : xj;
+        const R x = cur.r - cur.c * xp;
         x_prev = x;
-        backsub_node(A, G, n, i, x, rec_now, trace, bad);
+        backsub_store(A, G, n, i, x, cur.V, cur.C, rec_now, trace, bad);
+        n = nn;
+        cur = nxt;
+        xj = xjn;
     }
 }
 

@@ -113,3 +113,33 @@ def test_surrogate_screening_beats_random_choice(ngpu_built):
     print(f"mean true score: surrogate top 10 % {true[top].mean():.3f}, random 10 % {true[rand].mean():.3f}, "
           f"best possible {np.sort(true)[:200].mean():.3f}")
     assert true[top].mean() < 0.5 * true[rand].mean()
+
+
+@pytest.mark.gpu
+def test_inputs_device_matches_host():
+    import torch
+    u = np.random.default_rng(1).uniform(-1, 1, (5, 12))
+    got = ga.inputs_device(torch.tensor(u, device="cuda"), 3).cpu().numpy()
+    np.testing.assert_array_equal(got, ga._inputs(u, 3))
+
+
+@pytest.mark.gpu
+def test_device_screened_ga_with_a_pretrained_surrogate(ngpu_built):
+    """The surrogate trained once over the whole search space (independent of
+    the target), then the screened GA with every step on the device: the
+    best score never rises, each generation simulates the network's top 10 %
+    (or, on a fallback, every offspring), and the error it measured is
+    recorded per generation."""
+    prob = ga.FitProblem(n_comp=120, t_stop=120.0, stim_on=20.0, stim_off=100.0, levels=(0.3, 0.8), rec_every=4,
+                         seed=9)
+    fit = ga.train_surrogate(prob, n_train=4096, epochs=8, seed=0)
+    assert fit.n_train == 4096 and np.isfinite(fit.final_loss) and fit.sim_seconds > 0
+    prob.sim_count = 0
+    pop, gens = 256, 4
+    res = ga.run_screened_device(prob, fit.net, pop, gens, seed=2)
+    assert len(res.best) == gens and np.all(np.diff(res.best) <= 0)
+    keep = int(round(0.1 * pop))
+    expect = pop + sum(keep if m == "screened" else pop for _, _, m in res.notes)
+    assert prob.sim_count == expect
+    assert all(np.isfinite(e) for _, e, _ in res.notes)
+    assert res.best_u.shape == (12,) and np.all(np.abs(res.best_u) <= 1)
