@@ -511,9 +511,11 @@ def run_gemm(args):
 
     rows = {}
     g = torch.Generator(device="cuda").manual_seed(0)
-    # (name, M, N, K, bn, epilogue): epilogue 0 store fp32, 1 bias + GELU (three outputs)
+    # (name, M, N, K, bn, epilogue): epilogue 0 store fp32, 1 bias + GELU (three outputs),
+    # 4 store fp32 with K split over CTAs
     shapes = [("fwd_hidden_8192x512x512", 8192, 512, 512, 128, 1), ("fwd_input_8192x512x64", 8192, 512, 64, 128, 1),
               ("fwd_out_8192x32x512", 8192, 32, 512, 32, 0), ("dW_512x512x8192", 512, 512, 8192, 128, 0),
+              ("dW_512x512x8192_splitK", 512, 512, 8192, 128, 4),
               ("square_4096", 4096, 4096, 4096, 256, 0), ("square_8192", 8192, 8192, 8192, 256, 0)]
     for name, M, N, K, bn, epi in shapes:
         A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
@@ -541,7 +543,7 @@ def run_gemm(args):
         fl = 2.0 * M * N * K
         rows[name] = {"ms": ms, "tflops": fl / ms / 1e9, "cublas_ms": ms_cublas,
                       "cublas_tflops": fl / ms_cublas / 1e9, "bn": bn,
-                      "epilogue": "bias+gelu (f32, bf16, bf16^T)" if epi == 1 else "store f32",
+                      "epilogue": {0: "store f32", 1: "bias+gelu (f32, bf16, bf16^T)", 4: "store f32, split K"}[epi],
                       "max_rel_err_vs_fp32": err}
         del A, B, out, ob, obt
     v = rows["square_8192"]["tflops"]

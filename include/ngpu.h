@@ -340,7 +340,11 @@ int64_t ngpu_launch_count(int32_t reset);
  *   accumulation.  epilogue: 0 out_f32 = D; 1 z = D + bias: out_f32 = z,
  *   out_bf16 = gelu(z) (tanh form) and its transpose out_bf16_t[n][m];
  *   2 out_f32 = D + bias; 3 dz = D * gelu'(zin): out_bf16 = dz and
- *   out_bf16_t = dz^T.  bn: the N tile (32, 64, 128, 256).  A wait that
+ *   out_bf16_t = dz^T; 4 out_f32 = D with K split over CTAs (for K much
+ *   larger than M and N, as in the network's weight gradients: the output
+ *   is zeroed on the stream, the slices add their partial sums with
+ *   atomics, so the summation order varies from run to run within fp32
+ *   rounding).  bn: the N tile (32, 64, 128, 256).  A wait that
  *   exceeds its bound sets a device flag read (and cleared) by
  *   ngpu_gemm_error.  No counterpart in the reference.
  */

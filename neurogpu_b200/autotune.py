@@ -114,10 +114,18 @@ def tune_warps(model: Model | CellModel, params, amps, dts, stim_node: int, stim
     layout, needs per member)."""
     shapes = [(int(W), int(k)) for W in sorted({int(w) for w in candidates if 1 <= int(w) <= 8})
               for k in (sorted({int(i) for i in items if 1 <= int(i) <= 8}) if W > 1 else [1])]
+    cell = model.cell if isinstance(model, Model) else model
+    key = (_key(cell, int(np.asarray(params).shape[0]), int(np.asarray(amps).shape[0]), precision) + ":warps:" +
+           ",".join(f"{w}.{k}" for w, k in shapes))
+    _load(cache_file)
+    if key in _CACHE:
+        return _CACHE[key]
     r = tune(model, params, amps, dts, stim_node, stim_area, rec_nodes, v_init, steps=steps, warmup=warmup,
              precision=precision, lane_shapes=shapes, warp_shapes=(), cache_file=cache_file)
-    return {"n_warps": r["n_warps"], "items_per_warp": r["items_per_warp"],
-            "ms_per_step": {k.split(":", 1)[1]: v for k, v in r["ms_per_step"].items()}}
+    res = {"n_warps": r["n_warps"], "items_per_warp": r["items_per_warp"],
+           "ms_per_step": {k.split(":", 1)[1]: v for k, v in r["ms_per_step"].items()}}
+    _store(key, res, cache_file)
+    return res
 
 
 # --------------------------------------------------------- recording cadence

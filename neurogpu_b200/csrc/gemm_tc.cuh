@@ -2,14 +2,18 @@
 //
 //   D[M][N] = A[M][K] . B[N][K]^T     (A, B bf16, both K-major; D fp32 in TMEM)
 //
-// One CTA of 128 threads computes a 128 x BN tile.  K advances in tiles of
-// 64: all threads copy the next A / B tiles into a two-stage shared-memory
-// ring with cp.async (rows past M read as zeros) while the previous tile's
-// MMAs run; one thread issues four tcgen05.mma (K = 16 each) per tile and
-// commits them to that stage's mbarrier, which the copy into the stage waits
-// on before overwriting it.  The accumulator lives in tensor memory (BN fp32
-// columns x 128 lanes); after the last commit each warp reads its 32 lanes
-// with tcgen05.ld and applies the epilogue.
+// One CTA of 128 threads computes a 128 x BN tile over a range of K (all of
+// K, or one slice of it for the split-K epilogue).  K advances in tiles of
+// 64 through an S-stage shared-memory ring (S = 4, 3 for BN = 256): all
+// threads copy tile k + S - 1 into its stage with cp.async (rows past M read
+// as zeros) while the tensor cores work on tiles k .. k + S - 2; one thread
+// issues four tcgen05.mma (K = 16 each) per tile and commits them to that
+// stage's mbarrier, which the copy into the stage waits on before
+// overwriting it.  The accumulator lives in tensor memory (BN fp32 columns x
+// 128 lanes); after the last commit each warp reads its 32 lanes with
+// tcgen05.ld, 16 columns at a time, and stages them through shared memory
+// (the ring, free by then) so that row-major outputs are written with
+// coalesced stores: a warp store covers two rows of 16 columns.
 //
 // Shared-memory operand layout (no swizzle, K-major canonical layout): an
 // 8-row x 16-byte core matrix is 128 contiguous bytes; core matrices along K
@@ -38,6 +42,7 @@ enum GemmEpilogue : int {
     kEpiBiasGelu = 1,   // z = D + bias[n]: out_f32 = z, out_bf16 = gelu(z), out_bf16_t[n][m] = gelu(z)
     kEpiBias = 2,       // out_f32[m][n] = D + bias[n]
     kEpiGeluGrad = 3,   // dz = D * gelu'(zin[m][n]): out_bf16 = dz, out_bf16_t[n][m] = dz
+    kEpiSplitAdd = 4,   // out_f32[m][n] += D over this CTA's slice of K (split-K; out_f32 zeroed first)
 };
 
 struct GemmArgs {
@@ -51,6 +56,7 @@ struct GemmArgs {
     const float* bias;       // [N]
     const float* zin;        // [M][ldo]
     int* err;
+    int kt_split;            // 64-wide K tiles per CTA; CTA z takes tiles [z kt_split, (z+1) kt_split)
 };
 
 __device__ __forceinline__ float gelu_tanh(float z) {
@@ -118,71 +124,91 @@ __device__ __forceinline__ void load_tile(uint32_t dst, const __nv_bfloat16* src
     }
 }
 
+// Ring depth: four stages (three for the 256-wide tile, whose stage is 48 KB).
+template <int BN>
+__host__ __device__ constexpr int gemm_stages() {
+    return BN >= 256 ? 3 : 4;
+}
+
 template <int BN>
 struct GemmSmem {
-    alignas(1024) unsigned char a[2][kGemmBM * kGemmBK * 2];
-    alignas(1024) unsigned char b[2][BN * kGemmBK * 2];
-    alignas(8) uint64_t bar[2];
+    static constexpr int kStages = gemm_stages<BN>();
+    alignas(1024) unsigned char a[kStages][kGemmBM * kGemmBK * 2];
+    alignas(1024) unsigned char b[kStages][BN * kGemmBK * 2];
+    alignas(8) uint64_t bar[kStages];
     uint32_t tmem;
 };
+
+// Epilogue staging: per warp 32 rows x 16 columns of fp32, row stride 17
+// (conflict-free column writes), inside the ring once the MMAs are done.
+constexpr int kStageStride = 17;
+static_assert(kGemmBM * kGemmBK * 2 >= 4 * 32 * kStageStride * 4, "staging fits in the first A stage");
 
 template <int BN, int EPI>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
     static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "BN: a multiple of 16 in [32, 256]");
+    constexpr int S = gemm_stages<BN>();
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // align the ring to 1024 bytes (descriptor base offset 0)
-    GemmSmem<BN>& S = *reinterpret_cast<GemmSmem<BN>*>(
+    GemmSmem<BN>& Sm = *reinterpret_cast<GemmSmem<BN>*>(
         (void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
     constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // power of two >= 32 for BN in {32, 64, 128, 256}
 
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&Sm.tmem)),
                      "r"(kCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        mbar_init(smem_u32(&S.bar[0]), 1);
-        mbar_init(smem_u32(&S.bar[1]), 1);
+        for (int s = 0; s < S; ++s) mbar_init(smem_u32(&Sm.bar[s]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = S.tmem;
+    const uint32_t tmem = Sm.tmem;
 
-    const int KT = g.K / kGemmBK;
+    // this CTA's K tiles: [kt0, kt0 + KT) (the host gives every CTA at least one)
+    const int kt0 = blockIdx.z * g.kt_split;
+    const int KT = min(g.kt_split, g.K / kGemmBK - kt0);
     const int rows_a = min(kGemmBM, g.M - m0), rows_b = min(BN, g.N - n0);
-    const __nv_bfloat16* Ab = g.A + (size_t)m0 * g.lda;
-    const __nv_bfloat16* Bb = g.B + (size_t)n0 * g.ldb;
-    uint32_t phase[2] = {0, 0};
+    const __nv_bfloat16* Ab = g.A + (size_t)m0 * g.lda + (size_t)kt0 * kGemmBK;
+    const __nv_bfloat16* Bb = g.B + (size_t)n0 * g.ldb + (size_t)kt0 * kGemmBK;
+    uint32_t phases = 0;  // bit s: parity of stage s's next completion
     bool ok = true;
 
-    load_tile<kGemmBM>(smem_u32(S.a[0]), Ab, g.lda, rows_a);
-    load_tile<BN>(smem_u32(S.b[0]), Bb, g.ldb, rows_b);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    for (int kt = 0; kt < KT; ++kt) {
-        const int s = kt & 1;
-        if (kt + 1 < KT) {
-            const int sn = (kt + 1) & 1;
-            if (kt >= 1) {  // the MMAs of tile kt-1 read stage sn
-                ok = ok && mbar_wait(smem_u32(&S.bar[sn]), phase[sn]);
-                phase[sn] ^= 1;
-            }
-            load_tile<kGemmBM>(smem_u32(S.a[sn]), Ab + (size_t)(kt + 1) * kGemmBK, g.lda, rows_a);
-            load_tile<BN>(smem_u32(S.b[sn]), Bb + (size_t)(kt + 1) * kGemmBK, g.ldb, rows_b);
-            asm volatile("cp.async.commit_group;" ::: "memory");
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // prologue: tiles 0 .. S-2 in flight, one commit group each (empty past KT)
+#pragma unroll
+    for (int s = 0; s < S - 1; ++s) {
+        if (s < KT) {
+            load_tile<kGemmBM>(smem_u32(Sm.a[s]), Ab + (size_t)s * kGemmBK, g.lda, rows_a);
+            load_tile<BN>(smem_u32(Sm.b[s]), Bb + (size_t)s * kGemmBK, g.ldb, rows_b);
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt % S;
+        const int nk = kt + S - 1;
+        if (nk < KT) {
+            const int sn = nk % S;  // = (kt - 1) % S: the stage tile kt-1's MMAs read
+            if (kt >= 1) {
+                ok = ok && mbar_wait(smem_u32(&Sm.bar[sn]), (phases >> sn) & 1u);
+                phases ^= 1u << sn;
+            }
+            load_tile<kGemmBM>(smem_u32(Sm.a[sn]), Ab + (size_t)nk * kGemmBK, g.lda, rows_a);
+            load_tile<BN>(smem_u32(Sm.b[sn]), Bb + (size_t)nk * kGemmBK, g.ldb, rows_b);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        // S + kt groups committed; all but the newest S-1 done: tile kt's group is
+        asm volatile("cp.async.wait_group %0;" ::"n"(S - 1) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async data -> tensor core reads
         __syncthreads();
         if (threadIdx.x == 0 && ok) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(S.a[s]), sb = smem_u32(S.b[s]);
+            const uint32_t sa = smem_u32(Sm.a[s]), sb = smem_u32(Sm.b[s]);
 #pragma unroll
             for (int k = 0; k < kGemmBK / 16; ++k) {  // K = 16 per MMA: two core matrices along K
                 const uint64_t da = umma_desc(sa + k * 256), db = umma_desc(sb + k * 256);
@@ -194,22 +220,24 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&S.bar[s]))
+                             smem_u32(&Sm.bar[s]))
                          : "memory");
         }
-        __syncthreads();
     }
-    // the last commit covers every MMA this thread issued
+    // the last commit covers every MMA this thread issued: tile KT-1 is use
+    // (KT-1)/S of its stage, whose earlier uses were all waited on above
     if (KT > 0) {
-        const int s = (KT - 1) & 1;
-        ok = ok && mbar_wait(smem_u32(&S.bar[s]), phase[s]);
+        const int s = (KT - 1) % S;
+        ok = ok && mbar_wait(smem_u32(&Sm.bar[s]), (uint32_t)((KT - 1) / S) & 1u);
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    ok = __syncthreads_and(ok);
+    ok = __syncthreads_and(ok);  // also: every thread is done with the ring before it stages the epilogue
 
     if (ok) {
-        const int m = m0 + warp * 32 + lane;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        float* stg = reinterpret_cast<float*>(Sm.a[0]) + warp * 32 * kStageStride;
+        const int mw = m0 + warp * 32;  // this warp's first row
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 16) {
             uint32_t r[16];
@@ -220,30 +248,51 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
                   "=r"(r[15])
                 : "r"(trow + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (m < g.M) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int n = n0 + c0 + j;
-                    if (n >= g.N) continue;
-                    const float d = __uint_as_float(r[j]);
+            for (int j = 0; j < 16; ++j) stg[lane * kStageStride + j] = __uint_as_float(r[j]);
+            __syncwarp();
+            // coalesced pass: element e = j * 32 + lane is row e / 16, column e % 16
+#pragma unroll 4
+            for (int j = 0; j < 16; ++j) {
+                const int e = j * 32 + lane, row = e >> 4, col = e & 15;
+                const int m = mw + row, n = n0 + c0 + col;
+                float* sp = stg + row * kStageStride + col;
+                if (m < g.M && n < g.N) {
+                    const size_t o = (size_t)m * g.ldo + n;
+                    const float d = *sp;
                     if constexpr (EPI == kEpiStore) {
-                        g.out_f32[(size_t)m * g.ldo + n] = d;
+                        g.out_f32[o] = d;
                     } else if constexpr (EPI == kEpiBias) {
-                        g.out_f32[(size_t)m * g.ldo + n] = d + g.bias[n];
+                        g.out_f32[o] = d + g.bias[n];
+                    } else if constexpr (EPI == kEpiSplitAdd) {
+                        atomicAdd(g.out_f32 + o, d);
                     } else if constexpr (EPI == kEpiBiasGelu) {
                         const float z = d + g.bias[n];
                         const __nv_bfloat16 h = __float2bfloat16_rn(gelu_tanh(z));
-                        g.out_f32[(size_t)m * g.ldo + n] = z;
-                        g.out_bf16[(size_t)m * g.ldo + n] = h;
-                        g.out_bf16_t[(size_t)n * g.ldt + m] = h;
+                        g.out_f32[o] = z;
+                        g.out_bf16[o] = h;
+                        *sp = __bfloat162float(h);
                     } else {  // kEpiGeluGrad
-                        const float dz = d * gelu_tanh_grad(g.zin[(size_t)m * g.ldo + n]);
-                        const __nv_bfloat16 h = __float2bfloat16_rn(dz);
-                        g.out_bf16[(size_t)m * g.ldo + n] = h;
-                        g.out_bf16_t[(size_t)n * g.ldt + m] = h;
+                        const __nv_bfloat16 h = __float2bfloat16_rn(d * gelu_tanh_grad(g.zin[o]));
+                        g.out_bf16[o] = h;
+                        *sp = __bfloat162float(h);
                     }
                 }
             }
+            if constexpr (EPI == kEpiBiasGelu || EPI == kEpiGeluGrad) {
+                // the transposed bf16 copy, lane = row: a warp store is 32 consecutive rows
+                __syncwarp();
+                const int m = mw + lane;
+                if (m < g.M) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int n = n0 + c0 + j;
+                        if (n < g.N)
+                            g.out_bf16_t[(size_t)n * g.ldt + m] = __float2bfloat16_rn(stg[lane * kStageStride + j]);
+                    }
+                }
+            }
+            __syncwarp();  // the next chunk overwrites the staging rows
         }
     } else if (threadIdx.x == 0) {
         atomicExch(g.err, 1);

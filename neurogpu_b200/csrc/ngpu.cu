@@ -454,19 +454,24 @@ static double rows_per_node(const ngpu_model* m) {
 
 // CTAs per SM that `smem` bytes of dynamic shared memory and W warps of 80
 // registers allow (228 KB per SM, 1 KB of it reserved per CTA).
-static int ctas_per_sm(size_t smem, int W) {
-    // kernels of up to 8 warps use 80 registers; wider ones are compiled for 3 CTAs per SM
-    const int by_regs = W > kMaxWarps ? 3 : 65536 / (kLanes * W * 80);
+// CTAs per SM a wide (more than 8 warps) lane-instance kernel is compiled
+// for: 1 when the batch has at most one group per SM (registers are then
+// plentiful: 16 warps get 128), else 3 (one wave for large batches).
+static int wide_ctas_per_sm(int n_groups) { return n_groups <= kSmCount ? 1 : 3; }
+
+static int ctas_per_sm(size_t smem, int W, int n_groups) {
+    // kernels of up to 8 warps use 80 registers; wider ones are compiled for wide_ctas_per_sm
+    const int by_regs = W > kMaxWarps ? wide_ctas_per_sm(n_groups) : 65536 / (kLanes * W * 80);
     const int by_smem = (int)((228 * 1024) / (smem + 1024));
     return std::max(1, std::min(std::min(by_regs, by_smem), 64 / W));
 }
 
 // Stage the skeleton in shared memory when that costs no occupancy.
 template <typename R>
-static int choose_s2_stage(int n_nodes, int n_seps, int W) {
+static int choose_s2_stage(int n_nodes, int n_seps, int W, int n_groups) {
     if (W < 2 || n_seps < 2) return 0;
     const size_t plain = SmemPlan<R>::bytes(n_nodes), staged = SmemPlan<R>::bytes(n_nodes, n_seps, 1);
-    return staged <= 227 * 1024 && ctas_per_sm(staged, W) >= ctas_per_sm(plain, W) ? 1 : 0;
+    return staged <= 227 * 1024 && ctas_per_sm(staged, W, n_groups) >= ctas_per_sm(plain, W, n_groups) ? 1 : 0;
 }
 
 template <typename R>
@@ -1009,8 +1014,8 @@ int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
         }
     } else {
         s->part = make_partition(m, W, s->items_per_warp);
-        s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W)
-                                             : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W);
+        s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W, s->n_groups)
+                                             : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W, s->n_groups);
     }
     const int nj = s->part.n_jslots;
 #define ALLOC(field, type, bytes)                              \
@@ -1434,7 +1439,8 @@ static int sim_upload_nodes(ngpu_sim* s) {
             s->jit = ngpu_jit::module(m->mechset, s->precision == NGPU_FP64, picked, gs ? &gs->source : nullptr,
                                       s->ch_prefetch, s->folds, masks_cover(picked, all, s->ch_prefetch),
                                       s->layout == NGPU_LAYOUT_WARP_INSTANCE,
-                                      s->layout == NGPU_LAYOUT_LANE_INSTANCE ? std::max(8, s->n_warps) : 8);
+                                      s->layout == NGPU_LAYOUT_LANE_INSTANCE ? std::max(8, s->n_warps) : 8,
+                                      wide_ctas_per_sm(s->n_groups));
         }
         if (gs && !s->jit)
             return fail(NGPU_E_CUDA, "mechanism set '" + gs->name +
@@ -2194,19 +2200,38 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
 // ---- BF16 tensor-core GEMM (surrogate network) -------------------------------
 static __device__ int g_gemm_err;
 
+// The split of K over CTAs: the whole of K per CTA, except for the split-K
+// epilogue, which spreads K over enough CTAs to give every SM two (each
+// slice at least one 64-wide tile).
+static int gemm_k_split(const GemmArgs& g, int bn, int epi, int* splits) {
+    const int KT = g.K / kGemmBK;
+    const int tiles = ((g.M + kGemmBM - 1) / kGemmBM) * ((g.N + bn - 1) / bn);
+    int z = 1;
+    if (epi == kEpiSplitAdd) z = std::max(1, std::min(KT, (2 * 148 + tiles - 1) / tiles));
+    const int per = (KT + z - 1) / z;
+    *splits = (KT + per - 1) / per;
+    return per;
+}
+
 template <int BN, int EPI>
-static cudaError_t launch_gemm_bn(const GemmArgs& g, cudaStream_t st) {
+static cudaError_t launch_gemm_bn(GemmArgs g, cudaStream_t st) {
     const size_t smem = gemm_smem_bytes<BN>();
     cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tn<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + BN - 1) / BN);
+    int splits = 1;
+    g.kt_split = gemm_k_split(g, BN, EPI, &splits);
+    if (EPI == kEpiSplitAdd) {  // the slices add into a zeroed output
+        e = cudaMemsetAsync(g.out_f32, 0, sizeof(float) * ((size_t)(g.M - 1) * g.ldo + g.N), st);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + BN - 1) / BN, splits);
     k_gemm_bf16_tn<BN, EPI><<<grid, kGemmThreads, smem, st>>>(g);
     g_launches++;
     return cudaGetLastError();
 }
 
 template <int EPI>
-static cudaError_t launch_gemm_epi(const GemmArgs& g, int bn, cudaStream_t st) {
+static cudaError_t launch_gemm_epi(GemmArgs g, int bn, cudaStream_t st) {
     switch (bn) {
         case 32: return launch_gemm_bn<32, EPI>(g, st);
         case 64: return launch_gemm_bn<64, EPI>(g, st);
@@ -2226,7 +2251,8 @@ extern "C" int ngpu_gemm_bf16_tn(const void* A, const void* B, int32_t M, int32_
         return fail(NGPU_E_INVALID, "gemm: leading dimensions must be >= K and multiples of 8");
     if (((uintptr_t)A | (uintptr_t)B) & 15) return fail(NGPU_E_INVALID, "gemm: operands must be 16-byte aligned");
     if (bn != 32 && bn != 64 && bn != 128 && bn != 256) return fail(NGPU_E_INVALID, "gemm: bn must be 32, 64, 128 or 256");
-    const bool need_f32 = epilogue == kEpiStore || epilogue == kEpiBias || epilogue == kEpiBiasGelu;
+    const bool need_f32 = epilogue == kEpiStore || epilogue == kEpiBias || epilogue == kEpiBiasGelu ||
+                          epilogue == kEpiSplitAdd;
     const bool need_bf16 = epilogue == kEpiBiasGelu || epilogue == kEpiGeluGrad;
     if ((need_f32 && !out_f32) || (need_bf16 && (!out_bf16 || !out_bf16_t)) ||
         ((epilogue == kEpiBias || epilogue == kEpiBiasGelu) && !bias) || (epilogue == kEpiGeluGrad && !zin))
@@ -2236,13 +2262,14 @@ extern "C" int ngpu_gemm_bf16_tn(const void* A, const void* B, int32_t M, int32_
     cudaError_t e = cudaGetSymbolAddress((void**)&err, g_gemm_err);
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("gemm: ") + cudaGetErrorString(e));
     GemmArgs g{(const __nv_bfloat16*)A, (const __nv_bfloat16*)B, M, N, K, lda, ldb, out_f32,
-               (__nv_bfloat16*)out_bf16, (__nv_bfloat16*)out_bf16_t, ldo, ldt, bias, zin, err};
+               (__nv_bfloat16*)out_bf16, (__nv_bfloat16*)out_bf16_t, ldo, ldt, bias, zin, err, K / kGemmBK};
     cudaStream_t st = (cudaStream_t)cuda_stream;
     switch (epilogue) {
         case kEpiStore: e = launch_gemm_epi<kEpiStore>(g, bn, st); break;
         case kEpiBiasGelu: e = launch_gemm_epi<kEpiBiasGelu>(g, bn, st); break;
         case kEpiBias: e = launch_gemm_epi<kEpiBias>(g, bn, st); break;
         case kEpiGeluGrad: e = launch_gemm_epi<kEpiGeluGrad>(g, bn, st); break;
+        case kEpiSplitAdd: e = launch_gemm_epi<kEpiSplitAdd>(g, bn, st); break;
         default: return fail(NGPU_E_INVALID, "gemm: unknown epilogue");
     }
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("gemm launch: ") + cudaGetErrorString(e));

@@ -52,7 +52,8 @@ struct Module {
     bool prefetch = true;                   // channel-pass L2 prefetch compiled in (NGPU_CH_PREFETCH)
     bool complete = false;                  // the masks cover every node: no generic path (NGPU_CLASSES_COMPLETE)
     bool ti = false;                        // the thread-item layout's advance kernel compiled in
-    int adv_warps = 8;                      // the advance kernels' CTA size bound (warps), 3 CTAs per SM
+    int adv_warps = 8;                      // the advance kernels' CTA size bound (warps)
+    int adv_ctas = 3;                       // ... and CTAs per SM they are compiled for (above 8 warps)
     std::vector<uint32_t> masks;            // class k runs the code for masks[k]
     cudaLibrary_t lib = nullptr;
     cudaKernel_t init = nullptr;           // (SimArgs<R>)
@@ -122,15 +123,19 @@ inline bool enabled() {
 // header ngpu_generated.cuh).  prefetch: the channel pass's L2 prefetch.
 // ti: also the thread-item layout's advance kernel.
 // adv_warps: the advance kernels are bounded for CTAs of up to this many
-// warps, 3 per SM (8: 80 registers; 10: 64; 12: 56; 16: 40).
+// warps; above 8, for adv_ctas CTAs per SM (3 CTAs: 10 warps 64 registers,
+// 12: 56, 16: 40; 1 CTA, for batches of at most one CTA per SM: 16 warps
+// 128 registers).
 inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks, bool prefetch = true,
-                          const Folds& folds = {}, bool complete = false, bool ti = false, int adv_warps = 8) {
+                          const Folds& folds = {}, bool complete = false, bool ti = false, int adv_warps = 8,
+                          int adv_ctas = 3) {
     std::string list;
     for (size_t k = 0; k < masks.size(); ++k) list += (k ? ", " : "") + std::to_string(masks[k]) + "u";
     const std::string m = std::to_string(ms);
     const std::string R = fp64 ? "double" : "float";
     const std::string lb = adv_warps > 8
-                               ? "__launch_bounds__(" + std::to_string(32 * adv_warps) + ", 3)"
+                               ? "__launch_bounds__(" + std::to_string(32 * adv_warps) + ", " +
+                                     std::to_string(adv_ctas) + ")"
                                : "__launch_bounds__(ngpu::kLanes * ngpu::kMaxWarps, NGPU_ADV_MIN_BLOCKS)";
     std::string fold;
     if (!folds.empty()) {
@@ -199,13 +204,14 @@ inline std::string cache_dir() {
 // code of a generated mechanism set (ms 2), or nullptr.
 inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, const std::string* generated,
                         const std::string& arch, std::vector<char>* out, std::string* err, bool prefetch = true,
-                        const Folds& folds = {}, bool complete = false, bool ti = false, int adv_warps = 8) {
+                        const Folds& folds = {}, bool complete = false, bool ti = false, int adv_warps = 8,
+                        int adv_ctas = 3) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) {
         *err = last_log();
         return false;
     }
-    const std::string src = source(ms, fp64, masks, prefetch, folds, complete, ti, adv_warps);
+    const std::string src = source(ms, fp64, masks, prefetch, folds, complete, ti, adv_warps, adv_ctas);
     std::vector<std::string> opt_s = {"--gpu-architecture=sm_" + arch, "-std=c++17",
                                       "-lineinfo"};
     int vmaj = 0, vmin = 0;
@@ -306,7 +312,7 @@ inline bool build_cubin(int ms, bool fp64, const std::vector<uint32_t>& masks, c
 // code is *generated.  Modules live until the process exits.
 inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>& masks,
                             const std::string* generated, bool prefetch = true, const Folds& folds = {},
-                            bool complete = false, bool ti = false, int adv_warps = 8) {
+                            bool complete = false, bool ti = false, int adv_warps = 8, int adv_ctas = 3) {
     if (!generated && (!enabled() || masks.empty())) return nullptr;
     if (generated && !enabled()) {
         last_log() = "runtime compilation is off (NGPU_JIT=0)";
@@ -315,7 +321,9 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     std::lock_guard<std::mutex> lock(mu());
     static std::map<std::string, std::unique_ptr<Module>> cache;
     std::string key = std::to_string(mechset) + (fp64 ? "d" : "f") + (prefetch ? "p" : "n") + (complete ? "c" : "g") +
-                      (ti ? "t" : "") + (adv_warps > 8 ? "w" + std::to_string(adv_warps) : std::string()) + ":";
+                      (ti ? "t" : "") +
+                      (adv_warps > 8 ? "w" + std::to_string(adv_warps) + "x" + std::to_string(adv_ctas) : std::string()) +
+                      ":";
     for (uint32_t m : masks) key += std::to_string(m) + ",";
     for (const auto& f : folds) key += ";" + std::to_string(f.first) + "=" + float_literal(f.second);
     auto it = cache.find(key);
@@ -336,7 +344,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     std::string err;
     const std::string arch = std::to_string(maj) + std::to_string(min) + "a";
     if (!build_cubin(generated ? 2 : mechset, fp64, masks, generated, arch, &cubin, &err, prefetch, folds,
-                     complete, ti, adv_warps)) {
+                     complete, ti, adv_warps, adv_ctas)) {
         last_log() = err;
         cache[key] = nullptr;
         return nullptr;
@@ -348,6 +356,7 @@ inline const Module* module(int mechset, bool fp64, const std::vector<uint32_t>&
     mod->complete = complete;
     mod->ti = ti;
     mod->adv_warps = adv_warps;
+    mod->adv_ctas = adv_ctas;
     mod->masks = masks;
     cudaError_t e = cudaLibraryLoadData(&mod->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->init, mod->lib, "ngpu_jit_init");

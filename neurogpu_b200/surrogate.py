@@ -27,7 +27,7 @@ import numpy as np
 
 from . import _ffi
 
-EPI_STORE, EPI_BIAS_GELU, EPI_BIAS, EPI_GELU_GRAD = 0, 1, 2, 3
+EPI_STORE, EPI_BIAS_GELU, EPI_BIAS, EPI_GELU_GRAD, EPI_SPLIT = 0, 1, 2, 3, 4
 
 
 def _pad(n: int, m: int) -> int:
@@ -145,7 +145,7 @@ class SurrogateMLP:
         gW, gb = [None] * 4, [None] * 4
         # output layer: dW4^T[W][n_out_p] = H3^T . dY  (A = H3^T [W][Mp], B = dY^T [n_out_p][Mp])
         g4t = t.empty(W, self.n_out_p, device=self.dev)
-        self._gemm(a["H3t"], dybt, W, self.n_out_p, Mp, EPI_STORE, 32, g4t)
+        self._gemm(a["H3t"], dybt, W, self.n_out_p, Mp, EPI_SPLIT, 32, g4t)
         gW[3] = g4t.t().contiguous()
         gb[3] = dy[:, :self.n_out_p].sum(0)
         dz = dyb
@@ -156,7 +156,7 @@ class SurrogateMLP:
             self._gemm(dz, wt, Mp, W, dz.shape[1], EPI_GELU_GRAD, 128, None, dzb, dzbt, W, Mp, zin=a[f"Z{k + 1}"])
             kin = self.k_in if k == 0 else W
             g = t.empty(W, kin, device=self.dev)
-            self._gemm(dzbt, a[f"H{k}t"], W, kin, Mp, EPI_STORE, 64 if kin == 64 else 128, g)
+            self._gemm(dzbt, a[f"H{k}t"], W, kin, Mp, EPI_SPLIT, 64 if kin == 64 else 128, g)
             gW[k], gb[k] = g, dzb.float().sum(0)
             dz, wt = dzb, self.Wtb[k]
         return loss, gW, gb

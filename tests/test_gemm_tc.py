@@ -61,6 +61,22 @@ def test_gemm_matches_fp64(ngpu_built, M, N, K, bn):
     assert np.all(np.abs(got - want) <= bound)
 
 
+@pytest.mark.parametrize("M,N,K,bn", [(512, 512, 4096, 128), (512, 64, 8192, 64), (200, 20, 1024, 32),
+                                      (128, 128, 64, 128)])
+def test_gemm_split_k_matches_fp64(ngpu_built, M, N, K, bn):
+    """Epilogue 4: K spread over CTAs whose partial sums add into the zeroed
+    output; the same fp32 bound as one CTA per tile (sums of K terms in
+    another order)."""
+    rng = np.random.default_rng(M + 3 * N + K)
+    A = _bf16(rng.normal(size=(M, K)))
+    B = _bf16(rng.normal(size=(N, K)))
+    a64, b64 = A.float().numpy().astype(np.float64), B.float().numpy().astype(np.float64)
+    want = a64 @ b64.T
+    got, _, _ = _gemm(A, B, 4, bn)
+    bound = 1e-5 * (np.abs(a64) @ np.abs(b64).T) + 1e-30
+    assert np.all(np.abs(got - want) <= bound)
+
+
 def test_gemm_bias_gelu_epilogue(ngpu_built):
     rng = np.random.default_rng(7)
     M, N, K = 300, 128, 192
