@@ -34,6 +34,10 @@ _CACHE: dict[str, dict] = {}
 # candidate shapes: (warps per CTA, items per warp) of the lane layout and
 # (instances per CTA, items per instance) of the warp layout
 LANE_SHAPES = ((2, 2), (4, 2), (4, 3), (6, 3), (8, 2), (8, 3), (8, 4))
+# lane-layout CTAs of more than 8 warps, timed for batches of at most one
+# 32-instance group per SM (compiled then for one CTA per SM)
+WIDE_SHAPES = ((12, 2), (12, 3), (16, 2), (16, 3))
+SM_COUNT = 148
 WARP_SHAPES = ((1, 16), (1, 32), (1, 64), (2, 32), (4, 32), (8, 32))
 # the warp layout is timed up to this many instances (beyond, 32 instances
 # per CTA fill every SM several times over and the lane layout's coalesced
@@ -80,7 +84,9 @@ def tune(model: Model | CellModel, params, amps, dts, stim_node: int, stim_area:
     model = model if isinstance(model, Model) else Model(model)
     cell = model.cell
     n_sets, n_stim = int(np.asarray(params).shape[0]), int(np.asarray(amps).shape[0])
-    lane_shapes = tuple((int(w), int(k)) for w, k in lane_shapes if 1 <= int(w) <= 8 and 1 <= int(k) <= 8)
+    if lane_shapes is LANE_SHAPES and (n_sets * n_stim + 31) // 32 <= SM_COUNT:
+        lane_shapes = LANE_SHAPES + WIDE_SHAPES
+    lane_shapes = tuple((int(w), int(k)) for w, k in lane_shapes if 1 <= int(w) <= 16 and 1 <= int(k) <= 8)
     warp_shapes = tuple((int(w), int(k)) for w, k in warp_shapes if 1 <= int(w) <= 8 and 1 <= int(k) <= 512)
     if n_sets * n_stim > WARP_LAYOUT_MAX_INSTANCES:
         warp_shapes = ()
@@ -108,8 +114,9 @@ def tune(model: Model | CellModel, params, amps, dts, stim_node: int, stim_area:
 def tune_warps(model: Model | CellModel, params, amps, dts, stim_node: int, stim_area: float, rec_nodes,
                v_init: float, candidates=(2, 4, 6, 8), steps: int = 100, warmup: int = 20,
                precision: str = "fp32", cache_file: str | Path | None = None, items=(2, 3, 4)) -> dict:
-    """The lane layout's shape alone: times each (warp count, items per
-    warp) and returns {"n_warps": W, "items_per_warp": k, "ms_per_step":
+    """The lane layout's shape alone (up to 8 warps: the shapes a batch of
+    several morphologies runs): times each (warp count, items per warp) and
+    returns {"n_warps": W, "items_per_warp": k, "ms_per_step":
     {"W:k": ms}} (what a batch of several morphologies, which runs the lane
     layout, needs per member)."""
     shapes = [(int(W), int(k)) for W in sorted({int(w) for w in candidates if 1 <= int(w) <= 8})

@@ -924,6 +924,34 @@ static void sim_free(ngpu_sim* s) {
     delete s;
 }
 
+// The device side of the simulation's tree split (s->part): junction
+// accumulators and dV slots, work items, separators and segment links,
+// (re)allocated for the split and its items and separators uploaded.
+static int sim_upload_split(ngpu_sim* s) {
+    void** old[] = {(void**)&s->d_jacc, (void**)&s->d_jx, (void**)&s->d_comps, (void**)&s->d_seps, &s->d_sepv};
+    for (void** p : old)
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+    const size_t G = (size_t)s->n_groups, L = kLanes, esz = s->precision == NGPU_FP64 ? 8 : 4;
+    const size_t nj = std::max(1, s->part.n_jslots), ns = std::max<size_t>(1, s->part.seps.size());
+    int rc = NGPU_OK;
+    if (!(s->d_jacc = (double*)dmalloc(G * 2 * nj * L * sizeof(double), &rc))) return rc;
+    if (!(s->d_jx = dmalloc(G * nj * L * esz, &rc))) return rc;
+    if (!(s->d_comps = (DevComp*)dmalloc(sizeof(DevComp) * std::max<size_t>(1, s->part.comps.size()), &rc))) return rc;
+    if (!(s->d_seps = (DevSep*)dmalloc(sizeof(DevSep) * ns, &rc))) return rc;
+    if (!(s->d_sepv = dmalloc(G * 4 * ns * L * esz, &rc))) return rc;
+    std::vector<DevComp> dc;
+    for (const Comp& c : s->part.comps) dc.push_back({c.r, c.u, c.l, c.lk, c.light_lo, c.light_hi});
+    std::vector<DevSep> ds;
+    for (size_t k = 0; k < s->part.seps.size(); ++k)
+        ds.push_back({s->part.seps[k], s->part.sep_par[k], s->part.sep_comp[k], 0});
+    if (!dc.empty()) NGPU_CUDA(cudaMemcpy(s->d_comps, dc.data(), sizeof(DevComp) * dc.size(), cudaMemcpyHostToDevice));
+    NGPU_CUDA(cudaMemcpy(s->d_seps, ds.data(), sizeof(DevSep) * ds.size(), cudaMemcpyHostToDevice));
+    return NGPU_OK;
+}
+
 int ngpu_sim_create(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_t precision,
                     ngpu_sim** out) {
     return ngpu_sim_create_ex(m, n_sets, n_stim, precision, 0, out);
@@ -980,7 +1008,14 @@ int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
     const size_t G = (size_t)s->n_groups, L = kLanes;
     int rc = NGPU_OK;
     // warps per CTA and the tree split over them
+    // warps per CTA: a batch of at most one 32-instance group per SM leaves SMs
+    // idle, so its CTAs get up to 16 warps (a finer split of the tree, the
+    // runtime-compiled kernel at one CTA per SM: the HH cell at 2457
+    // instances runs 1.4x faster, the TTPC-like cell at 33 instances 1.5x);
+    // larger batches up to 8 (three CTAs per SM at 80 registers)
     int W = std::min(8, std::max(1, m->n / 48));
+    if (s->n_groups <= kSmCount && !ti && ngpu_jit::enabled() && ngpu_jit::nvrtc().ok)
+        W = std::min(kMaxWideWarps, std::max(1, m->n / 32));
     if (const char* ev = getenv("NGPU_WARPS")) W = std::max(1, std::min(kMaxWideWarps, atoi(ev)));
     if (n_warps > 0) W = n_warps;
     W = std::min(W, m->n);
@@ -1017,7 +1052,6 @@ int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
         s->s2_stage = precision == NGPU_FP64 ? choose_s2_stage<double>(m->n, (int)s->part.seps.size(), W, s->n_groups)
                                              : choose_s2_stage<float>(m->n, (int)s->part.seps.size(), W, s->n_groups);
     }
-    const int nj = s->part.n_jslots;
 #define ALLOC(field, type, bytes)                              \
     s->field = (type)dmalloc((bytes), &rc);                    \
     if (!s->field) {                                           \
@@ -1029,24 +1063,14 @@ int ngpu_sim_create_layout(ngpu_model* m, int32_t n_sets, int32_t n_stim, int32_
     ALLOC(d_slab, void*, G * m->slab_rows * L * esz);
     ALLOC(d_ptab, float*, G * m->ptab_rows * L * sizeof(float));
     ALLOC(d_scr, void*, G * 3 * m->n * L * esz);
-    ALLOC(d_jacc, double*, G * 2 * std::max(1, nj) * L * sizeof(double));
-    ALLOC(d_jx, void*, G * std::max(1, nj) * L * esz);
-    ALLOC(d_comps, DevComp*, sizeof(DevComp) * std::max<size_t>(1, s->part.comps.size()));
-    ALLOC(d_seps, DevSep*, sizeof(DevSep) * std::max<size_t>(1, s->part.seps.size()));
-    ALLOC(d_sepv, void*, G * 4 * std::max<size_t>(1, s->part.seps.size()) * L * esz);
     ALLOC(d_inst_stim, int*, sizeof(int) * s->n_pad);
     ALLOC(d_bad, int*, sizeof(int) * s->n_pad);
     ALLOC(d_row_param, int*, sizeof(int) * m->row_param.size());
     ALLOC(d_row_sec, int*, sizeof(int) * m->row_sec.size());
 #undef ALLOC
-    {
-        std::vector<DevComp> dc;
-        for (const Comp& c : s->part.comps) dc.push_back({c.r, c.u, c.l, c.lk, c.light_lo, c.light_hi});
-        std::vector<DevSep> ds;
-        for (size_t k = 0; k < s->part.seps.size(); ++k)
-            ds.push_back({s->part.seps[k], s->part.sep_par[k], s->part.sep_comp[k], 0});
-        if (!dc.empty()) cudaMemcpy(s->d_comps, dc.data(), sizeof(DevComp) * dc.size(), cudaMemcpyHostToDevice);
-        cudaMemcpy(s->d_seps, ds.data(), sizeof(DevSep) * ds.size(), cudaMemcpyHostToDevice);
+    if ((rc = sim_upload_split(s)) != NGPU_OK) {
+        sim_free(s);
+        return rc;
     }
     std::vector<int> inst_stim(s->n_pad);
     for (int k = 0; k < s->n_pad; ++k) inst_stim[k] = std::min(k, s->n_inst - 1) % n_stim;
@@ -1591,9 +1615,22 @@ int ngpu_batch_create(ngpu_sim* const* sims, int32_t n, ngpu_batch** out) {
         if (sims[k]->batch) return fail(NGPU_E_INVALID, "a simulation belongs to one batch at a time");
         if (sims[k]->layout != NGPU_LAYOUT_LANE_INSTANCE)
             return fail(NGPU_E_INVALID, "a batch holds lane-instance simulations only");
-        if (sims[k]->n_warps > kMaxWarps)
-            return fail(NGPU_E_INVALID, "a batch holds simulations of at most " + std::to_string(kMaxWarps) +
-                                            " warps per CTA");
+    }
+    // the batch kernel runs CTAs of up to kMaxWarps warps: a member created
+    // with wider CTAs (a small batch of its own) is split again for them
+    // and must be initialised again (through the batch)
+    for (int k = 0; k < n; ++k) {
+        ngpu_sim* s = sims[k];
+        if (s->n_warps <= kMaxWarps) continue;
+        const int W = std::min(kMaxWarps, std::max(1, s->m->n / 48));
+        s->n_warps = W;
+        s->part = make_partition(s->m, W, s->items_per_warp);
+        s->s2_stage = s->precision == NGPU_FP64
+                          ? choose_s2_stage<double>(s->m->n, (int)s->part.seps.size(), W, s->n_groups)
+                          : choose_s2_stage<float>(s->m->n, (int)s->part.seps.size(), W, s->n_groups);
+        const int rc = sim_upload_split(s);
+        if (rc != NGPU_OK) return rc;
+        s->initialized = false;
     }
     ngpu_batch* b = new (std::nothrow) ngpu_batch();
     if (!b) return fail(NGPU_E_NOMEM, "host allocation failed");

@@ -143,7 +143,11 @@ def test_uneven_batch_fp64_vs_oracle_sample(ngpu_built, oracle, workloads):
     rounding)."""
     from neurogpu_b200.sim import Batch
     sims = _sims(workloads, precision="fp64")
+    # members this small default to CTAs of more than 8 warps; the batch
+    # kernel takes up to 8, so joining the batch splits them again
+    assert max(s.layout()["cta_warps"] for s in sims) > 8
     b = Batch(sims)
+    assert all(s.layout()["cta_warps"] <= 8 for s in sims)
     assert sims[0].param_folds() >= 15
     b.init(workloads[0].v_init)
     b.advance(0, workloads[0].nt)

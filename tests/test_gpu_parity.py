@@ -95,6 +95,26 @@ def test_items_per_warp_split_matches_oracle(ngpu_built, refs, cfg, name, items)
     assert err <= TOL_FP64_MV, f"{name}, {items} items per warp: FP64 max|dV| = {err:.3e} mV"
 
 
+@pytest.mark.parametrize("name,warps", [("hh", 4), ("hh", 8), ("hh", 12), ("ttpc", 8), ("ttpc", 16)])
+def test_cta_warps_match_oracle(ngpu_built, refs, cfg, name, warps):
+    """Lane-instance CTAs of 4 to 16 warps (these batches are at most one
+    32-instance group per SM, so CTAs of more than 8 warps run the
+    runtime-compiled kernel at one CTA per SM, the library's default here):
+    FP64 against the oracle."""
+    w = cfg[name]
+    got = _gpu_run(w, "fp64", n_warps=warps)
+    err = np.max(np.abs(got.astype(np.float64) - refs[name]))
+    assert err <= TOL_FP64_MV, f"{name}, {warps} warps: FP64 max|dV| = {err:.3e} mV"
+
+
+def test_small_batch_default_is_wide(ngpu_built, cfg):
+    from neurogpu_b200.sim import Simulator
+    w = cfg["ttpc"]
+    s = Simulator(w.cell, w.n_sets, w.n_stim, "fp32")
+    assert s.layout()["layout"] == "lane" and s.layout()["cta_warps"] == 16
+    s.close()
+
+
 @pytest.mark.parametrize("name", ["passive", "hh", "ttpc"])
 def test_warp_layout_fp64_matches_oracle(ngpu_built, refs, cfg, name):
     """The warp-instance layout (one warp per instance, the tree split over
