@@ -26,7 +26,12 @@
 //
 // Every wait is bounded: past the limit the kernel records an error in
 // *err, skips the epilogue and still frees its tensor memory.
+//
+// k_gemm_bf16_tma below is the TMA-fed, warp-specialised form with
+// 128-byte-swizzled operands; the host runs it where it can build the tensor
+// maps, and this cp.async kernel otherwise.
 #pragma once
+#include <cuda.h>  // CUtensorMap
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -144,6 +149,76 @@ struct GemmSmem {
 constexpr int kStageStride = 17;
 static_assert(kGemmBM * kGemmBK * 2 >= 4 * 32 * kStageStride * 4, "staging fits in the first A stage");
 
+// Epilogue of a 128 x BN tile whose accumulator is in tensor memory at
+// `tmem`: each warp reads its 32 lanes (rows), 16 columns at a time, stages
+// them in shared memory at `stage` (4 x 32 x kStageStride floats) and writes
+// the outputs with coalesced stores (see GemmEpilogue).
+template <int BN, int EPI>
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, float* stage, int m0, int n0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    {
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        float* stg = stage + warp * 32 * kStageStride;
+        const int mw = m0 + warp * 32;  // this warp's first row
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(trow + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 16; ++j) stg[lane * kStageStride + j] = __uint_as_float(r[j]);
+            __syncwarp();
+            // coalesced pass: element e = j * 32 + lane is row e / 16, column e % 16
+#pragma unroll 4
+            for (int j = 0; j < 16; ++j) {
+                const int e = j * 32 + lane, row = e >> 4, col = e & 15;
+                const int m = mw + row, n = n0 + c0 + col;
+                float* sp = stg + row * kStageStride + col;
+                if (m < g.M && n < g.N) {
+                    const size_t o = (size_t)m * g.ldo + n;
+                    const float d = *sp;
+                    if constexpr (EPI == kEpiStore) {
+                        g.out_f32[o] = d;
+                    } else if constexpr (EPI == kEpiBias) {
+                        g.out_f32[o] = d + g.bias[n];
+                    } else if constexpr (EPI == kEpiSplitAdd) {
+                        atomicAdd(g.out_f32 + o, d);
+                    } else if constexpr (EPI == kEpiBiasGelu) {
+                        const float z = d + g.bias[n];
+                        const __nv_bfloat16 h = __float2bfloat16_rn(gelu_tanh(z));
+                        g.out_f32[o] = z;
+                        g.out_bf16[o] = h;
+                        *sp = __bfloat162float(h);
+                    } else {  // kEpiGeluGrad
+                        const __nv_bfloat16 h = __float2bfloat16_rn(d * gelu_tanh_grad(g.zin[o]));
+                        g.out_bf16[o] = h;
+                        *sp = __bfloat162float(h);
+                    }
+                }
+            }
+            if constexpr (EPI == kEpiBiasGelu || EPI == kEpiGeluGrad) {
+                // the transposed bf16 copy, lane = row: a warp store is 32 consecutive rows
+                __syncwarp();
+                const int m = mw + lane;
+                if (m < g.M) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int n = n0 + c0 + j;
+                        if (n < g.N)
+                            g.out_bf16_t[(size_t)n * g.ldt + m] = __float2bfloat16_rn(stg[lane * kStageStride + j]);
+                    }
+                }
+            }
+            __syncwarp();  // the next chunk overwrites the staging rows
+        }
+    }
+}
+
 template <int BN, int EPI>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
     static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "BN: a multiple of 16 in [32, 256]");
@@ -152,7 +227,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
     // align the ring to 1024 bytes (descriptor base offset 0)
     GemmSmem<BN>& Sm = *reinterpret_cast<GemmSmem<BN>*>(
         (void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
     constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // power of two >= 32 for BN in {32, 64, 128, 256}
 
@@ -235,65 +310,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
     ok = __syncthreads_and(ok);  // also: every thread is done with the ring before it stages the epilogue
 
     if (ok) {
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        float* stg = reinterpret_cast<float*>(Sm.a[0]) + warp * 32 * kStageStride;
-        const int mw = m0 + warp * 32;  // this warp's first row
-#pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            uint32_t r[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(trow + (uint32_t)c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int j = 0; j < 16; ++j) stg[lane * kStageStride + j] = __uint_as_float(r[j]);
-            __syncwarp();
-            // coalesced pass: element e = j * 32 + lane is row e / 16, column e % 16
-#pragma unroll 4
-            for (int j = 0; j < 16; ++j) {
-                const int e = j * 32 + lane, row = e >> 4, col = e & 15;
-                const int m = mw + row, n = n0 + c0 + col;
-                float* sp = stg + row * kStageStride + col;
-                if (m < g.M && n < g.N) {
-                    const size_t o = (size_t)m * g.ldo + n;
-                    const float d = *sp;
-                    if constexpr (EPI == kEpiStore) {
-                        g.out_f32[o] = d;
-                    } else if constexpr (EPI == kEpiBias) {
-                        g.out_f32[o] = d + g.bias[n];
-                    } else if constexpr (EPI == kEpiSplitAdd) {
-                        atomicAdd(g.out_f32 + o, d);
-                    } else if constexpr (EPI == kEpiBiasGelu) {
-                        const float z = d + g.bias[n];
-                        const __nv_bfloat16 h = __float2bfloat16_rn(gelu_tanh(z));
-                        g.out_f32[o] = z;
-                        g.out_bf16[o] = h;
-                        *sp = __bfloat162float(h);
-                    } else {  // kEpiGeluGrad
-                        const __nv_bfloat16 h = __float2bfloat16_rn(d * gelu_tanh_grad(g.zin[o]));
-                        g.out_bf16[o] = h;
-                        *sp = __bfloat162float(h);
-                    }
-                }
-            }
-            if constexpr (EPI == kEpiBiasGelu || EPI == kEpiGeluGrad) {
-                // the transposed bf16 copy, lane = row: a warp store is 32 consecutive rows
-                __syncwarp();
-                const int m = mw + lane;
-                if (m < g.M) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const int n = n0 + c0 + j;
-                        if (n < g.N)
-                            g.out_bf16_t[(size_t)n * g.ldt + m] = __float2bfloat16_rn(stg[lane * kStageStride + j]);
-                    }
-                }
-            }
-            __syncwarp();  // the next chunk overwrites the staging rows
-        }
+        gemm_epilogue<BN, EPI>(g, tmem, reinterpret_cast<float*>(Sm.a[0]), m0, n0);
     } else if (threadIdx.x == 0) {
         atomicExch(g.err, 1);
     }
@@ -301,6 +318,152 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// TMA-fed, warp-specialised form of the same GEMM (the default where the
+// driver's tensor-map encoder is available).
+//
+// Operands arrive by TMA (cp.async.bulk.tensor, this GPU's own memory, no
+// multicast) as 64-wide K tiles in the 128-byte-swizzled K-major layout: a
+// row's 64 bf16 (128 bytes) is one swizzle atom row, 8 rows make a 1024-byte
+// atom (SBO = 1024), and each 16-wide K step of the MMA starts 32 bytes
+// further into the atom.  One thread of warp 0 is the producer: per K tile
+// it waits until the stage's previous MMAs are done (the stage's `empty`
+// barrier, which tcgen05.commit arrives on), then posts the tile's byte
+// count on the stage's `full` barrier and issues the two tile loads, which
+// complete it.  One thread of warp 1 issues the MMAs: it waits on `full`,
+// issues four tcgen05.mma and commits them to `empty`; after the last tile
+// it commits to `done`.  No block barrier inside the K loop.  All four
+// warps then run the same epilogue as the cp.async kernel.  Rows past M or
+// N are zero-filled by TMA; every wait is bounded as above.
+template <int BN>
+__host__ __device__ constexpr int tma_stages() {
+    return BN >= 256 ? 4 : (BN >= 128 ? 6 : 8);
+}
+
+template <int BN>
+struct TmaSmem {
+    static constexpr int kStages = tma_stages<BN>();
+    alignas(1024) unsigned char a[kStages][kGemmBM * kGemmBK * 2];
+    alignas(1024) unsigned char b[kStages][BN * kGemmBK * 2];
+    alignas(8) uint64_t full[kStages];
+    alignas(8) uint64_t empty[kStages];
+    alignas(8) uint64_t done;
+    uint32_t tmem;
+};
+
+// Shared-memory matrix descriptor of a 128-byte-swizzled K-major tile
+// (start >> 4; LBO 16 bytes, unused for this layout; SBO 1024 bytes;
+// version 1 at bit 46; layout type 2 = SWIZZLE_128B at bit 61).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// 2-D tile load: the box at (x = K element, y = row) of the tensor map into
+// shared memory at dst, completing `bytes` on barrier bar.  x is a multiple
+// of 64 elements (128 bytes).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tma(const __grid_constant__ CUtensorMap tma_a,
+                                                               const __grid_constant__ CUtensorMap tma_b, GemmArgs g) {
+    static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "BN: a multiple of 16 in [32, 256]");
+    constexpr int S = tma_stages<BN>();
+    constexpr uint32_t kTileBytes = (uint32_t)(kGemmBM + BN) * kGemmBK * 2;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TmaSmem<BN>& Sm = *reinterpret_cast<TmaSmem<BN>*>((void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
+    constexpr uint32_t kCols = BN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&Sm.tmem)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(smem_u32(&Sm.full[s]), 1);
+            mbar_init(smem_u32(&Sm.empty[s]), 1);
+        }
+        mbar_init(smem_u32(&Sm.done), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tma_a) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tma_b) : "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = Sm.tmem;
+
+    const int kt0 = blockIdx.z * g.kt_split;
+    const int KT = min(g.kt_split, g.K / kGemmBK - kt0);
+    bool ok = true;
+    if (warp == 0 && lane == 0) {  // producer
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % S;
+            if (kt >= S) ok = ok && mbar_wait(smem_u32(&Sm.empty[s]), (uint32_t)(kt / S - 1) & 1u);
+            const uint32_t full = smem_u32(&Sm.full[s]);
+            mbar_arrive_expect_tx(full, kTileBytes);
+            tma_load_2d(smem_u32(Sm.a[s]), &tma_a, (kt0 + kt) * kGemmBK, m0, full);
+            tma_load_2d(smem_u32(Sm.b[s]), &tma_b, (kt0 + kt) * kGemmBK, n0, full);
+        }
+    } else if (warp == 1 && lane == 0) {  // MMA issuer
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % S;
+            ok = ok && mbar_wait(smem_u32(&Sm.full[s]), (uint32_t)(kt / S) & 1u);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (ok) {
+                const uint32_t sa = smem_u32(Sm.a[s]), sb = smem_u32(Sm.b[s]);
+#pragma unroll
+                for (int k = 0; k < kGemmBK / 16; ++k) {  // 16 bf16 = 32 bytes further into the swizzle atom
+                    const uint64_t da = umma_desc_sw128(sa + k * 32), db = umma_desc_sw128(sb + k * 32);
+                    const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(umma_idesc<BN>()), "r"(acc)
+                        : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&Sm.empty[s]))
+                         : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&Sm.done))
+                     : "memory");
+    }
+    __syncwarp();
+    ok = ok && mbar_wait(smem_u32(&Sm.done), 0u);  // every MMA (and so every load) is done
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    ok = __syncthreads_and(ok);
+    if (ok) {
+        gemm_epilogue<BN, EPI>(g, tmem, reinterpret_cast<float*>(Sm.a[0]), m0, n0);
+    } else if (threadIdx.x == 0) {
+        atomicExch(g.err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+template <int BN>
+constexpr size_t gemm_tma_smem_bytes() {
+    return sizeof(TmaSmem<BN>) + 1024;
 }
 
 template <int BN>

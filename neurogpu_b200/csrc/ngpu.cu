@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/ngpu.h"
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 #include "features.cuh"
 #include "ga.cuh"
 #include "gemm_tc.cuh"
@@ -2250,8 +2251,66 @@ static int gemm_k_split(const GemmArgs& g, int bn, int epi, int* splits) {
     return per;
 }
 
+// The driver's tensor-map encoder (cuTensorMapEncodeTiled), looked up once
+// through the runtime; nullptr where the driver does not offer it.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        }
+        return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }();
+    return fn;
+}
+
+// Tensor map of a bf16 operand [rows][ld] read in boxes of 64 (K) x box_rows,
+// 128-byte swizzle, zero fill past the edges.
+static bool gemm_tensor_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int K, int ld, int box_rows) {
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(__nv_bfloat16)};
+    const cuuint32_t box[2] = {(cuuint32_t)kGemmBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA kernel runs where the tensor maps can be built and every tile box
+// fits its operand (M >= 128 rows, N >= BN); NGPU_GEMM_TMA=0 selects the
+// cp.async kernel everywhere.
+static bool gemm_use_tma(const GemmArgs& g, int bn) {
+    const char* ev = getenv("NGPU_GEMM_TMA");
+    if (ev && ev[0] == '0') return false;
+    return g.M >= kGemmBM && g.N >= bn && tensor_map_encoder() != nullptr;
+}
+
 template <int BN, int EPI>
 static cudaError_t launch_gemm_bn(GemmArgs g, cudaStream_t st) {
+    if (gemm_use_tma(g, BN)) {
+        CUtensorMap ta, tb;
+        if (gemm_tensor_map(&ta, g.A, g.M, g.K, g.lda, kGemmBM) && gemm_tensor_map(&tb, g.B, g.N, g.K, g.ldb, BN)) {
+            const size_t smem = gemm_tma_smem_bytes<BN>();
+            cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tma<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            int splits = 1;
+            g.kt_split = gemm_k_split(g, BN, EPI, &splits);
+            if (EPI == kEpiSplitAdd) {
+                e = cudaMemsetAsync(g.out_f32, 0, sizeof(float) * ((size_t)(g.M - 1) * g.ldo + g.N), st);
+                if (e != cudaSuccess) return e;
+            }
+            dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + BN - 1) / BN, splits);
+            k_gemm_bf16_tma<BN, EPI><<<grid, kGemmThreads, smem, st>>>(ta, tb, g);
+            g_launches++;
+            return cudaGetLastError();
+        }
+    }
     const size_t smem = gemm_smem_bytes<BN>();
     cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tn<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

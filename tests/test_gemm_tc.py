@@ -20,6 +20,14 @@ def _gelu_grad(z):
     return 0.5 * (1 + t) + 0.5 * z * (1 - t * t) * 0.7978845608028654 * (1 + 3 * 0.044715 * z * z)
 
 
+@pytest.fixture(params=["tma", "cp.async"])
+def gemm_path(request, monkeypatch):
+    """Both forms of the kernel: the TMA-fed warp-specialised one (the
+    default) and the cp.async one (NGPU_GEMM_TMA=0)."""
+    monkeypatch.setenv("NGPU_GEMM_TMA", "1" if request.param == "tma" else "0")
+    return request.param
+
+
 def _bf16(x):
     import torch
     return torch.as_tensor(x, dtype=torch.float32).to(torch.bfloat16)
@@ -50,7 +58,7 @@ def _gemm(A, B, epi=0, bn=128, bias=None, zin=None):
 
 @pytest.mark.parametrize("M,N,K,bn", [(128, 128, 64, 128), (256, 512, 512, 128), (200, 20, 64, 32),
                                       (1000, 96, 128, 64), (384, 512, 256, 256), (8192, 512, 512, 128)])
-def test_gemm_matches_fp64(ngpu_built, M, N, K, bn):
+def test_gemm_matches_fp64(ngpu_built, gemm_path, M, N, K, bn):
     rng = np.random.default_rng(M + N + K)
     A = _bf16(rng.normal(size=(M, K)))
     B = _bf16(rng.normal(size=(N, K)))
@@ -63,7 +71,7 @@ def test_gemm_matches_fp64(ngpu_built, M, N, K, bn):
 
 @pytest.mark.parametrize("M,N,K,bn", [(512, 512, 4096, 128), (512, 64, 8192, 64), (200, 20, 1024, 32),
                                       (128, 128, 64, 128)])
-def test_gemm_split_k_matches_fp64(ngpu_built, M, N, K, bn):
+def test_gemm_split_k_matches_fp64(ngpu_built, gemm_path, M, N, K, bn):
     """Epilogue 4: K spread over CTAs whose partial sums add into the zeroed
     output; the same fp32 bound as one CTA per tile (sums of K terms in
     another order)."""
@@ -77,7 +85,7 @@ def test_gemm_split_k_matches_fp64(ngpu_built, M, N, K, bn):
     assert np.all(np.abs(got - want) <= bound)
 
 
-def test_gemm_bias_gelu_epilogue(ngpu_built):
+def test_gemm_bias_gelu_epilogue(ngpu_built, gemm_path):
     rng = np.random.default_rng(7)
     M, N, K = 300, 128, 192
     A, B = _bf16(rng.normal(size=(M, K))), _bf16(rng.normal(size=(N, K)) * 0.2)
@@ -90,7 +98,7 @@ def test_gemm_bias_gelu_epilogue(ngpu_built):
     np.testing.assert_array_equal(ht, h.T)
 
 
-def test_gemm_gelu_grad_epilogue(ngpu_built):
+def test_gemm_gelu_grad_epilogue(ngpu_built, gemm_path):
     rng = np.random.default_rng(8)
     M, N, K = 256, 64, 128
     A, B = _bf16(rng.normal(size=(M, K))), _bf16(rng.normal(size=(N, K)) * 0.3)
