@@ -61,6 +61,45 @@ def test_static_entry_point_matches_regular_run(ngpu_built):
     model.close()
 
 
+def test_static_entry_point_ttpc_set_and_repeated_site(ngpu_built):
+    """The TTPC mechanism set's kernel (the passive cable runs it), with a
+    recording site requested twice, against ngpu_run; and a warm call leaves
+    the device's free memory as it found it (no allocation)."""
+    import torch
+    from neurogpu_b200 import configs
+    from neurogpu_b200.sim import Model, run
+    w = configs.passive_cable(n_sets=6, t_stop=40.0)
+    rec = np.array([0, 17, 17, w.cell.n_nodes - 1], dtype=np.int32)
+    model = Model(w.cell)
+    ref = run(model, w.params, w.amps, w.dts, w.stim_node, w.stim_area, rec, w.v_init).astype(np.float64)
+    from neurogpu_b200 import _ffi
+    stream = torch.cuda.current_stream().cuda_stream
+    dev = torch.device("cuda", 0)
+    params = torch.from_numpy(np.ascontiguousarray(w.params, dtype=np.float32)).to(dev)
+    amps = torch.from_numpy(np.ascontiguousarray(w.amps, dtype=np.float32)).to(dev)
+    dts = torch.from_numpy(w.dts).to(dev)
+    outs = [torch.full((w.n_sets, w.n_stim, rec.size, w.nt), float("nan"), dtype=torch.float32, device=dev)
+            for _ in range(2)]
+
+    def call(out):
+        _ffi.check("ngpu_run_static", _ffi.lib().ngpu_run_static(
+            model.handle, w.n_sets, C.c_void_p(params.data_ptr()), w.n_stim, w.nt, C.c_void_p(amps.data_ptr()),
+            C.c_void_p(dts.data_ptr()), w.stim_node, w.stim_area, rec.size, _ffi.ptr(rec), w.v_init,
+            C.c_void_p(out.data_ptr()), C.c_void_p(stream)))
+        torch.cuda.synchronize()
+    call(outs[0])
+    free_before = torch.cuda.mem_get_info()[0]
+    call(outs[1])                                   # warm: every buffer is the caller's or the static array
+    assert torch.cuda.mem_get_info()[0] == free_before
+    first, second = (o.cpu().numpy() for o in outs)
+    for got in (first, second):
+        assert got.shape == ref.shape and np.all(np.isfinite(got))
+        assert np.array_equal(got[:, :, 1], got[:, :, 2])
+        assert float(np.max(np.abs(got - ref))) <= TOL_SUB_MV
+    assert np.array_equal(first, second)
+    model.close()
+
+
 def test_static_entry_point_rejects_oversize_runs(ngpu_built):
     import torch
     from neurogpu_b200 import _ffi, configs
