@@ -1515,10 +1515,21 @@ static BatchArgs<R> make_batch_args(ngpu_batch* b) {
     BatchArgs<R> B;
     memset((void*)&B, 0, sizeof(B));
     B.n = (int)b->sims.size();
-    int c = 0;
+    // CTAs are dealt to the members in order of decreasing cost per CTA (the
+    // tree's channel weight): the GPU starts the longest CTAs first and fills
+    // in with the short ones, instead of ending on a tail of long CTAs
+    std::vector<int> order(B.n);
+    std::vector<int64_t> cost(B.n, 0);
     for (int k = 0; k < B.n; ++k) {
-        B.sim[k] = make_args<R>(b->sims[k]);
-        B.cta0[k] = c;
+        order[k] = k;
+        for (int64_t w : b->sims[k]->m->weight) cost[k] += w;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    int c = 0;
+    for (int j = 0; j < B.n; ++j) {
+        const int k = order[j];
+        B.sim[j] = make_args<R>(b->sims[k]);
+        B.cta0[j] = c;
         c += b->sims[k]->n_groups;
     }
     B.cta0[B.n] = c;
