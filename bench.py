@@ -486,8 +486,10 @@ def run_gemm(args):
     (batch 8192, width 512: forward layers, the weight gradients over the
     batch) and at square sizes, against torch.matmul (cuBLAS) on the same
     operands.  Device time with CUDA events over `--steps` calls after
-    `--warmup`; value = TFLOP/s of the 8192^3 GEMM, frac of the measured
-    cuBLAS bf16 peak (MEASURED_PEAKS.json bf16_tflops, burst)."""
+    `--warmup`, and per call inside a CUDA graph of 20 calls (graph_ms: the
+    host's per-call work, which bounds the small shapes from Python, left
+    out); value = TFLOP/s of the 8192^3 GEMM, frac of the measured cuBLAS
+    bf16 peak (MEASURED_PEAKS.json bf16_tflops, burst)."""
     import torch
     from neurogpu_b200 import _ffi
     L = _ffi.lib()
@@ -509,6 +511,30 @@ def run_gemm(args):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / args.steps
 
+    def graph_ms(fn, n=20):
+        """Device time of one call with the host out of the loop: n calls
+        captured once as a CUDA graph, the graph replayed after warm-up."""
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            fn()
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(n):
+                fn()
+        for _ in range(max(args.warmup, 1)):
+            graph.replay()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+        del graph
+        return a.elapsed_time(b) / n
+
     rows = {}
     g = torch.Generator(device="cuda").manual_seed(0)
     # (name, M, N, K, bn, epilogue): epilogue 0 store fp32, 1 bias + GELU (three outputs),
@@ -524,14 +550,17 @@ def run_gemm(args):
         ob = torch.empty(M, N, device="cuda", dtype=torch.bfloat16)
         obt = torch.empty(N, M, device="cuda", dtype=torch.bfloat16)
         bias = torch.zeros(N, device="cuda", dtype=torch.float32)
-        st = torch.cuda.current_stream().cuda_stream
-
         def ours():
             _ffi.check("ngpu_gemm_bf16_tn", L.ngpu_gemm_bf16_tn(
                 A.data_ptr(), B.data_ptr(), M, N, K, K, K, epi, bn, out.data_ptr(),
                 ob.data_ptr() if epi == 1 else None, obt.data_ptr() if epi == 1 else None, N, M,
-                bias.data_ptr() if epi == 1 else None, None, st))
+                bias.data_ptr() if epi == 1 else None, None, torch.cuda.current_stream().cuda_stream))
         ms = dev_ms(ours)
+        try:
+            ms_graph = graph_ms(ours)
+        except Exception as exc:  # capture refused: report the eager figure only
+            print(f"gemm {name}: graph timing skipped ({exc})", file=sys.stderr)
+            ms_graph = None
         ref = torch.matmul(A.float(), B.float().t()) if M * N * K <= 4096 ** 3 else None
         ours()
         torch.cuda.synchronize()
@@ -540,12 +569,16 @@ def run_gemm(args):
             got = out if epi == 0 else out - bias
             err = float((got - ref).abs().max() / ref.abs().max())
         ms_cublas = dev_ms(lambda: torch.matmul(A, B.t()))
+        cb_out = torch.empty(M, N, device="cuda", dtype=torch.bfloat16)
+        ms_cublas_graph = graph_ms(lambda: torch.matmul(A, B.t(), out=cb_out))
         fl = 2.0 * M * N * K
         rows[name] = {"ms": ms, "tflops": fl / ms / 1e9, "cublas_ms": ms_cublas,
-                      "cublas_tflops": fl / ms_cublas / 1e9, "bn": bn,
+                      "cublas_tflops": fl / ms_cublas / 1e9,
+                      "graph_ms": ms_graph, "graph_tflops": fl / ms_graph / 1e9 if ms_graph else None,
+                      "cublas_graph_ms": ms_cublas_graph, "bn": bn,
                       "epilogue": {0: "store f32", 1: "bias+gelu (f32, bf16, bf16^T)", 4: "store f32, split K"}[epi],
                       "max_rel_err_vs_fp32": err}
-        del A, B, out, ob, obt
+        del A, B, out, ob, obt, cb_out
     v = rows["square_8192"]["tflops"]
     print(json.dumps({
         "metric": "tcgen05 BF16 GEMM TFLOP/s (8192^3)", "value": v, "unit": "TFLOP/s", "higher_is_better": True,

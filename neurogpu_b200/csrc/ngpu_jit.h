@@ -148,6 +148,7 @@ inline std::string source(int ms, bool fp64, const std::vector<uint32_t>& masks,
     }
     return std::string(ms == 2 ? "#define NGPU_GENERATED_NODE 1\n" : "") +
            std::string(prefetch ? "" : "#define NGPU_CH_PREFETCH 0\n") +
+           std::string(adv_warps > 8 && adv_ctas == 1 ? "#define NGPU_CH_AHEAD 0\n" : "") +
            std::string(complete ? "#define NGPU_CLASSES_COMPLETE 1\n" : "") + fold +
            "#include \"sim_kernels.cuh\"\n"
            "using JitClasses = ngpu::MaskList<" + list + ">;\n"

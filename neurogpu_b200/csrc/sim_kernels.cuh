@@ -72,6 +72,12 @@ constexpr int kMaxWarps = 8;   // 256 threads; with 3 CTAs per SM the 85-registe
 #ifndef NGPU_CH_PREFETCH
 #define NGPU_CH_PREFETCH 1
 #endif
+// Without that prefetch, the channel pass starts each node's loads one node
+// early (channels_item).  The runtime-specialised kernels for CTAs of more
+// than 8 warps at one CTA per SM turn it off: there it measured 4 % slower.
+#ifndef NGPU_CH_AHEAD
+#define NGPU_CH_AHEAD 1
+#endif
 
 // Per-node record, identical for every instance; staged in shared memory
 // once per launch (32 bytes in FP32).
@@ -282,6 +288,15 @@ __device__ __forceinline__ void prefetch_channels(const Group<R>& G, const NodeR
         if (n.srows) prefetch_l2(G.slab + (size_t)n.srow * kLanes, n.srows * kLanes * sizeof(R));
         if (n.prows) prefetch_l2(G.ptab + (size_t)n.prow * kLanes, n.prows * kLanes * sizeof(float));
     }
+}
+
+// L2 prefetch of node n's state and parameter rows, one row per lane (the
+// row's 128 bytes are one cache line; lane r's own element lies in row r).
+template <typename R>
+__device__ __forceinline__ void prefetch_rows_l2(const Group<R>& G, const NodeRec<R>& n) {
+    const int r = threadIdx.x & 31;
+    if (r < n.srows) asm volatile("prefetch.global.L2 [%0];" ::"l"(G.slab + (size_t)(n.srow + r) * kLanes));
+    if (r < n.prows) asm volatile("prefetch.global.L2 [%0];" ::"l"(G.ptab + (size_t)(n.prow + r) * kLanes));
 }
 
 // A junction row: its FP64 sum with the chain carry and the accumulator of
@@ -685,21 +700,48 @@ __device__ __forceinline__ void channels_item(const SimArgs<R>& A, const Group<R
     SpineCarry<R> k;
     k.reset();
     R e_l = 0;
-    int vi = -1;  // node whose V was read last as a parent voltage
-    R vv = 0;
     constexpr bool pf = NGPU_CH_PREFETCH != 0 && !TI;
+    // Without the bulk prefetch (models whose nodes read few rows), a node's
+    // loads are started one node early instead: its voltages (its own and
+    // its parent's; the pass writes no voltage) into registers, its state and
+    // parameter rows into L2 (one prefetch per row, lane r taking row r).
+    // Either alone measured slower on B200 (the node still waits for the
+    // other); both together, 2.7 % faster on the TTPC-like cell.  Models with
+    // the bulk prefetch keep the register budget for their channel code.
+    constexpr bool ahead = NGPU_CH_AHEAD != 0 && !pf && !TI;
     if (pf && n > 0) prefetch_channels(G, nr[node_at(0)]);
     if (pf && n > 1) prefetch_channels(G, nr[node_at(1)]);
+    int vi = -1;  // node whose V was read last as a parent voltage (!ahead)
+    R vv = 0;
+    int i_nx = 0;  // the next node and its voltages (ahead)
+    R v_nx = 0, vp_nx = 0;
+    if (ahead && n > 0) {
+        i_nx = node_at(0);
+        v_nx = G.vbuf[(size_t)i_nx * 2 * kLanes];
+        vp_nx = i_nx == 0 ? v_nx : G.vbuf[(size_t)nr[i_nx].parent * 2 * kLanes];
+    }
     for (int p = 0; p < n; ++p) {
-        const int i = node_at(p);
+        const int i = ahead ? i_nx : node_at(p);
         const NodeRec<R> nd = nr[i];
         if (pf && p + 2 < n) prefetch_channels(G, nr[node_at(p + 2)]);
-        R V;
-        if (vi == i) V = vv;
-        else V = G.vbuf[(size_t)i * 2 * kLanes];
-        const R vp = i == 0 ? V : G.vbuf[(size_t)nd.parent * 2 * kLanes];
-        vi = nd.parent;
-        vv = vp;
+        R V, vp;
+        if constexpr (ahead) {
+            V = v_nx;
+            vp = vp_nx;
+            if (p + 1 < n) {
+                i_nx = node_at(p + 1);
+                const NodeRec<R>& nn = nr[i_nx];
+                v_nx = i_nx == nd.parent ? vp : G.vbuf[(size_t)i_nx * 2 * kLanes];
+                vp_nx = i_nx == 0 ? v_nx : G.vbuf[(size_t)nn.parent * 2 * kLanes];
+                prefetch_rows_l2(G, nn);
+            }
+        } else {
+            if (vi == i) V = vv;
+            else V = G.vbuf[(size_t)i * 2 * kLanes];
+            vp = i == 0 ? V : G.vbuf[(size_t)nd.parent * 2 * kLanes];
+            vi = nd.parent;
+            vv = vp;
+        }
         R x, rhs, e;
         assemble_node<R, MS, false, Classes>(A, G, nd, i, V, vp, dt, dtn_inv, istim_amp, x, rhs, e);
         if (p < n_light) {
