@@ -539,7 +539,9 @@ def run_gemm(args):
     g = torch.Generator(device="cuda").manual_seed(0)
     # (name, M, N, K, bn, epilogue): epilogue 0 store fp32, 1 bias + GELU (three outputs),
     # 4 store fp32 with K split over CTAs
-    shapes = [("fwd_hidden_8192x512x512", 8192, 512, 512, 128, 1), ("fwd_input_8192x512x64", 8192, 512, 64, 128, 1),
+    shapes = [("fwd_hidden_8192x512x512", 8192, 512, 512, 128, 1),
+              ("fwd_hidden_8192x512x512_bn256", 8192, 512, 512, 256, 1),
+              ("fwd_input_8192x512x64", 8192, 512, 64, 128, 1), ("fwd_input_8192x512x64_bn256", 8192, 512, 64, 256, 1),
               ("fwd_out_8192x32x512", 8192, 32, 512, 32, 0), ("dW_512x512x8192", 512, 512, 8192, 128, 0),
               ("dW_512x512x8192_splitK", 512, 512, 8192, 128, 4),
               ("square_4096", 4096, 4096, 4096, 256, 0), ("square_8192", 8192, 8192, 8192, 256, 0)]

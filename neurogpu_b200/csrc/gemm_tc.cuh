@@ -38,6 +38,10 @@
 namespace ngpu {
 
 constexpr int kGemmThreads = 128;
+// The TMA kernel's CTA: one producer thread and one MMA thread during the
+// main loop, then all 16 warps in the epilogue (four per 32-lane quarter of
+// tensor memory, each on its own column slice).
+constexpr int kTmaThreads = 512;
 constexpr int kGemmBM = 128;
 constexpr int kGemmBK = 64;
 constexpr uint32_t kSpinLimit = 1u << 26;
@@ -150,18 +154,24 @@ constexpr int kStageStride = 17;
 static_assert(kGemmBM * kGemmBK * 2 >= 4 * 32 * kStageStride * 4, "staging fits in the first A stage");
 
 // Epilogue of a 128 x BN tile whose accumulator is in tensor memory at
-// `tmem`: each warp reads its 32 lanes (rows), 16 columns at a time, stages
-// them in shared memory at `stage` (4 x 32 x kStageStride floats) and writes
-// the outputs with coalesced stores (see GemmEpilogue).
-template <int BN, int EPI>
+// `tmem`, by the CTA's NW warps: warp w reads the 32 lanes (rows) of quarter
+// w % 4 (the lanes tcgen05.ld lets it reach) over column slice w / 4 of the
+// tile, 16 columns at a time, stages them in shared memory at `stage`
+// (NW x 32 x kStageStride floats) and writes the outputs with coalesced
+// stores (see GemmEpilogue).  Warps past the last slice have no work.
+template <int BN, int EPI, int NW = 4>
 __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, float* stage, int m0, int n0) {
+    constexpr int kSlices = (NW / 4) < (BN / 16) ? (NW / 4) : (BN / 16);
+    constexpr int kCols = BN / kSlices;  // a multiple of 16
+    static_assert(NW % 4 == 0 && kCols % 16 == 0, "epilogue slices");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    {
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const int q = warp & 3, slice = warp >> 2;
+    if (slice < kSlices) {
+        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         float* stg = stage + warp * 32 * kStageStride;
-        const int mw = m0 + warp * 32;  // this warp's first row
+        const int mw = m0 + q * 32;  // this warp's first row
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
+        for (int c0 = slice * kCols; c0 < (slice + 1) * kCols; c0 += 16) {
             uint32_t r[16];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -310,7 +320,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tn(GemmArgs g) {
     ok = __syncthreads_and(ok);  // also: every thread is done with the ring before it stages the epilogue
 
     if (ok) {
-        gemm_epilogue<BN, EPI>(g, tmem, reinterpret_cast<float*>(Sm.a[0]), m0, n0);
+        gemm_epilogue<BN, EPI, kGemmThreads / 32>(g, tmem, reinterpret_cast<float*>(Sm.a[0]), m0, n0);
     } else if (threadIdx.x == 0) {
         atomicExch(g.err, 1);
     }
@@ -376,7 +386,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 }
 
 template <int BN, int EPI>
-__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tma(const __grid_constant__ CUtensorMap tma_a,
+__global__ void __launch_bounds__(kTmaThreads) k_gemm_bf16_tma(const __grid_constant__ CUtensorMap tma_a,
                                                                const __grid_constant__ CUtensorMap tma_b, GemmArgs g) {
     static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "BN: a multiple of 16 in [32, 256]");
     constexpr int S = tma_stages<BN>();
@@ -451,7 +461,8 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tma(const __grid_con
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     ok = __syncthreads_and(ok);
     if (ok) {
-        gemm_epilogue<BN, EPI>(g, tmem, reinterpret_cast<float*>(Sm.a[0]), m0, n0);
+        static_assert(sizeof(Sm.a) >= (size_t)kTmaThreads * kStageStride * 4, "staging fits in the A stages");
+        gemm_epilogue<BN, EPI, kTmaThreads / 32>(g, tmem, reinterpret_cast<float*>(Sm.a[0]), m0, n0);
     } else if (threadIdx.x == 0) {
         atomicExch(g.err, 1);
     }

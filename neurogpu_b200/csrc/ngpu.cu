@@ -2250,13 +2250,14 @@ extern "C" int ngpu_run_static(ngpu_model* m, int32_t n_sets, const float* param
 static __device__ int g_gemm_err;
 
 // The split of K over CTAs: the whole of K per CTA, except for the split-K
-// epilogue, which spreads K over enough CTAs to give every SM two (each
-// slice at least one 64-wide tile).
-static int gemm_k_split(const GemmArgs& g, int bn, int epi, int* splits) {
+// epilogue, which spreads K over up to `slots` CTAs (the resident CTAs of
+// one wave: two per SM for the cp.async kernel, one for the TMA kernel),
+// each slice at least one 64-wide tile.
+static int gemm_k_split(const GemmArgs& g, int bn, int epi, int slots, int* splits) {
     const int KT = g.K / kGemmBK;
     const int tiles = ((g.M + kGemmBM - 1) / kGemmBM) * ((g.N + bn - 1) / bn);
     int z = 1;
-    if (epi == kEpiSplitAdd) z = std::max(1, std::min(KT, (2 * 148 + tiles - 1) / tiles));
+    if (epi == kEpiSplitAdd) z = std::max(1, std::min(KT, slots / tiles));
     const int per = (KT + z - 1) / z;
     *splits = (KT + per - 1) / per;
     return per;
@@ -2311,13 +2312,13 @@ static cudaError_t launch_gemm_bn(GemmArgs g, cudaStream_t st) {
                                                  (int)smem);
             if (e != cudaSuccess) return e;
             int splits = 1;
-            g.kt_split = gemm_k_split(g, BN, EPI, &splits);
+            g.kt_split = gemm_k_split(g, BN, EPI, kSmCount, &splits);  // one CTA per SM: one wave
             if (EPI == kEpiSplitAdd) {
                 e = cudaMemsetAsync(g.out_f32, 0, sizeof(float) * ((size_t)(g.M - 1) * g.ldo + g.N), st);
                 if (e != cudaSuccess) return e;
             }
             dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + BN - 1) / BN, splits);
-            k_gemm_bf16_tma<BN, EPI><<<grid, kGemmThreads, smem, st>>>(ta, tb, g);
+            k_gemm_bf16_tma<BN, EPI><<<grid, kTmaThreads, smem, st>>>(ta, tb, g);
             g_launches++;
             return cudaGetLastError();
         }
@@ -2326,7 +2327,7 @@ static cudaError_t launch_gemm_bn(GemmArgs g, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tn<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int splits = 1;
-    g.kt_split = gemm_k_split(g, BN, EPI, &splits);
+    g.kt_split = gemm_k_split(g, BN, EPI, 2 * kSmCount, &splits);
     if (EPI == kEpiSplitAdd) {  // the slices add into a zeroed output
         e = cudaMemsetAsync(g.out_f32, 0, sizeof(float) * ((size_t)(g.M - 1) * g.ldo + g.N), st);
         if (e != cudaSuccess) return e;
