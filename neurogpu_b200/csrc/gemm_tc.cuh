@@ -29,7 +29,9 @@
 //
 // k_gemm_bf16_tma below is the TMA-fed, warp-specialised form with
 // 128-byte-swizzled operands; the host runs it where it can build the tensor
-// maps, and this cp.async kernel otherwise.
+// maps, and this cp.async kernel otherwise.  k_gemm_bf16_tma_persistent is
+// its persistent form (one CTA per SM, two accumulators in tensor memory)
+// for GEMMs of more than two tiles per SM.
 #pragma once
 #include <cuda.h>  // CUtensorMap
 #include <cuda_bf16.h>
@@ -154,21 +156,24 @@ constexpr int kStageStride = 17;
 static_assert(kGemmBM * kGemmBK * 2 >= 4 * 32 * kStageStride * 4, "staging fits in the first A stage");
 
 // Epilogue of a 128 x BN tile whose accumulator is in tensor memory at
-// `tmem`, by the CTA's NW warps: warp w reads the 32 lanes (rows) of quarter
-// w % 4 (the lanes tcgen05.ld lets it reach) over column slice w / 4 of the
-// tile, 16 columns at a time, stages them in shared memory at `stage`
-// (NW x 32 x kStageStride floats) and writes the outputs with coalesced
-// stores (see GemmEpilogue).  Warps past the last slice have no work.
+// `tmem`, by NW warps, the CTA's warps w0 .. w0 + NW - 1: warp w reads the 32
+// lanes (rows) of quarter w % 4 (the lanes tcgen05.ld lets it reach) over
+// column slice (w - w0) / 4 of the tile, 16 columns at a time, stages them in
+// shared memory at `stage` (NW x 32 x kStageStride floats) and writes the
+// outputs with coalesced stores (see GemmEpilogue).  Any four consecutive
+// warps cover the four quarters, so the group w0 + 4k .. w0 + 4k + 3 takes
+// slice k whatever w0 is.  Warps past the last slice have no work.
 template <int BN, int EPI, int NW = 4>
-__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, float* stage, int m0, int n0) {
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, float* stage, int m0, int n0,
+                                              int w0 = 0) {
     constexpr int kSlices = (NW / 4) < (BN / 16) ? (NW / 4) : (BN / 16);
     constexpr int kCols = BN / kSlices;  // a multiple of 16
     static_assert(NW % 4 == 0 && kCols % 16 == 0, "epilogue slices");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q = warp & 3, slice = warp >> 2;
+    const int q = warp & 3, slice = (warp - w0) >> 2;
     if (slice < kSlices) {
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
-        float* stg = stage + warp * 32 * kStageStride;
+        float* stg = stage + (warp - w0) * 32 * kStageStride;
         const int mw = m0 + q * 32;  // this warp's first row
 #pragma unroll 1
         for (int c0 = slice * kCols; c0 < (slice + 1) * kCols; c0 += 16) {
@@ -470,6 +475,179 @@ __global__ void __launch_bounds__(kTmaThreads) k_gemm_bf16_tma(const __grid_cons
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+// Persistent form of the TMA kernel, for GEMMs of more than one wave of
+// tiles: one CTA per SM walks its share of the work units (tile, K slice)
+// with the accumulator double-buffered in tensor memory (2 x BN columns), so
+// the epilogue of unit t runs while the MMAs of unit t + 1 issue.  Warp 0
+// (one thread) streams K tiles through the S-stage ring across units; warp 1
+// (one thread) issues the MMAs into buffer t & 1, after waiting on that
+// buffer's `tempty` barrier (its previous contents read out), and commits the
+// unit's last MMAs to `tfull`; warps 2..9 wait on `tfull`, run the epilogue
+// out of tensor memory through their own staging area (the ring stays in
+// use), and arrive on `tempty` (8 arrivals).  Units run in groups of
+// kPersistGroupM row tiles, column tiles within a group, so the CTAs working
+// at the same time share operand tiles in L2.  Every wait is bounded; a role
+// whose wait gives up records the error and stops, and the others' waits
+// then run out in turn.
+constexpr int kPersistThreads = 10 * 32;
+constexpr int kPersistEpiWarps = 8;  // overlapped with the MMAs, so fewer warps suffice; the ring keeps 4-8 stages
+constexpr int kPersistGroupM = 16;
+
+template <int BN>
+__host__ __device__ constexpr int persist_stages() {
+    return BN >= 256 ? 4 : (BN >= 128 ? 6 : 8);
+}
+
+template <int BN>
+struct PersistSmem {
+    static constexpr int kStages = persist_stages<BN>();
+    alignas(1024) unsigned char a[kStages][kGemmBM * kGemmBK * 2];
+    alignas(1024) unsigned char b[kStages][BN * kGemmBK * 2];
+    alignas(16) float stage[kPersistEpiWarps * 32 * kStageStride];
+    alignas(8) uint64_t full[kStages];
+    alignas(8) uint64_t empty[kStages];
+    alignas(8) uint64_t tfull[2];
+    alignas(8) uint64_t tempty[2];
+    uint32_t tmem;
+};
+
+// Work unit u: K slice z = u / tiles, tile u % tiles in grouped order.
+__device__ __forceinline__ void persist_unit(int u, int n_mt, int n_nt, int& mt, int& nt, int& z) {
+    const int tiles = n_mt * n_nt;
+    z = u / tiles;
+    const int t = u - z * tiles;
+    const int per_group = kPersistGroupM * n_nt;
+    const int grp = t / per_group, r = t - grp * per_group;
+    const int gm = min(kPersistGroupM, n_mt - grp * kPersistGroupM);  // rows in this (last) group
+    mt = grp * kPersistGroupM + r % gm;
+    nt = r / gm;
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kPersistThreads, 1)
+    k_gemm_bf16_tma_persistent(const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
+                               GemmArgs g, int n_units, int n_mt, int n_nt) {
+    static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "BN: a multiple of 16 in [32, 256]");
+    constexpr int S = persist_stages<BN>();
+    constexpr uint32_t kTileBytes = (uint32_t)(kGemmBM + BN) * kGemmBK * 2;
+    constexpr uint32_t kCols = 2 * BN;  // two accumulators
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    PersistSmem<BN>& Sm =
+        *reinterpret_cast<PersistSmem<BN>*>((void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int KT_all = g.K / kGemmBK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&Sm.tmem)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(smem_u32(&Sm.full[s]), 1);
+            mbar_init(smem_u32(&Sm.empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&Sm.tfull[b]), 1);
+            mbar_init(smem_u32(&Sm.tempty[b]), kPersistEpiWarps);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tma_a) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tma_b) : "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = Sm.tmem;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {  // producer: K tiles of every unit through the ring
+            uint32_t it = 0;
+            for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+                int mt, nt, z;
+                persist_unit(u, n_mt, n_nt, mt, nt, z);
+                const int kt0 = z * g.kt_split, KT = min(g.kt_split, KT_all - kt0);
+                for (int kt = 0; kt < KT && ok; ++kt, ++it) {
+                    const uint32_t s = it % S, n = it / S;
+                    if (n >= 1) ok = mbar_wait(smem_u32(&Sm.empty[s]), (n - 1) & 1u);
+                    if (!ok) break;
+                    const uint32_t full = smem_u32(&Sm.full[s]);
+                    mbar_arrive_expect_tx(full, kTileBytes);
+                    tma_load_2d(smem_u32(Sm.a[s]), &tma_a, (kt0 + kt) * kGemmBK, mt * kGemmBM, full);
+                    tma_load_2d(smem_u32(Sm.b[s]), &tma_b, (kt0 + kt) * kGemmBK, nt * BN, full);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            uint32_t it = 0, t = 0;
+            for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x, ++t) {
+                int mt, nt, z;
+                persist_unit(u, n_mt, n_nt, mt, nt, z);
+                const int kt0 = z * g.kt_split, KT = min(g.kt_split, KT_all - kt0);
+                const uint32_t b = t & 1u, j = t >> 1;  // buffer, its use count
+                if (j >= 1) ok = mbar_wait(smem_u32(&Sm.tempty[b]), (j - 1) & 1u);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_addr = tmem + b * (uint32_t)BN;
+                for (int kt = 0; kt < KT; ++kt, ++it) {
+                    const uint32_t s = it % S, n = it / S;
+                    ok = mbar_wait(smem_u32(&Sm.full[s]), n & 1u);
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(Sm.a[s]), sb = smem_u32(Sm.b[s]);
+#pragma unroll
+                    for (int k = 0; k < kGemmBK / 16; ++k) {
+                        const uint64_t da = umma_desc_sw128(sa + k * 32), db = umma_desc_sw128(sb + k * 32);
+                        const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(acc_addr),
+                            "l"(da), "l"(db), "r"(umma_idesc<BN>()), "r"(acc)
+                            : "memory");
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&Sm.empty[s]))
+                                 : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&Sm.tfull[b]))
+                             : "memory");
+            }
+        }
+    } else {  // epilogue warps 2 .. 9
+        uint32_t t = 0;
+        for (int u = blockIdx.x; u < n_units; u += gridDim.x, ++t) {
+            int mt, nt, z;
+            persist_unit(u, n_mt, n_nt, mt, nt, z);
+            const uint32_t b = t & 1u, j = t >> 1;
+            ok = mbar_wait(smem_u32(&Sm.tfull[b]), j & 1u);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            gemm_epilogue<BN, EPI, kPersistEpiWarps>(g, tmem + b * (uint32_t)BN, Sm.stage, mt * kGemmBM, nt * BN,
+                                                     2);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&Sm.tempty[b]))
+                                        : "memory");
+        }
+    }
+    __syncwarp();  // warps 0 and 1 reconverge after their one-thread roles
+    if (!ok) atomicExch(g.err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+template <int BN>
+constexpr size_t gemm_persist_smem_bytes() {
+    return sizeof(PersistSmem<BN>) + 1024;
 }
 
 template <int BN>

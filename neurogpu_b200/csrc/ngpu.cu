@@ -2302,22 +2302,52 @@ static bool gemm_use_tma(const GemmArgs& g, int bn) {
     return g.M >= kGemmBM && g.N >= bn && tensor_map_encoder() != nullptr;
 }
 
+// More than two work units (tiles x K slices) per SM: the persistent
+// kernel, one CTA per SM, unless NGPU_GEMM_PERSISTENT=0.  Measured on B200:
+// 8192^3 0.809 ms against 0.889 one CTA per tile, 4096^3 0.115 against
+// 0.123; at 1.7 tiles per SM (8192 x 512 x 512, 128-wide tiles) the overlap
+// gains less than the one-CTA-per-tile kernel's 16-warp epilogue (0.029
+// against 0.024 ms).
+static bool gemm_use_persistent(int units) {
+    const char* ev = getenv("NGPU_GEMM_PERSISTENT");
+    if (ev && ev[0] == '0') return false;
+    return units > 2 * kSmCount;
+}
+
 template <int BN, int EPI>
 static cudaError_t launch_gemm_bn(GemmArgs g, cudaStream_t st) {
     if (gemm_use_tma(g, BN)) {
         CUtensorMap ta, tb;
         if (gemm_tensor_map(&ta, g.A, g.M, g.K, g.lda, kGemmBM) && gemm_tensor_map(&tb, g.B, g.N, g.K, g.ldb, BN)) {
+            const int n_mt = (g.M + kGemmBM - 1) / kGemmBM, n_nt = (g.N + BN - 1) / BN;
+            int splits = 1;
+            const int per = gemm_k_split(g, BN, EPI, kSmCount, &splits);
+            if (gemm_use_persistent(n_mt * n_nt * splits)) {
+                const size_t smem = gemm_persist_smem_bytes<BN>();
+                cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tma_persistent<BN, EPI>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+                g.kt_split = per;
+                if (EPI == kEpiSplitAdd) {
+                    e = cudaMemsetAsync(g.out_f32, 0, sizeof(float) * ((size_t)(g.M - 1) * g.ldo + g.N), st);
+                    if (e != cudaSuccess) return e;
+                }
+                const int units = n_mt * n_nt * splits;
+                k_gemm_bf16_tma_persistent<BN, EPI><<<std::min(units, kSmCount), kPersistThreads, smem, st>>>(
+                    ta, tb, g, units, n_mt, n_nt);
+                g_launches++;
+                return cudaGetLastError();
+            }
             const size_t smem = gemm_tma_smem_bytes<BN>();
             cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16_tma<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
             if (e != cudaSuccess) return e;
-            int splits = 1;
-            g.kt_split = gemm_k_split(g, BN, EPI, kSmCount, &splits);  // one CTA per SM: one wave
+            g.kt_split = per;  // split-K: one CTA per SM, one wave
             if (EPI == kEpiSplitAdd) {
                 e = cudaMemsetAsync(g.out_f32, 0, sizeof(float) * ((size_t)(g.M - 1) * g.ldo + g.N), st);
                 if (e != cudaSuccess) return e;
             }
-            dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + BN - 1) / BN, splits);
+            dim3 grid(n_mt, n_nt, splits);
             k_gemm_bf16_tma<BN, EPI><<<grid, kTmaThreads, smem, st>>>(ta, tb, g);
             g_launches++;
             return cudaGetLastError();

@@ -108,3 +108,49 @@ def test_gemm_gelu_grad_epilogue(ngpu_built, gemm_path):
     want = d64 * _gelu_grad(zin.astype(np.float64))
     np.testing.assert_allclose(dz, want, rtol=1e-2, atol=1e-2)
     np.testing.assert_array_equal(dzt, dz.T)
+
+
+def _units(M, N, bn):
+    return -(-M // 128) * -(-N // bn)
+
+
+@pytest.mark.parametrize("M,N,K,bn", [(4200, 300, 192, 32), (2560, 1024, 256, 64), (4800, 1000, 128, 128),
+                                      (4400, 2304, 320, 256)])
+def test_persistent_gemm_matches_fp64_and_per_tile_kernel(ngpu_built, monkeypatch, M, N, K, bn):
+    """More than two tiles per SM (ragged edges included): the persistent kernel,
+    whose accumulator is double-buffered in tensor memory, against FP64 and,
+    bit for bit, against the one-CTA-per-tile kernel (same MMAs in the same
+    order per tile)."""
+    assert _units(M, N, bn) > 2 * 148
+    monkeypatch.setenv("NGPU_GEMM_TMA", "1")
+    rng = np.random.default_rng(M + N + K + bn)
+    A = _bf16(rng.normal(size=(M, K)))
+    B = _bf16(rng.normal(size=(N, K)))
+    a64, b64 = A.float().numpy().astype(np.float64), B.float().numpy().astype(np.float64)
+    got, _, _ = _gemm(A, B, 0, bn)
+    bound = 1e-5 * (np.abs(a64) @ np.abs(b64).T) + 1e-30
+    assert np.all(np.abs(got - a64 @ b64.T) <= bound)
+    monkeypatch.setenv("NGPU_GEMM_PERSISTENT", "0")
+    per_tile, _, _ = _gemm(A, B, 0, bn)
+    np.testing.assert_array_equal(got, per_tile)
+
+
+@pytest.mark.parametrize("epi,M,N,K,bn", [(1, 7700, 640, 128, 128), (3, 9500, 256, 64, 64), (2, 19000, 512, 64, 256)])
+def test_persistent_gemm_epilogues_match_per_tile_kernel(ngpu_built, monkeypatch, epi, M, N, K, bn):
+    """The fused epilogues (bias + GELU with its transposed copy, GELU'
+    gradient, bias) out of the persistent kernel's two accumulators: equal,
+    bit for bit, to the one-CTA-per-tile kernel's."""
+    assert _units(M, N, bn) > 2 * 148
+    monkeypatch.setenv("NGPU_GEMM_TMA", "1")
+    rng = np.random.default_rng(epi * 1000 + M)
+    A, B = _bf16(rng.normal(size=(M, K))), _bf16(rng.normal(size=(N, K)) * 0.2)
+    bias = rng.normal(size=N).astype(np.float32) if epi in (1, 2) else None
+    zin = rng.normal(size=(M, N)).astype(np.float32) if epi == 3 else None
+    got = _gemm(A, B, epi, bn, bias=bias, zin=zin)
+    monkeypatch.setenv("NGPU_GEMM_PERSISTENT", "0")
+    ref = _gemm(A, B, epi, bn, bias=bias, zin=zin)
+    for g_, r_ in zip(got, ref):
+        np.testing.assert_array_equal(g_, r_)
+    if epi == 2:
+        z64 = A.float().numpy().astype(np.float64) @ B.float().numpy().astype(np.float64).T + bias
+        np.testing.assert_allclose(got[0], z64, rtol=1e-4, atol=1e-4)
