@@ -18,6 +18,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -410,6 +411,10 @@ struct ngpu_sim {
     size_t trace_bytes = 0;
     float* d_tmp_out = nullptr;
     size_t tmp_out_bytes = 0;
+    float* d_params_in = nullptr;  // the caller's [set][param][section] table, uploaded
+    size_t params_in_bytes = 0;
+    void* h_stage = nullptr;       // pinned host staging for host-buffer copies
+    size_t stage_bytes = 0;
     // stimulus / recording (internal node numbering)
     int nt = 0, stim_node = 0;
     double stim_scale = 0.0;
@@ -919,10 +924,53 @@ static void sim_free(ngpu_sim* s) {
     void* ptrs[] = {s->d_nodes, s->d_vbuf, s->d_slab, s->d_ptab, s->d_scr, s->d_jacc, s->d_jx,
                     s->d_inst_stim, s->d_bad, s->d_row_param, s->d_row_sec, s->d_amps,
                     s->d_dts, s->d_trace, s->d_tmp_out, s->d_comps, s->d_seps, s->d_sepv, s->d_prange,
-                    s->d_phash};
+                    s->d_phash, s->d_params_in};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (s->h_stage) cudaFreeHost(s->h_stage);
     delete s;
+}
+
+// Host-buffer copies.  A copy between pageable host memory and the device
+// runs at a few GB/s: the driver stages it through its own pinned buffer,
+// one page at a time on one thread, and a fresh destination (a new numpy
+// array) also takes its first-touch page faults on that thread.  The
+// simulation's own pinned staging buffer (grown to the largest copy, kept
+// for the next call) moves at full link speed, and the host side of the copy
+// (pageable <-> pinned) is split over several threads.  Measured on B200 for
+// the 98 MB trace of the TTPC-like batch: 25 ms through the driver's path.
+static void* sim_stage(ngpu_sim* s, size_t bytes) {
+    if (s->stage_bytes >= bytes) return s->h_stage;
+    if (s->h_stage) cudaFreeHost(s->h_stage);
+    s->h_stage = nullptr;
+    s->stage_bytes = 0;
+    if (cudaHostAlloc(&s->h_stage, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();  // no pinned memory: the caller takes the driver's path
+        s->h_stage = nullptr;
+        return nullptr;
+    }
+    s->stage_bytes = bytes;
+    return s->h_stage;
+}
+
+static void host_copy_parallel(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kPerThreadMin = size_t(4) << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t want = std::min<size_t>(std::min<size_t>(16, std::max(1u, hw / 2)), bytes / kPerThreadMin);
+    const size_t T = std::max<size_t>(1, want);
+    if (T == 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes / T + 4095) / 4096 * 4096;
+    std::vector<std::thread> th;
+    th.reserve(T - 1);
+    for (size_t k = 1; k < T; ++k) {
+        const size_t lo = std::min(bytes, k * part), hi = std::min(bytes, lo + part);
+        if (hi > lo) th.emplace_back([=] { std::memcpy((char*)dst + lo, (const char*)src + lo, hi - lo); });
+    }
+    std::memcpy(dst, src, std::min(bytes, part));
+    for (auto& t : th) t.join();
 }
 
 // The device side of the simulation's tree split (s->part): junction
@@ -1242,17 +1290,28 @@ int ngpu_sim_set_params(ngpu_sim* s, const float* params, int32_t on_device) {
     const ngpu_model* m = s->m;
     const size_t n = (size_t)s->n_sets * m->n_params * m->n_sections;
     const float* src = params;
-    float* tmp = nullptr;
     if (!on_device) {
-        int rc = NGPU_OK;
-        tmp = (float*)dmalloc(n * sizeof(float), &rc);
-        if (!tmp) return rc;
-        cudaError_t e = cudaMemcpy(tmp, params, n * sizeof(float), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            cudaFree(tmp);
-            return fail(NGPU_E_CUDA, std::string("params upload: ") + cudaGetErrorString(e));
+        // the upload buffer stays with the simulation for the next call
+        const size_t bytes = n * sizeof(float);
+        if (s->params_in_bytes < bytes) {
+            if (s->d_params_in) cudaFree(s->d_params_in);
+            s->d_params_in = nullptr;
+            s->params_in_bytes = 0;
+            int rc = NGPU_OK;
+            s->d_params_in = (float*)dmalloc(bytes, &rc);
+            if (!s->d_params_in) return rc;
+            s->params_in_bytes = bytes;
         }
-        src = tmp;
+        cudaError_t e;
+        if (void* stg = sim_stage(s, bytes)) {
+            host_copy_parallel(stg, params, bytes);
+            e = cudaMemcpyAsync(s->d_params_in, stg, bytes, cudaMemcpyHostToDevice, 0);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(0);  // the staging buffer is free again
+        } else {
+            e = cudaMemcpy(s->d_params_in, params, bytes, cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("params upload: ") + cudaGetErrorString(e));
+        src = s->d_params_in;
     }
     const size_t total = (size_t)s->n_groups * m->ptab_rows * kLanes;
     int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
@@ -1260,11 +1319,6 @@ int ngpu_sim_set_params(ngpu_sim* s, const float* params, int32_t on_device) {
                                      m->n_sections, s->n_stim, s->n_inst, s->n_groups, s->d_ptab);
     g_launches++;
     cudaError_t e = cudaGetLastError();
-    if (tmp) {
-        cudaError_t e2 = cudaDeviceSynchronize();
-        cudaFree(tmp);
-        if (e == cudaSuccess) e = e2;
-    }
     if (e != cudaSuccess) return fail(NGPU_E_CUDA, std::string("param gather: ") + cudaGetErrorString(e));
     s->has_params = true;
     return sim_find_folds(s);
@@ -1947,17 +2001,22 @@ int ngpu_sim_get_trace(ngpu_sim* s, float* out, int32_t on_device, void* cuda_st
     cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     bool identity = (n_rec == nr);
     for (int r = 0; r < n_rec && identity; ++r) identity = s->rec_cols[r] == r;
+    // a host destination is written through the pinned staging buffer
+    const size_t bytes_out = sizeof(float) * (size_t)n_rec * ns * s->n_inst;
+    float* stg = on_device ? nullptr : (float*)sim_stage(s, bytes_out);
+    float* dst = stg ? stg : out;
     if (identity) {
-        NGPU_CUDA(cudaMemcpyAsync(out, s->d_tmp_out, bytes_u, kind, st));
+        NGPU_CUDA(cudaMemcpyAsync(dst, s->d_tmp_out, bytes_u, kind, st));
     } else {
         // duplicated sites: strided copies of each requested column
         for (int r = 0; r < n_rec; ++r) {
-            NGPU_CUDA(cudaMemcpy2DAsync(out + (size_t)r * ns, sizeof(float) * n_rec * ns,
+            NGPU_CUDA(cudaMemcpy2DAsync(dst + (size_t)r * ns, sizeof(float) * n_rec * ns,
                                         s->d_tmp_out + (size_t)s->rec_cols[r] * ns, sizeof(float) * per_inst_u,
                                         sizeof(float) * ns, s->n_inst, kind, st));
         }
     }
     NGPU_CUDA(cudaStreamSynchronize(st));
+    if (stg) host_copy_parallel(out, stg, bytes_out);
     return NGPU_OK;
 }
 
@@ -1997,6 +2056,10 @@ int ngpu_run(ngpu_model* m, int32_t n_sets, const float* params, int32_t n_stim,
         if (rc) return rc;
     }
     if (lock.owns_lock()) m->run_cache = nullptr;  // taken; kept again below on success
+    // one pinned staging buffer for both host copies (parameters in, trace out;
+    // pinning takes ~3 ms per MB, so it is sized once for the larger)
+    sim_stage(s, std::max(sizeof(float) * (size_t)n_sets * m->n_params * m->n_sections,
+                          sizeof(float) * (size_t)n_sets * n_stim * std::max(0, n_rec) * std::max(0, nt)));
     if ((rc = ngpu_sim_set_params(s, params, 0)) ||
         (rc = ngpu_sim_set_stimulus(s, nt, amps, dts, stim_node, stim_area_um2, 0)) ||
         (rc = ngpu_sim_set_recording(s, n_rec, rec_nodes, 1)) || (rc = ngpu_sim_init(s, v_init, nullptr)) ||
