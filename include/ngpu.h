@@ -145,8 +145,11 @@ int ngpu_model_split_info(const ngpu_model *m, int32_t n_warps, int32_t *perm, i
 /* ngpu_run keeps its simulation's device buffers with the model and reuses
  * them when the next call has the same n_sets, n_stim and precision (a call
  * with another shape replaces them; ngpu_model_destroy releases them), so
- * repeated calls allocate and release no device memory.  Concurrent calls on
- * one model are safe: a call that finds the buffers in use runs on its own. */
+ * repeated calls allocate and release no device memory.  With them it keeps a
+ * pinned host staging buffer, sized for the larger of the parameter table and
+ * the trace, through which both host copies run (the host side split over
+ * threads).  Concurrent calls on one model are safe: a call that finds the
+ * buffers in use runs on its own. */
 int ngpu_run(ngpu_model *m, int32_t n_sets, const float *params, int32_t n_stim, int32_t nt,
              const float *amps, const float *dts, int32_t stim_node, float stim_area_um2,
              int32_t n_rec, const int32_t *rec_nodes, float v_init, int32_t precision,
