@@ -70,14 +70,21 @@ struct GemmArgs {
     int kt_split;            // 64-wide K tiles per CTA; CTA z takes tiles [z kt_split, (z+1) kt_split)
 };
 
+// The tensor-core unit's tanh (tanh.approx.f32, one instruction; relative
+// error ~5e-4, below the bf16 rounding of the outputs it feeds).
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float gelu_tanh(float z) {
     const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-    return 0.5f * z * (1.0f + tanhf(u));
+    return 0.5f * z * (1.0f + tanh_fast(u));
 }
 __device__ __forceinline__ float gelu_tanh_grad(float z) {
     const float z2 = z * z;
     const float u = 0.7978845608028654f * (z + 0.044715f * z2 * z);
-    const float t = tanhf(u);
+    const float t = tanh_fast(u);
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z2);
 }
 
@@ -155,6 +162,65 @@ struct GemmSmem {
 constexpr int kStageStride = 17;
 static_assert(kGemmBM * kGemmBK * 2 >= 4 * 32 * kStageStride * 4, "staging fits in the first A stage");
 
+// One output element of the epilogue: accumulator value *sp of row m,
+// column n (o = m * ldo + n); the bf16 epilogues leave their rounded value in
+// *sp for the transposed copy.
+template <int EPI>
+__device__ __forceinline__ void epi_one(const GemmArgs& g, float* sp, size_t o, int n) {
+    const float d = *sp;
+    if constexpr (EPI == kEpiStore) {
+        g.out_f32[o] = d;
+    } else if constexpr (EPI == kEpiBias) {
+        g.out_f32[o] = d + g.bias[n];
+    } else if constexpr (EPI == kEpiSplitAdd) {
+        atomicAdd(g.out_f32 + o, d);
+    } else if constexpr (EPI == kEpiBiasGelu) {
+        const float z = d + g.bias[n];
+        const __nv_bfloat16 h = __float2bfloat16_rn(gelu_tanh(z));
+        g.out_f32[o] = z;
+        g.out_bf16[o] = h;
+        *sp = __bfloat162float(h);
+    } else {  // kEpiGeluGrad
+        const __nv_bfloat16 h = __float2bfloat16_rn(d * gelu_tanh_grad(g.zin[o]));
+        g.out_bf16[o] = h;
+        *sp = __bfloat162float(h);
+    }
+}
+
+// Four consecutive elements (n a multiple of 4, all four inside N) with
+// 16-byte f32 and 8-byte bf16 accesses; the caller checked the alignment.
+template <int EPI>
+__device__ __forceinline__ void epi_vec4(const GemmArgs& g, float* sp, size_t o, int n) {
+    static_assert(EPI != kEpiSplitAdd, "split-K atomics go one element per lane");
+    float d[4] = {sp[0], sp[1], sp[2], sp[3]};
+    if constexpr (EPI == kEpiStore || EPI == kEpiBias) {
+        if constexpr (EPI == kEpiBias) {
+            const float4 b = *reinterpret_cast<const float4*>(g.bias + n);
+            d[0] += b.x, d[1] += b.y, d[2] += b.z, d[3] += b.w;
+        }
+        *reinterpret_cast<float4*>(g.out_f32 + o) = make_float4(d[0], d[1], d[2], d[3]);
+    } else {
+        float v[4];
+        if constexpr (EPI == kEpiBiasGelu) {
+            const float4 b = *reinterpret_cast<const float4*>(g.bias + n);
+            const float z[4] = {d[0] + b.x, d[1] + b.y, d[2] + b.z, d[3] + b.w};
+            *reinterpret_cast<float4*>(g.out_f32 + o) = make_float4(z[0], z[1], z[2], z[3]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[q] = gelu_tanh(z[q]);
+        } else {  // kEpiGeluGrad
+            const float4 z = *reinterpret_cast<const float4*>(g.zin + o);
+            v[0] = d[0] * gelu_tanh_grad(z.x), v[1] = d[1] * gelu_tanh_grad(z.y);
+            v[2] = d[2] * gelu_tanh_grad(z.z), v[3] = d[3] * gelu_tanh_grad(z.w);
+        }
+        const __nv_bfloat162 lo = __floats2bfloat162_rn(v[0], v[1]), hi = __floats2bfloat162_rn(v[2], v[3]);
+        uint2 pk;
+        pk.x = *reinterpret_cast<const uint32_t*>(&lo);
+        pk.y = *reinterpret_cast<const uint32_t*>(&hi);
+        *reinterpret_cast<uint2*>(g.out_bf16 + o) = pk;
+        sp[0] = __low2float(lo), sp[1] = __high2float(lo), sp[2] = __low2float(hi), sp[3] = __high2float(hi);
+    }
+}
+
 // Epilogue of a 128 x BN tile whose accumulator is in tensor memory at
 // `tmem`, by NW warps, the CTA's warps w0 .. w0 + NW - 1: warp w reads the 32
 // lanes (rows) of quarter w % 4 (the lanes tcgen05.ld lets it reach) over
@@ -171,6 +237,9 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
     static_assert(NW % 4 == 0 && kCols % 16 == 0, "epilogue slices");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = warp & 3, slice = (warp - w0) >> 2;
+    // 4-wide accesses need rows that start on 16 bytes (f32) and 8 bytes (bf16)
+    const uintptr_t al16 = (uintptr_t)g.out_f32 | (uintptr_t)g.bias | (uintptr_t)g.zin;
+    const bool vec = g.ldo % 4 == 0 && (al16 & 15) == 0 && ((uintptr_t)g.out_bf16 & 7) == 0;
     if (slice < kSlices) {
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         float* stg = stage + (warp - w0) * 32 * kStageStride;
@@ -188,31 +257,33 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, 
 #pragma unroll
             for (int j = 0; j < 16; ++j) stg[lane * kStageStride + j] = __uint_as_float(r[j]);
             __syncwarp();
-            // coalesced pass: element e = j * 32 + lane is row e / 16, column e % 16
+            if constexpr (EPI == kEpiSplitAdd) {
+                // atomics one element per lane: element e = j * 32 + lane is row e / 16,
+                // column e % 16 (a warp's atomics cover 2 rows of 16 columns)
 #pragma unroll 4
-            for (int j = 0; j < 16; ++j) {
-                const int e = j * 32 + lane, row = e >> 4, col = e & 15;
-                const int m = mw + row, n = n0 + c0 + col;
-                float* sp = stg + row * kStageStride + col;
-                if (m < g.M && n < g.N) {
-                    const size_t o = (size_t)m * g.ldo + n;
-                    const float d = *sp;
-                    if constexpr (EPI == kEpiStore) {
-                        g.out_f32[o] = d;
-                    } else if constexpr (EPI == kEpiBias) {
-                        g.out_f32[o] = d + g.bias[n];
-                    } else if constexpr (EPI == kEpiSplitAdd) {
-                        atomicAdd(g.out_f32 + o, d);
-                    } else if constexpr (EPI == kEpiBiasGelu) {
-                        const float z = d + g.bias[n];
-                        const __nv_bfloat16 h = __float2bfloat16_rn(gelu_tanh(z));
-                        g.out_f32[o] = z;
-                        g.out_bf16[o] = h;
-                        *sp = __bfloat162float(h);
-                    } else {  // kEpiGeluGrad
-                        const __nv_bfloat16 h = __float2bfloat16_rn(d * gelu_tanh_grad(g.zin[o]));
-                        g.out_bf16[o] = h;
-                        *sp = __bfloat162float(h);
+                for (int j = 0; j < 16; ++j) {
+                    const int e = j * 32 + lane, row = e >> 4, col = e & 15;
+                    const int m = mw + row, n = n0 + c0 + col;
+                    if (m < g.M && n < g.N)
+                        epi_one<EPI>(g, stg + row * kStageStride + col, (size_t)m * g.ldo + n, n);
+                }
+            } else {
+                // coalesced pass: group e = j * 32 + lane is row e / 4, columns 4 (e % 4) .. + 3
+                // (a warp store covers 8 rows of 16 columns)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int e = j * 32 + lane, row = e >> 2, cg = (e & 3) * 4;
+                    const int m = mw + row, n = n0 + c0 + cg;
+                    float* sp = stg + row * kStageStride + cg;
+                    if (m < g.M && n < g.N) {
+                        const size_t o = (size_t)m * g.ldo + n;
+                        if (vec && n + 4 <= g.N) {
+                            epi_vec4<EPI>(g, sp, o, n);
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 4; ++k)
+                                if (n + k < g.N) epi_one<EPI>(g, sp + k, o + k, n + k);
+                        }
                     }
                 }
             }
