@@ -347,8 +347,11 @@ int64_t ngpu_launch_count(int32_t reset);
  *   larger than M and N, as in the network's weight gradients: the output
  *   is zeroed on the stream, the slices add their partial sums with
  *   atomics, so the summation order varies from run to run within fp32
- *   rounding).  bn: the N tile (32, 64, 128, 256).  A wait that
- *   exceeds its bound sets a device flag read (and cleared) by
+ *   rounding).  bn: the N tile (32, 64, 128, 256).  GELU's tanh is the
+ *   hardware approximation (relative error ~5e-4, below the bf16 outputs'
+ *   rounding).  More than two tiles per SM run on the persistent kernel
+ *   (one CTA per SM, results bit for bit those of one CTA per tile).  A
+ *   wait that exceeds its bound sets a device flag read (and cleared) by
  *   ngpu_gemm_error.  No counterpart in the reference.
  */
 int ngpu_gemm_bf16_tn(const void *A, const void *B, int32_t M, int32_t N, int32_t K, int32_t lda, int32_t ldb,
