@@ -71,7 +71,7 @@ def parse_args():
     ap.add_argument("--ga-epochs", type=int, default=30)
     ap.add_argument("--model", default="ttpc_like", choices=sorted(MODELS),
                     help="the cell of the default workload: the TTPC-like headline, or the HH-type cell")
-    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga", "ga_ops", "gemm"],
+    ap.add_argument("--workload", default="ttpc_like", choices=["ttpc_like", "uneven_batch", "ga", "ga_ops", "gemm", "explore"],
                     help="uneven_batch: 8192 sets over 200/800/1500/3000-compartment trees x 5 protocols, "
                          "one launch per chunk, the run captured as a CUDA graph (auxiliary line)")
     return ap.parse_args()
@@ -355,6 +355,126 @@ def run_uneven(args):
     batch.close()
 
 
+EXPLORE_BASELINE = 3.83e8  # compartment-steps/s of the reference's exploration run (RunTimes.csv)
+
+
+def run_explore(args):
+    """Exploration line: the reference's parameter-exploration run
+    (GUI/run_neuroGPU.py, GUI/plot_param_explor.py) on its own shipped model,
+    the 512-compartment BBP TTPC cell of GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/
+    Data (tests/golden/ttpc512): the 100 x 100 grid over GA parameters 0 and 2
+    of its opt_table.csv (10,000 sets), 3168 steps of 0.1 ms under
+    Stim_raw0.csv, and every trace's dV/dt peak-count score, computed where
+    the trace lies.  One bench step = init + every step of the run + the
+    score, parameters resident (device-timed).  e2e: explore.explore() from
+    the host grid to the host score map (AllParams rows built and uploaded,
+    scores read back).  vs_baseline: the reference's RunTimes.csv for this
+    run, 10,000 sets in 42,307.5 ms (init + H2D + kernel + D2H on its GPU)
+    = 3.83e8 compartment-steps/s."""
+    import torch
+    from neurogpu_b200 import _ffi, evaluator, explore, formats
+    rank, world, local = dist_setup(args.gpus)
+    from neurogpu_b200.mechsets import TTPC
+    d = ROOT / "tests" / "golden" / "ttpc512"
+    m = formats.read_data_dir(d, stim_index=0, params_file="AllParams_reference.csv")
+    # the shipped AllParams_for_params.csv marks GA parameters at entries that do
+    # not match opt_table.csv's names; parameter 0 is g_pas in every section and
+    # parameter 2 the soma's gNaTs2_t here
+    tmpl, _, _ = evaluator.load_mapping(d)
+    nc = m.cell.n_sections
+    nats = tmpl.reshape(-1, nc)[TTPC.param_index("gNaTs2_tbar_NaTs2_t")]
+    mapping = explore.mapping_for(tmpl, nc, {0: (TTPC.param_index("g_pas"), None),
+                                             2: (TTPC.param_index("gNaTs2_tbar_NaTs2_t"),
+                                                 np.nonzero(nats == nats.max())[0])})
+    _, _, _, base = explore.read_opt_table(d / "opt_table.csv")
+    grid = explore.gen_params(base)
+    sim, score_dt = explore.grid_simulation(m, mapping, grid)
+    nt = int(m.amps.shape[1])
+    chunk = min(args.chunk, nt)
+
+    def one_run():
+        sim.init(m.v_init)
+        for t0 in range(0, nt, chunk):
+            sim.advance(t0, min(chunk, nt - t0))
+        return sim.dvdt_peaks(score_dt)
+
+    for _ in range(args.warmup):
+        one_run()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    _ffi.lib().ngpu_launch_count(1)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        counts = one_run()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(_ffi.lib().ngpu_launch_count(0))
+    clk = clocks.stop() if clocks else None
+    cs_step = len(grid) * m.cell.n_nodes * nt
+    rate, el_s = weak_scaling_rate(cs_step * args.steps, ev0.elapsed_time(ev1) / 1e3, world)
+    bad = sim.n_bad()
+    c = counts.cpu().numpy()
+    # the score kernel alone (the run's trace buffer in place): 4 bytes read per
+    # sample, 4 written per trace
+    for _ in range(3):
+        sim.dvdt_peaks(score_dt)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record(stream)
+    for _ in range(reps):
+        sim.dvdt_peaks(score_dt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    score_ms = e0.elapsed_time(e1) / reps
+    score_bytes = len(grid) * (sim.n_samples + 1) * 4
+    peak, peak_kind = hbm_peak()
+    # end to end through the public call, host grid -> host score map
+    e2e_s = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scores, _ = explore.explore(m, mapping, base)
+        torch.cuda.synchronize()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_best = min(e2e_s)
+    h2d = len(grid) * m.cell.n_params() * m.cell.n_sections * 4 + nt * 8
+    if rank == 0:
+        print(json.dumps({
+            "metric": "compartment-steps/s (reference exploration run, TTPC 512 x 10000)", "value": rate,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": rate / EXPLORE_BASELINE, "dtype": "f32",
+            "data": "the reference's shipped model and stimulus, its exploration grid",
+            "config": {"workload": "explore", "model": "tests/golden/ttpc512 (BBP TTPC, 512 compartments)",
+                       "n_sets": len(grid), "grid": "the reference's gen_params: GA parameter 0 (g_pas, every "
+                       "section) over linspace(0, 10, 100) x parameter 2 (somatic gNaTs2_t) over "
+                       "linspace(0, 20, 100)", "timesteps_per_step": nt,
+                       "dt_ms": float(m.dts[0]), "launch_chunk": chunk,
+                       "score": "scipy.signal.find_peaks(diff(v)/0.1, 15, distance=5) count per trace, on the GPU",
+                       "l2": "state larger than L2 (no flush)"},
+            "baseline": {"value": EXPLORE_BASELINE, "source": "GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/Data/"
+                         "RunTimes.csv: 10000 sets, 42307.5 ms, the reference's GPU (not recorded)"},
+            "e2e": {"value": cs_step / e2e_best, "unit": UNIT, "seconds": e2e_best, "seconds_each": e2e_s,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": len(grid) * 4,
+                    "vs_baseline": cs_step / e2e_best / EXPLORE_BASELINE,
+                    "includes": "grid and AllParams rows on the host, simulator creation, parameter upload, "
+                                "init, run, score, score map to the host"},
+            "score_kernel": {"ms": score_ms, "algorithmic_bytes": score_bytes,
+                             "achieved_gbs": score_bytes / score_ms / 1e6, "peak_gbs": peak,
+                             "frac": score_bytes / score_ms / 1e6 / peak, "peak_source": peak_kind,
+                             "note": "k_dvdt_peaks over the run's trace buffer in place; traces in L2 "
+                                     "after the first pass (127 MB, about L2's size)"},
+            "scores": {"spiking_sets": int((c > 0).sum()), "max_count": int(c.max()),
+                       "map_equals_e2e_call": bool(np.array_equal(scores.reshape(-1), c[:, 0]))},
+            "gpu_launches": launches, "clocks": clk, "non_finite_instances": bad}))
+
+
 def run_ga(args):
     """Config-5 line: GA time-to-score, surrogate-screened vs plain, on one
     GPU.  The cell: the 500-node HH-type cell, 12 free parameters (8
@@ -604,6 +724,8 @@ def main():
         return run_uneven(args)
     if args.workload == "gemm":
         return run_gemm(args)
+    if args.workload == "explore":
+        return run_explore(args)
     import torch
     from neurogpu_b200 import _ffi
     from neurogpu_b200.sim import Model, Simulator, run

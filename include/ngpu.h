@@ -262,6 +262,29 @@ int ngpu_sim_features(ngpu_sim *s, int32_t site, double dt, double stim_on, doub
                       float *out_dev, void *cuda_stream);
 
 /*
+ * Parameter-exploration score per trace: the number of peaks that
+ * scipy.signal.find_peaks(dvdt, height=height, distance=distance) finds in
+ * dvdt = diff(v) / dt (dt: the sample spacing, ms), computed on the GPU.
+ * Replaces the host scoring of the reference's exploration run
+ * (GUI/plot_param_explor.py:77-107: find_peaks(dvdt, 15, distance=5) on each
+ * of the 10,000 traces of GUI/run_neuroGPU.py's grid, read back from
+ * VHotP0.dat).  Equal-height peaks closer than `distance` keep the later one.
+ *   ngpu_trace_dvdt_peaks  traces at v_dev[t * stride_trace + s * stride_sample]
+ *                          (device memory); out_dev [n_traces] int32
+ *   ngpu_sim_dvdt_peaks    a simulation's own trace buffer, recording site
+ *                          `site`: out_dev [n_sets][n_stim]
+ *   scratch_dev: device memory of at least ngpu_dvdt_peaks_scratch_bytes
+ *   bytes (the candidate peaks of every trace), owned by the caller.
+ *   Errors: dt <= 0, distance < 1, a NaN height, too small a scratch.
+ */
+int64_t ngpu_dvdt_peaks_scratch_bytes(int32_t n_traces, int32_t n_samples);
+int ngpu_trace_dvdt_peaks(const float *v_dev, int64_t stride_trace, int64_t stride_sample, int32_t n_traces,
+                          int32_t n_samples, double dt, double height, int32_t distance, void *scratch_dev,
+                          int64_t scratch_bytes, int32_t *out_dev, void *cuda_stream);
+int ngpu_sim_dvdt_peaks(ngpu_sim *s, int32_t site, double dt, double height, int32_t distance, void *scratch_dev,
+                        int64_t scratch_bytes, int32_t *out_dev, void *cuda_stream);
+
+/*
  * Runtime specialisation of the advance kernel.  At initialisation a
  * simulation (or, at creation, a batch), FP32 or FP64, gets a kernel compiled
  * with NVRTC for its model's mechanism masks (up to 16): nodes with those masks

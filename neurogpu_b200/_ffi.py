@@ -82,6 +82,9 @@ def lib() -> C.CDLL:
             "ngpu_sim_param_rows": (C.c_int, [P, P, P]),
             "ngpu_trace_features": (C.c_int, [P, I64, I64, I32, I32, C.c_double, C.c_double, C.c_double, F32, P, P]),
             "ngpu_sim_features": (C.c_int, [P, I32, C.c_double, C.c_double, C.c_double, F32, P, P]),
+            "ngpu_dvdt_peaks_scratch_bytes": (I64, [I32, I32]),
+            "ngpu_trace_dvdt_peaks": (C.c_int, [P, I64, I64, I32, I32, D, D, I32, P, I64, P, P]),
+            "ngpu_sim_dvdt_peaks": (C.c_int, [P, I32, D, D, I32, P, I64, P, P]),
             "ngpu_jit_build": (C.c_int, [I32, I32, P, I32, I32, I32, P]),
             "ngpu_mechset_define": (C.c_int, [C.c_char_p, C.c_char_p, I32, P, P, P, I32, P, P]),
             "ngpu_jit_log": (C.c_char_p, []),

@@ -24,6 +24,7 @@
 
 #include "../../include/ngpu.h"
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
+#include "explore.cuh"
 #include "features.cuh"
 #include "ga.cuh"
 #include "gemm_tc.cuh"
@@ -1914,6 +1915,69 @@ int ngpu_sim_features(ngpu_sim* s, int32_t site, double dt, double stim_on, doub
     a.threshold = threshold;
     a.out = out_dev;
     return launch_features(a, (cudaStream_t)cuda_stream);
+}
+
+// ------------------------------------------------------------------ exploration score
+
+int64_t ngpu_dvdt_peaks_scratch_bytes(int32_t n_traces, int32_t n_samples) {
+    if (n_traces < 0 || n_samples < 0) return 0;
+    return (int64_t)peak_scratch_cap(n_samples) * n_traces * (int64_t)sizeof(int32_t);
+}
+
+static int launch_dvdt_peaks(PeakArgs a, int64_t scratch_bytes, cudaStream_t st) {
+    if (!(a.dt > 0) || !std::isfinite(a.dt) || std::isnan(a.height))
+        return fail(NGPU_E_INVALID, "dvdt peaks: need dt > 0 (finite) and a height that is not NaN");
+    if (a.distance < 1) return fail(NGPU_E_INVALID, "dvdt peaks: distance must be >= 1 sample");
+    if (a.n_samples < 0 || a.n_samples >= (1 << 29) || a.n_traces < 0)
+        return fail(NGPU_E_INVALID, "dvdt peaks: sample count out of range (< 2^29)");
+    if (a.n_traces == 0) return NGPU_OK;
+    a.cap = peak_scratch_cap(a.n_samples);
+    const int64_t need = ngpu_dvdt_peaks_scratch_bytes(a.n_traces, a.n_samples);
+    if (scratch_bytes < need)
+        return fail(NGPU_E_INVALID, "dvdt peaks: scratch holds " + std::to_string(scratch_bytes) + " bytes, needs " +
+                                        std::to_string(need));
+    if (!a.v || !a.out || !a.pos) return fail(NGPU_E_INVALID, "dvdt peaks: null pointer");
+    k_dvdt_peaks<<<(a.n_traces + 127) / 128, 128, 0, st>>>(a);
+    g_launches++;
+    NGPU_CUDA(cudaGetLastError());
+    return NGPU_OK;
+}
+
+int ngpu_trace_dvdt_peaks(const float* v_dev, int64_t stride_trace, int64_t stride_sample, int32_t n_traces,
+                          int32_t n_samples, double dt, double height, int32_t distance, void* scratch_dev,
+                          int64_t scratch_bytes, int32_t* out_dev, void* cuda_stream) {
+    if (stride_trace < 0 || stride_sample < 1) return fail(NGPU_E_INVALID, "dvdt peaks: bad strides");
+    PeakArgs a;
+    a.v = v_dev;
+    a.stride_trace = stride_trace;
+    a.stride_sample = stride_sample;
+    a.n_traces = n_traces;
+    a.n_samples = n_samples;
+    a.dt = dt;
+    a.height = height;
+    a.distance = distance;
+    a.pos = (int32_t*)scratch_dev;
+    a.out = out_dev;
+    return launch_dvdt_peaks(a, scratch_bytes, (cudaStream_t)cuda_stream);
+}
+
+int ngpu_sim_dvdt_peaks(ngpu_sim* s, int32_t site, double dt, double height, int32_t distance, void* scratch_dev,
+                        int64_t scratch_bytes, int32_t* out_dev, void* cuda_stream) {
+    if (!s) return fail(NGPU_E_INVALID, "null simulation");
+    if (!s->initialized || !s->d_trace) return fail(NGPU_E_STATE, "run the simulation first");
+    if (site < 0 || site >= (int)s->rec_cols.size()) return fail(NGPU_E_INVALID, "recording site out of range");
+    PeakArgs a;
+    a.v = s->d_trace + (size_t)s->rec_cols[site] * s->n_pad;  // [sample][column][instance]
+    a.stride_trace = 1;
+    a.stride_sample = (int64_t)s->n_rec_unique * s->n_pad;
+    a.n_traces = s->n_inst;
+    a.n_samples = s->n_samples;
+    a.dt = dt;
+    a.height = height;
+    a.distance = distance;
+    a.pos = (int32_t*)scratch_dev;
+    a.out = out_dev;
+    return launch_dvdt_peaks(a, scratch_bytes, (cudaStream_t)cuda_stream);
 }
 
 int ngpu_sim_param_rows(const ngpu_sim* s, int32_t* rows_read, int32_t* rows_total) {

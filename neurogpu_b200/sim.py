@@ -203,6 +203,23 @@ class Simulator:
             C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
         return out
 
+    def dvdt_peaks(self, dt: float, site: int = 0, height: float = 15.0, distance: int = 5, stream=None):
+        """Exploration score of every instance's trace at recording site
+        `site`, computed where the trace lies (ngpu_sim_dvdt_peaks): the
+        number of peaks scipy.signal.find_peaks(diff(v) / dt, height,
+        distance) finds; an int32 CUDA tensor [n_sets, n_stim].  dt: the
+        sample spacing (step dt x rec_every)."""
+        import torch
+        L = _ffi.lib()
+        need = int(L.ngpu_dvdt_peaks_scratch_bytes(self.n_sets * self.n_stim, self.n_samples))
+        scratch = torch.empty(max(need, 4), dtype=torch.uint8, device="cuda")
+        out = torch.empty((self.n_sets, self.n_stim), dtype=torch.int32, device="cuda")
+        _ffi.check("ngpu_sim_dvdt_peaks", L.ngpu_sim_dvdt_peaks(
+            self._h, int(site), float(dt), float(height), int(distance), C.c_void_p(scratch.data_ptr()),
+            scratch.numel(), C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        self._keep_scratch = scratch  # until the stream has used it
+        return out
+
     def layout(self) -> dict:
         """{"layout": "lane" | "warp", "cta_warps": .., "items": ..} with the
         library's choices filled in (ngpu_sim_layout)."""

@@ -6,7 +6,7 @@ results).
 1. Copies the input files of three reference models (data, not code):
      ttpc512/   GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/Data/{BasicConstSegP.csv,
                 Sim.csv, Stim_meta.csv, Stim_raw0.csv, times.csv,
-                AllParams_reference.csv}
+                AllParams_reference.csv, AllParams_for_params.csv, opt_table.csv}
      mainen384/ Figures/FigureS4_mainen/Data/{BasicConstSegP.csv, ParamsM.csv,
                 Sim.csv, Stim_meta.csv, Stim_raw.csv, times.csv} + Fmatrix.csv
      passive384/ Figures/FigureS3_passive/Data/{same} + Fmatrix.csv
@@ -35,7 +35,7 @@ from oracle_py import REFERENCE_DIR as REF  # noqa: E402
 MODELS = {
     "ttpc512": ("GUI/BBP_TTPC_EXAMPLE/pyNeuroGPU_unix/Data",
                 ["BasicConstSegP.csv", "Sim.csv", "Stim_meta.csv", "Stim_raw0.csv", "times.csv",
-                 "AllParams_reference.csv"], None),
+                 "AllParams_reference.csv", "AllParams_for_params.csv", "opt_table.csv"], None),
     "mainen384": ("Figures/FigureS4_mainen/Data",
                   ["BasicConstSegP.csv", "ParamsM.csv", "Sim.csv", "Stim_meta.csv", "Stim_raw.csv",
                    "times.csv"], "Figures/FigureS4_mainen/Fmatrix.csv"),
