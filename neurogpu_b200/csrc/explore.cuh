@@ -54,6 +54,8 @@ __host__ __device__ __forceinline__ double dvdt_at(const PeakArgs& a, const floa
 
 // Removed peaks carry kPeakGone in their position word, kept ones kPeakKept.
 constexpr int32_t kPeakGone = 1 << 30, kPeakKept = 1 << 29;
+// Samples loaded ahead per thread (rows in flight; the scan is latency-bound).
+constexpr int kPeakChunk = 32;
 
 // The score of trace t (one thread's work; host-callable for tests).
 __host__ __device__ inline int dvdt_peaks_trace(const PeakArgs& a, int t) {
@@ -61,36 +63,53 @@ __host__ __device__ inline int dvdt_peaks_trace(const PeakArgs& a, int t) {
     int32_t* pos = a.pos + t;
     const int64_t ps = a.n_traces;
     const int nx = a.n_samples - 1;  // dvdt samples
-    // 1 + 2: local maxima at or above the height, in position order
+    // 1 + 2: local maxima at or above the height, in position order.  One
+    // pass over the samples, kPeakChunk loads in flight: x[j] is formed from
+    // samples j and j + 1 as they arrive, and a candidate is a rising sample
+    // (x[j-1] < x[j], 1 <= j <= nx - 2) whose run of equal values ends in a
+    // smaller sample (a peak at the run's middle), in a larger one (no peak;
+    // that sample is the next candidate) or in a NaN or the trace's end (no
+    // peak).  These are the decisions of scipy's scan, taken as the samples
+    // stream by instead of by looking ahead.
     int m = 0;
     if (nx >= 3) {
-        double xm = dvdt_at(a, v, 0), xi = dvdt_at(a, v, 1);
-        int i = 1;
-        while (i < nx - 1) {
-            bool advanced = false;
-            if (xm < xi) {
-                int ia = i + 1;
-                double xa = dvdt_at(a, v, ia);
-                while (ia < nx - 1 && xa == xi) {
-                    ++ia;
-                    xa = dvdt_at(a, v, ia);
-                }
-                if (xa < xi) {
-                    if (xi >= a.height && m < a.cap) pos[(int64_t)m++ * ps] = (i + ia - 1) / 2;
-                    // continue after sample ia (it is below the plateau: no peak starts there)
-                    i = ia + 1;
-                    if (i < nx - 1) {
-                        xm = xa;
-                        xi = dvdt_at(a, v, i);
-                        // x[i-1] is sample ia
+        float vprev = v[0];
+        double xprev = 0.0, pv = 0.0;
+        bool cand = false;
+        int i0 = 0;
+        for (int s0 = 1; s0 < a.n_samples; s0 += kPeakChunk) {
+            float buf[kPeakChunk];
+#pragma unroll
+            for (int u = 0; u < kPeakChunk; ++u)
+                if (s0 + u < a.n_samples) buf[u] = v[(int64_t)(s0 + u) * a.stride_sample];
+#pragma unroll
+            for (int u = 0; u < kPeakChunk; ++u) {
+                const int j = s0 + u - 1;  // dvdt sample of samples j, j + 1
+                if (j + 1 < a.n_samples) {
+                    const double x = ((double)buf[u] - (double)vprev) / a.dt;
+                    vprev = buf[u];
+                    if (j > 0) {
+                        if (cand) {
+                            if (x == pv) {
+                                // the run goes on
+                            } else if (x < pv) {
+                                if (pv >= a.height && m < a.cap) pos[(int64_t)m++ * ps] = (i0 + j - 1) / 2;
+                                cand = false;
+                            } else if (x > pv) {
+                                cand = j <= nx - 2;
+                                i0 = j;
+                                pv = x;
+                            } else {
+                                cand = false;  // NaN
+                            }
+                        } else if (xprev < x && j <= nx - 2) {
+                            cand = true;
+                            i0 = j;
+                            pv = x;
+                        }
                     }
-                    advanced = true;
+                    xprev = x;
                 }
-            }
-            if (!advanced) {
-                ++i;
-                xm = xi;
-                if (i < nx - 1) xi = dvdt_at(a, v, i);
             }
         }
     }
@@ -139,7 +158,7 @@ __host__ __device__ inline int dvdt_peaks_trace(const PeakArgs& a, int t) {
     return kept;
 }
 
-__global__ void __launch_bounds__(128) k_dvdt_peaks(const PeakArgs a) {
+__global__ void __launch_bounds__(64) k_dvdt_peaks(const PeakArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < a.n_traces) a.out[t] = dvdt_peaks_trace(a, t);
 }

@@ -1937,7 +1937,8 @@ static int launch_dvdt_peaks(PeakArgs a, int64_t scratch_bytes, cudaStream_t st)
         return fail(NGPU_E_INVALID, "dvdt peaks: scratch holds " + std::to_string(scratch_bytes) + " bytes, needs " +
                                         std::to_string(need));
     if (!a.v || !a.out || !a.pos) return fail(NGPU_E_INVALID, "dvdt peaks: null pointer");
-    k_dvdt_peaks<<<(a.n_traces + 127) / 128, 128, 0, st>>>(a);
+    // 64 threads a CTA: the traces of an exploration (10,000) spread over every SM
+    k_dvdt_peaks<<<(a.n_traces + 63) / 64, 64, 0, st>>>(a);
     g_launches++;
     NGPU_CUDA(cudaGetLastError());
     return NGPU_OK;
