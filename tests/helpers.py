@@ -44,3 +44,47 @@ def subthreshold_error(a: np.ndarray, b: np.ndarray, dt: float, window_ms: float
         if keep.any():
             worst = max(worst, float(np.max(np.abs(x[keep] - y[keep]))))
     return worst
+
+
+def numpy_cell_run(cell, amps, dts, stim_node: int, stim_area: float, rec_nodes, v_init: float, node_fn):
+    """FP64 numpy statement of one instance's run: the step of the FP64 oracle
+    (oracle/oracle.c run_instance, the reference's U/CudaStuff.cu:227-330) on
+    `cell`'s tree, with the channel update of node i given by
+    node_fn(i, init, v, dt, states) -> (states, I, G) (init: states at steady
+    state for v; otherwise the state update over dt at v; then the current I
+    and conductance G at v with the new states).  amps [nt] nA.  Returns V at
+    rec_nodes before each step's update, [n_rec, nt]."""
+    par = np.asarray(cell.parent)
+    a = np.asarray(cell.a, dtype=np.float64)
+    b = np.asarray(cell.b, dtype=np.float64)
+    cm = np.asarray(cell.cm, dtype=np.float64)
+    n = par.size
+    nt = len(amps)
+    V = np.full(n, float(v_init))
+    st, cur, cond = [None] * n, np.zeros(n), np.zeros(n)
+    for i in range(n):
+        st[i], cur[i], cond[i] = node_fn(i, True, float(v_init), float(dts[0]), None)
+    out = np.zeros((len(rec_nodes), nt))
+    for t in range(nt):
+        dt = float(dts[t])
+        out[:, t] = V[rec_nodes]
+        rhs = -cur.copy()
+        rhs[stim_node] += 100.0 * float(amps[t]) / stim_area
+        d = cond + cm / (dt * 1000.0)
+        for i in range(1, n):
+            dv = V[par[i]] - V[i]
+            rhs[i] -= a[i] * dv
+            rhs[par[i]] += b[i] * dv
+        for i in range(n - 1, 0, -1):  # leaf -> root, excess form
+            p = par[i]
+            di = d[i] - a[i]
+            d[p] += -b[i] * (d[i] / di)
+            rhs[p] += -b[i] * (rhs[i] / di)
+            d[i] = di
+        rhs[0] /= d[0]
+        for i in range(1, n):
+            rhs[i] = (rhs[i] - a[i] * rhs[par[i]]) / d[i]
+        V += rhs
+        for i in range(n):
+            st[i], cur[i], cond[i] = node_fn(i, False, V[i], dt, st[i])
+    return out

@@ -91,10 +91,9 @@ def test_table_errors():
         nmodl.generate({"q": bp}, tables={"q": {"f": (XS, YS)}})
 
 
-@pytest.mark.gpu
-def test_table_channel_runs_fp32_against_fp64(ngpu_built):
-    """A spiking cell with the HH demo channels and the table channel, FP32
-    against FP64 within the parity bounds."""
+def _table_workload(n_sets=8, t_stop=60.0, dt=0.025):
+    """A cell with the HH demo channels and the table channel (soma: hhdemo,
+    ktab, pas; dendrites: ktab, pas; axon: hhdemo, pas)."""
     from neurogpu_b200 import configs, nmodl
     from neurogpu_b200.model import build_model
     mods = sorted(MOD_DIR.glob("*.mod")) + sorted(TAB_DIR.glob("*.mod"))
@@ -109,14 +108,20 @@ def test_table_channel_runs_fp32_against_fp64(ngpu_built):
     base[g.param_index("g_pas")] = 3e-4
     base[g.param_index("e_pas")] = -65.0
     base[g.param_index("gbar_ktab")] = 0.005
-    n_sets, dt, t_stop = 8, 0.025, 60.0
     mult = np.exp(rng.uniform(np.log(0.7), np.log(1.4), (n_sets, 1)))
     params = np.broadcast_to(base[None, :, None], (n_sets, g.n_params, cell.n_sections)).copy()
     params[:, g.param_index("gnabar_hhdemo"), :] *= mult
     nt = int(round(t_stop / dt))
     amps = configs.step_amps([0.3, 0.8], nt, dt, 5.0, 50.0)
-    w = configs.Workload("demo_tab", cell, params.astype(np.float32), amps, dt, 0, float(cell.area[0]),
-                         np.array([0], dtype=np.int32), -65.0)
+    return configs.Workload("demo_tab", cell, params.astype(np.float32), amps, dt, 0, float(cell.area[0]),
+                            np.array([0], dtype=np.int32), -65.0), g
+
+
+@pytest.mark.gpu
+def test_table_channel_runs_fp32_against_fp64(ngpu_built):
+    """A spiking cell with the HH demo channels and the table channel, FP32
+    against FP64 within the parity bounds."""
+    w, _ = _table_workload()
     v32, bad32 = _sim(w, "fp32")
     v64, bad64 = _sim(w, "fp64")
     assert bad32 == 0 and bad64 == 0
