@@ -275,7 +275,9 @@ int ngpu_sim_features(ngpu_sim *s, int32_t site, double dt, double stim_on, doub
  *                          `site`: out_dev [n_sets][n_stim]
  *   scratch_dev: device memory of at least ngpu_dvdt_peaks_scratch_bytes
  *   bytes (the candidate peaks of every trace), owned by the caller.
- *   Errors: dt <= 0, distance < 1, a NaN height, too small a scratch.
+ *   The kernel runs on cuda_stream: the simulation's launches must be on
+ *   the same stream or finished.  Errors: dt <= 0, distance < 1, a NaN
+ *   height, too small a scratch.
  */
 int64_t ngpu_dvdt_peaks_scratch_bytes(int32_t n_traces, int32_t n_samples);
 int ngpu_trace_dvdt_peaks(const float *v_dev, int64_t stride_trace, int64_t stride_sample, int32_t n_traces,

@@ -186,6 +186,25 @@ def test_gen_params_is_the_reference_grid():
         explore.gen_params(base, 1, None, 1, None)
 
 
+def test_calc_scores_layout(tmp_path, monkeypatch):
+    """calc_scores on the host side: a VHotP file read as the reference
+    reads it, the overhang dropped, trace k at cell (k // nbins, k % nbins)
+    (the counts themselves come from the restatement here)."""
+    import torch
+    from neurogpu_b200 import formats
+    monkeypatch.setattr(explore, "dvdt_peak_counts", lambda v, dt, height, distance: torch.tensor(
+        [fpr.dvdt_peak_count(x, dt, height, distance) for x in v], dtype=torch.int32))
+    rng = np.random.default_rng(15)
+    nb = 5
+    tr = _spiky_traces(rng, nb * nb, 200)
+    p = tmp_path / "VHotP0.dat"
+    formats.write_vhot(p, np.concatenate([tr.reshape(-1).astype(np.float64), np.zeros(11)]))
+    s = explore.calc_scores(p, nbins=nb)
+    assert s.shape == (nb, nb) and s.dtype == np.float64
+    assert np.array_equal(s.reshape(-1), [fpr.dvdt_peak_count(v, DT) for v in tr])
+    assert s.max() > 0
+
+
 def test_entry_points_reject_bad_arguments(ngpu_built):
     """Argument checks of the C ABI (they return before any launch)."""
     from neurogpu_b200 import _ffi
