@@ -165,6 +165,32 @@ def test_kernel_code_on_the_host_matches_the_restatement(probe):
         assert _probe_counts(probe, np.zeros((1, n), dtype=np.float32) + np.arange(n) * 5)[0] == 0
 
 
+def test_kernel_code_on_oracle_traces(probe):
+    """Spiking traces of the reference's shipped TTPC cell (the FP64 oracle,
+    a 3 x 4 grid over g_pas and the soma's gNaTs2_t, 3168 steps of 0.1 ms),
+    rounded to float32 as the simulator records them: the kernel's per-trace
+    code built for the host counts what scipy counts."""
+    import oracle_py
+    from neurogpu_b200 import evaluator, formats
+    m = formats.read_data_dir(GOLD / "ttpc512", stim_index=0, params_file="AllParams_reference.csv")
+    mapping, g_na = _ttpc512_mapping(m)
+    base = np.zeros(14)
+    base[0], base[2] = 3e-5, g_na
+    grid = explore.gen_params(base, 0, base[0] * np.array([0.5, 1.0, 2.0]), 2,
+                              base[2] * np.array([0.25, 0.5, 1.0, 2.0]))
+    rows = evaluator.allparams_from_mapping(grid, *mapping)
+    nc = m.cell.n_sections
+    fp = rows.reshape(len(rows), rows.shape[1] // nc, nc).astype(np.float32)
+    params = formats.map_params(fp, int(m.raw["basic_const"]["NModels"][0]), fp.shape[1])
+    c = m.cell
+    v = np.asarray(oracle_py.run(c.parent, c.a, c.b, c.cm, c.section, c.n_sections, c.mechset.id, c.mech_mask,
+                                 params, m.amps[:1], m.dts, m.stim_node, m.stim_area, m.rec_nodes[:1], m.v_init))
+    tr = v[:, 0, 0, :].astype(np.float32)
+    got = _probe_counts(probe, tr)
+    assert _check_against_scipy(tr, got) >= 10
+    assert got.min() >= 1 and got.max() >= 10
+
+
 def test_gen_params_is_the_reference_grid():
     """The reference's nested loop (GUI/run_neuroGPU.py:15-31), restated."""
     names, lb, ub, base = explore.read_opt_table(GOLD / "ttpc512" / "opt_table.csv")
