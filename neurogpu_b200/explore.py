@@ -134,6 +134,8 @@ def calc_scores(volts, nbins: int = NBINS, dt: float = DT, height: float = HEIGH
     psize = nbins * nbins
     v = v.reshape(-1)
     nt = v.size // psize
+    if nt < 1:
+        raise ValueError(f"{v.size} samples hold no trace for each of the {psize} grid points")
     v = v[:nt * psize].reshape(psize, nt)   # the file's overhang is dropped, as there
     counts = dvdt_peak_counts(v, dt=dt, height=height, distance=distance)
     return counts.cpu().numpy().astype(np.float64).reshape(nbins, nbins)

@@ -229,6 +229,8 @@ def test_calc_scores_layout(tmp_path, monkeypatch):
     assert s.shape == (nb, nb) and s.dtype == np.float64
     assert np.array_equal(s.reshape(-1), [fpr.dvdt_peak_count(v, DT) for v in tr])
     assert s.max() > 0
+    with pytest.raises(ValueError):
+        explore.calc_scores(np.zeros(nb * nb - 1), nbins=nb)
 
 
 def test_entry_points_reject_bad_arguments(ngpu_built):
