@@ -45,7 +45,7 @@ def nrnMread(fileName) -> np.ndarray:
 # ---------------------------------------------------------------- AllParams
 def allparams_from_mapping(params_input: Sequence[Sequence[float]], template_row: Sequence[float],
                            indicator_row: Sequence[float], corrections: dict | None = None,
-                           out_path: str | Path | None = None) -> np.ndarray:
+                           out_path: str | Path | None = None, dtype=np.float64) -> np.ndarray:
     """GA parameter vectors -> AllParams rows (extractModel_mappings.py:290-331).
 
     template_row: one AllParams row of the model (AllParams_reference.csv);
@@ -54,13 +54,16 @@ def allparams_from_mapping(params_input: Sequence[Sequence[float]], template_row
     (create_params_to_all_params, :258-272); corrections: index -> value
     applied to every row (correction_mappings.json, :240-251).  Writes
     AllParams.csv as the reference does (the set count, then '%.5E' rows)
-    when out_path is given.  Returns [n_sets, len(template_row)] float64."""
+    when out_path is given.  Returns [n_sets, len(template_row)] of `dtype`
+    (float64; float32 gives the same values rounded entry by entry, built
+    without a float64 copy, as the simulator takes them)."""
     tmpl = np.asarray(template_row, dtype=np.float64)
     ind = np.asarray(indicator_row, dtype=np.float64)
     params = np.asarray(params_input, dtype=np.float64)
     if params.ndim != 2:
         raise ValueError("params_input must be [n_sets][n_params]")
-    out = np.repeat(tmpl[None, :], params.shape[0], axis=0)
+    out = np.empty((params.shape[0], tmpl.size), dtype=dtype)
+    out[:] = tmpl.astype(dtype)[None, :]
     for k in range(params.shape[1]):
         pos = np.nonzero(ind == PARAM_INDICATOR_BASE + k)[0]
         out[:, pos] = params[:, k:k + 1]

@@ -157,11 +157,11 @@ def grid_simulation(model: "formats.ReferenceModel", mapping: tuple, grid: np.nd
     shortest decimal that gives its float32 value back, the value times.csv
     holds (0.1, not the float32 0.100000001)."""
     from .sim import Model, Simulator
-    rows = allparams_from_mapping(grid, *mapping)
+    rows = allparams_from_mapping(grid, *mapping, dtype=np.float32)
     cell = model.cell
     n_comps = cell.n_sections
     n_file_params = rows.shape[1] // n_comps
-    file_params = rows.reshape(len(rows), n_file_params, n_comps).astype(np.float32)
+    file_params = rows.reshape(len(rows), n_file_params, n_comps)
     n_models = int(model.raw["basic_const"]["NModels"][0]) if model.raw else None
     params = formats.map_params(file_params, n_models, n_file_params) if n_models else file_params
     amps = np.asarray(model.amps[0] if stim is None else stim, dtype=np.float32).reshape(1, -1)

@@ -304,6 +304,20 @@ def _ttpc512_mapping(m):
                                           2: (TTPC.param_index("gNaTs2_tbar_NaTs2_t"), soma)}), nats.max()
 
 
+def test_float32_rows_equal_the_rounded_float64_rows():
+    """allparams_from_mapping(..., dtype=float32), the rows the exploration
+    uploads, equal the float64 rows rounded entry by entry, bit for bit."""
+    from neurogpu_b200 import evaluator, formats
+    m = formats.read_data_dir(GOLD / "ttpc512", stim_index=0, params_file="AllParams_reference.csv")
+    (tmpl, ind, _), g_na = _ttpc512_mapping(m)
+    _, _, _, base = explore.read_opt_table(GOLD / "ttpc512" / "opt_table.csv")
+    grid = explore.gen_params(base)
+    r64 = evaluator.allparams_from_mapping(grid, tmpl, ind, {5: 0.25})
+    r32 = evaluator.allparams_from_mapping(grid, tmpl, ind, {5: 0.25}, dtype=np.float32)
+    assert r32.dtype == np.float32 and r64.dtype == np.float64
+    assert np.array_equal(r32.view(np.uint32), r64.astype(np.float32).view(np.uint32))
+
+
 def test_mapping_for_marks_the_given_entries():
     from neurogpu_b200 import evaluator, formats
     m = formats.read_data_dir(GOLD / "ttpc512", stim_index=0, params_file="AllParams_reference.csv")
