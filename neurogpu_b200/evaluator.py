@@ -263,9 +263,9 @@ class MultiStimEvaluator:
 
     def simulate(self, param_values) -> np.ndarray:
         """V at the recording site, [n_individuals][n_stims][nt]."""
-        rows = allparams_from_mapping(param_values, *self.mapping)
+        rows = allparams_from_mapping(param_values, *self.mapping, dtype=np.float32)
         n_comps, n_file_params = self.model.cell.n_sections, rows.shape[1] // self.model.cell.n_sections
-        file_params = rows.reshape(len(rows), n_file_params, n_comps).astype(np.float32)
+        file_params = rows.reshape(len(rows), n_file_params, n_comps)
         n_models = int(self.model.raw["basic_const"]["NModels"][0]) if self.model.raw else None
         params = formats.map_params(file_params, n_models, n_file_params) if n_models else file_params
         run = self.run
